@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 pair-histogram hot path: pair-evals/s of the mixed-precision kernel vs the
+plain FP64 kernel on the 3D workload (N=65536 points in the unit cube, Float64, L2SF/T2SF/L3SF/T3SF
+fused, 64 log bins 1e-4..sqrt(3); seeded synthetic data).
+
+One step = one full pass of the pair loop over the workload (all N(N-1)/2 pairs, every operator).
+  value  : mixed kernel, inputs resident in HBM, device outputs; CUDA events on the library's stream,
+           L2 flushed (256 MiB write) before every timed step.
+  e2e    : the same metric through the C ABI with host buffers: H2D of x,u (pinned) + kernels + D2H of
+           sums/counts inside the timed region.
+  fp64   : the plain FP64 kernel on the same workload, timed like `value`.
+Multi-GPU (torchrun): every rank runs the whole workload (replicas, weak scaling); the elapsed time
+is the max over ranks.
+
+--impl reference: the reference's CPU path restated (ThreadedBackend: round-robin outer-index chunks,
+per-thread histograms), all host threads, on a bounded sample of the same workload.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "structurefunctions.jl_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "pair-evals/s mixed-precision vs FP64 kernel on B200; p50/p99 slice latency"
+UNIT = "pair-evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample length")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [t.strip() for t in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------ ours
+
+def measure_peak(device, fp64):
+    lib = C.CDLL(os.path.join(ROOT, "structurefunctions.jl_b200", "libsfb200_probe.so"))
+    lib.sfb200_probe_fma.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    t, ms = C.c_double(), C.c_double()
+    rc = lib.sfb200_probe_fma(device, 1 if fp64 else 0, C.byref(t), C.byref(ms))
+    return t.value if rc == 0 else None
+
+
+def run_ours(args):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    import sfb200 as SF
+    from sfb200 import _abi, _lib, synthetic
+    from sfb200.api import plan_description
+
+    w = synthetic.config(args.config)
+    x_host = np.asfortranarray(w.x)
+    u_host = np.asfortranarray(w.u)
+    n = w.n
+    pairs = w.pairs
+    ctx = _lib.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+
+    # device-resident inputs: column-major (W, N) == row-major (N, W)
+    xd = torch.from_numpy(np.ascontiguousarray(x_host.T)).cuda()
+    ud = torch.from_numpy(np.ascontiguousarray(u_host.T)).cuda()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def make(precision):
+        desc, keep = plan_description(w.ops, w.u.shape[0], w.distance_bins, w.value_bins, w.metric, precision,
+                                      w.x.dtype, w.u.dtype)
+        plan = _lib.Plan(ctx, desc, keep)
+        sums = torch.zeros(plan.n_sums, dtype=torch.float64, device="cuda")
+        counts = torch.zeros(plan.n_counts, dtype=torch.int64, device="cuda")
+        return plan, sums, counts
+
+    def device_steps(plan, sums, counts, steps, warmup):
+        flags = _abi.RUN_DEVICE_INPUT | _abi.RUN_DEVICE_OUTPUT
+        launches = 0
+        kernel_ms = []
+        for _ in range(warmup):
+            plan.run(xd.data_ptr(), ud.data_ptr(), n, flags, sums.data_ptr(), counts.data_ptr(), ctx.stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        total = 0.0
+        with torch.cuda.stream(stream):
+            for _ in range(steps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                plan.run(xd.data_ptr(), ud.data_ptr(), n, flags, sums.data_ptr(), counts.data_ptr(), ctx.stream)
+                e1.record(stream)
+                e1.synchronize()
+                total += e0.elapsed_time(e1)
+                st = plan.stats()
+                kernel_ms.append(st["kernel_ms"])
+                launches += st["kernel_launches"]
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return total, kernel_ms, launches, plan.stats()
+
+    clocks = ClockSampler(local)
+    mixed, msums, mcounts = make("mixed")
+    fp64, fsums, fcounts = make("fp64")
+
+    clocks.start()
+    t_mixed, kms_mixed, launches_mixed, st_mixed = device_steps(mixed, msums, mcounts, args.steps, args.warmup)
+    t_fp64, kms_fp64, launches_fp64, st_fp64 = device_steps(fp64, fsums, fcounts, args.steps, args.warmup)
+    clk = clocks.stop()
+
+    # counts of the two kernels must agree (bit-exact binning in both)
+    same_counts = bool(torch.equal(mcounts, fcounts))
+
+    # e2e through the C ABI with host buffers (pinned)
+    xp = torch.from_numpy(np.ascontiguousarray(x_host.T)).pin_memory()
+    up = torch.from_numpy(np.ascontiguousarray(u_host.T)).pin_memory()
+    hs = torch.zeros(mixed.n_sums, dtype=torch.float64).pin_memory()
+    hc = torch.zeros(mixed.n_counts, dtype=torch.int64).pin_memory()
+    for _ in range(args.warmup):
+        mixed.run(xp.data_ptr(), up.data_ptr(), n, 0, hs.data_ptr(), hc.data_ptr(), ctx.stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e2e_total = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        mixed.run(xp.data_ptr(), up.data_ptr(), n, 0, hs.data_ptr(), hc.data_ptr(), ctx.stream)
+        e2e_total += time.perf_counter() - t0
+    torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t_mixed = max_over_ranks(t_mixed)
+    t_fp64 = max_over_ranks(t_fp64)
+    e2e_total = max_over_ranks(e2e_total * 1e3)
+
+    ms_mixed = t_mixed / args.steps
+    ms_fp64 = t_fp64 / args.steps
+    value = world * pairs / (ms_mixed * 1e-3)
+    fp64_value = world * pairs / (ms_fp64 * 1e-3)
+    e2e_value = world * pairs / (e2e_total / args.steps * 1e-3)
+
+    kmed_mixed = sorted(kms_mixed)[len(kms_mixed) // 2]
+    kmed_fp64 = sorted(kms_fp64)[len(kms_fp64) // 2]
+    peak32 = measure_peak(local, False)
+    peak64 = measure_peak(local, True)
+    flops = w.flops_per_pair
+    achieved = flops * pairs / (kmed_mixed * 1e-3) / 1e12
+    achieved64 = flops * pairs / (kmed_fp64 * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"{args.config}_mixed_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_mixed,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "precision": "mixed: FP32 pair arithmetic with two-sum accumulation, FP64 recheck of near-edge/short "
+                         "pairs, FP64 merge",
+            "data": "synthetic (seeded; no dataset)",
+            "config": {
+                "workload": w.name,
+                "n_points": n,
+                "pairs_per_step": pairs,
+                "operators": [repr(o) for o in w.ops],
+                "distance_bins": len(w.distance_bins) - 1,
+                "l2": "flushed before every timed step (256 MiB write); inputs 3 MB",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "tile": st_mixed["tile"],
+                "blocks": st_mixed["blocks"],
+            },
+            "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms_fp64, "kernel_ms": kmed_fp64,
+                     "roofline_frac_fp64": (achieved64 / peak64) if peak64 else None},
+            "mixed_over_fp64": value / fp64_value,
+            "counts_equal_mixed_fp64": same_counts,
+            "rechecked_pairs_per_step": st_mixed["rechecked"],
+            "roofline": {
+                "bound": "fp32",
+                "achieved": achieved,
+                "peak": peak32,
+                "unit": "TFLOP/s",
+                "frac": (achieved / peak32) if peak32 else None,
+                "traffic": traffic,
+                "flops_per_pair": flops,
+                "kernel_ms": kmed_mixed,
+                "peak_source": "measured FP32 FMA probe on this GPU (MEASURED_PEAKS.json has no FP32 vector "
+                               "figure); nominal 148 SM x 128 lanes x 2 x clock",
+            },
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": int(x_host.nbytes + u_host.nbytes),
+                    "d2h_bytes_per_step": int(mixed.n_sums * 8 + mixed.n_counts * 8 + 8)},
+            "gpu_launches": launches_mixed,
+            "clocks": clk,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    mixed.close()
+    fp64.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------------------ CPU
+
+def cpu_sample_rate(w, npts, threads):
+    import oracle_py
+    from sfb200.api import plan_description
+
+    desc, keep = plan_description(w.ops, w.u.shape[0], w.distance_bins, w.value_bins, w.metric, "fp64",
+                                  w.x.dtype, w.u.dtype)
+    x = w.x[:, :npts]
+    u = w.u[:, :npts]
+    t0 = time.perf_counter()
+    oracle_py.run(desc, x, u, threads=threads)
+    dt = time.perf_counter() - t0
+    return npts * (npts - 1) // 2 / dt, dt
+
+
+def cpu_baseline(w, seconds):
+    import oracle_py
+
+    threads = max(1, oracle_py.threads_available())
+    rate, _ = cpu_sample_rate(w, min(w.n, 4096), threads)
+    npts = int(min(w.n, math.sqrt(2.0 * rate * seconds)))
+    rate, dt = cpu_sample_rate(w, npts, threads)
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {npts} points of the workload ({npts * (npts - 1) // 2} pairs), {dt:.1f} s; "
+                      "C restatement of ThreadedBackend (round-robin outer-index chunks, per-thread histograms)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    import oracle_py
+    from sfb200 import synthetic
+
+    w = synthetic.config(args.config)
+    threads = max(1, oracle_py.threads_available())
+    rate0, _ = cpu_sample_rate(w, min(w.n, 4096), threads)
+    per_step = 2.0 if args.steps <= 10 else 1.0
+    npts = int(min(w.n, math.sqrt(2.0 * rate0 * per_step)))
+    for _ in range(args.warmup):
+        cpu_sample_rate(w, min(npts, 2048), threads)
+    total, pairs = 0.0, 0
+    for _ in range(args.steps):
+        r, dt = cpu_sample_rate(w, npts, threads)
+        total += dt
+        pairs += npts * (npts - 1) // 2
+    value = pairs / total
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": w.name, "sample_points_per_step": npts},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"first {npts} of {w.n} points per step; C restatement of the reference "
+                                   "ThreadedBackend (no Julia toolchain on this machine)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,194 @@
+/*
+ * sfb200.h -- C ABI of the B200 pair-histogram backend for structure functions.
+ *
+ * One library call replaces the O(N^2) pair loop that the reference runs behind
+ * `calculate_structure_function` / `calculate_structure_function!`:
+ *
+ *   reference entry                         file:line (jbphyswx/StructureFunctions.jl)
+ *   --------------------------------------  -------------------------------------------------------
+ *   public 1D entry                         src/Calculations/dispatch.jl:64-91
+ *   public joint (distance x value) entry   src/Calculations/dispatch.jl:108-136
+ *   mutating entry (accumulate into)        src/Calculations/dispatch.jl:346-373
+ *   backend routing (a B200Backend method)  src/Calculations/dispatch.jl:377-594
+ *   Euclidean pair loop                     src/Calculations/serial.jl:68-101
+ *   non-Euclidean (sphere) pair loop        src/Calculations/serial.jl:228-267
+ *   joint pair loops                        src/Calculations/serial_2d.jl:49-85, 260-303
+ *   squared-distance digitize plans         src/BinEdges.jl:410-558
+ *   LinearBinEdges search                   src/BinEdges.jl:114-131
+ *   result accumulators                     src/StructureFunctionObjects.jl:50-115
+ *
+ * Everything in this header is plain C: pointers, sizes, enums and POD structs. No CUDA or
+ * torch type appears in a signature; CUDA streams travel as `void*`.
+ *
+ * Conventions
+ *   - x is (W, N) column-major: x[k + W*i] is coordinate k of point i. W = D for flat geometry,
+ *     W = 2 (lon, lat) for the sphere. u is (D, N) column-major, D in {2, 3}.
+ *   - Bins are right-inclusive (a, b]; a pair lands in bin b (1-based in the reference) when
+ *     edge[b-1] < key <= edge[b]. Out-of-range pairs are dropped, as in the reference.
+ *   - Outputs: sums are double, counts are uint64. For a 1D plan with n_ops operators and nb
+ *     distance bins, sums is (nb, n_ops) column-major (operator k at sums + k*nb) and counts
+ *     has nb entries (shared by all operators: a pair is counted once per bin). For a joint plan
+ *     (exactly one operator), sums and counts are (n_dist, n_val) column-major, as the reference's
+ *     StructureFunction2DSumsAndCounts matrices.
+ *   - Every call returns 0 on success or a negative sfb200_status. Nothing aborts or traps.
+ */
+#ifndef SFB200_H
+#define SFB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SFB200_ABI_VERSION 1
+#define SFB200_MAX_OPS 8
+
+#if defined(__GNUC__)
+#define SFB200_API __attribute__((visibility("default")))
+#else
+#define SFB200_API
+#endif
+
+typedef enum {
+    SFB200_OK = 0,
+    SFB200_ERR_INVALID_ARG = -1,   /* maps to ArgumentError in the host glue */
+    SFB200_ERR_UNSUPPORTED = -2,   /* maps to ArgumentError: shape/metric/operator not on this path */
+    SFB200_ERR_OOM = -3,
+    SFB200_ERR_CUDA = -4,
+    SFB200_ERR_TIMEOUT = -5,
+    SFB200_ERR_QUEUE_FULL = -6,
+    SFB200_ERR_DIMENSION = -7      /* maps to DimensionMismatch */
+} sfb200_status;
+
+/* Pair geometry, chosen by the host from the distance metric (reference
+ * src/HelperFunctions.jl:390-417 pair_geometry_for). */
+typedef enum {
+    SFB200_GEOM_FLAT = 0,    /* Distances.Euclidean -> FlatGeometry{D} */
+    SFB200_GEOM_SPHERE = 1   /* Distances.Haversine(radius) / SphericalAngle -> SphericalGeometry{D} */
+} sfb200_geometry;
+
+/* Angle unit of sphere coordinates: Haversine takes degrees, SphericalAngle radians
+ * (reference src/HelperFunctions.jl:404-409). */
+typedef enum { SFB200_ANGLE_DEG = 0, SFB200_ANGLE_RAD = 1 } sfb200_angle_unit;
+
+/* Operator kinds (reference src/StructureFunctionTypes.jl:43-151). */
+typedef enum {
+    SFB200_OP_PROJECTED = 0, /* ProjectedStructureFunctionType{NL,NT}: L2SF={2,0}, T2SF={0,2}, L3SF={3,0},
+                                T3SF={0,3}, L2T1SF={2,1}, L1T2SF={1,2}, delta-u_L={1,0}, ... */
+    SFB200_OP_S2 = 1,        /* SecondOrderStructureFunctionType: |du|^2 */
+    SFB200_OP_S3 = 2,        /* ThirdOrderStructureFunctionType: du_L |du|^2 */
+    SFB200_OP_FULLVEC = 3,   /* FullVectorStructureFunctionType{NF}: |du|^NF */
+    SFB200_OP_T2C = 4,       /* TransverseComponentSecondOrderStructureFunctionType: |du_t|^2/(D-1) */
+    SFB200_OP_L1T2C = 5      /* LongitudinalTransverseComponentThirdOrderStructureFunctionType */
+} sfb200_op_kind;
+
+typedef struct {
+    int32_t kind; /* sfb200_op_kind */
+    int32_t nl;   /* PROJECTED: longitudinal power NL >= 0 */
+    int32_t nt;   /* PROJECTED: transverse power NT >= 0 */
+    int32_t nf;   /* FULLVEC: power NF >= 0 */
+} sfb200_operator;
+
+/* Bin-edge descriptions (reference src/BinEdges.jl). */
+typedef enum {
+    SFB200_BINS_TABLE = 0,   /* sorted edge vector (BinEdges, binary search). For flat geometry the
+                                library squares the edges in double (= _sq_edges(Float64, v),
+                                src/BinEdges.jl:440). */
+    SFB200_BINS_SQTABLE = 1, /* flat only: the caller passes the squared-edge table itself, as built by
+                                squared_digitize_plan(...).sqedges (src/BinEdges.jl:447-463); this is
+                                how Float32 edges and LogBinEdges keep the reference's exact table. */
+    SFB200_BINS_LINEAR = 2   /* LinearBinEdges (an AbstractRange): FMA search of src/BinEdges.jl:114-131
+                                with (first, last, inv_step, step, n_edges) as stored by the reference. */
+} sfb200_bins_kind;
+
+typedef struct {
+    int32_t kind;        /* sfb200_bins_kind */
+    int32_t n_edges;     /* number of edges (bins = n_edges - 1); >= 2 */
+    const double* edges; /* TABLE / SQTABLE: n_edges values, copied at plan creation */
+    double first, last, inv_step, step; /* LINEAR */
+} sfb200_bins;
+
+typedef enum {
+    SFB200_PREC_FP64 = 0,  /* plain form: every pair in FP64 */
+    SFB200_PREC_MIXED = 1  /* FP32 bulk, FP64 recheck of near-edge / short / near-antipodal pairs,
+                              FP64 merge */
+} sfb200_precision;
+
+typedef enum { SFB200_F64 = 0, SFB200_F32 = 1 } sfb200_dtype;
+
+typedef struct {
+    int32_t geometry;    /* sfb200_geometry */
+    int32_t dim;         /* velocity components D in {2, 3} */
+    int32_t angle_unit;  /* sphere only */
+    double radius;       /* sphere only: r = radius * central angle */
+    int32_t n_ops;       /* 1..SFB200_MAX_OPS (joint plans: exactly 1) */
+    sfb200_operator ops[SFB200_MAX_OPS];
+    sfb200_bins distance;
+    int32_t joint;       /* 0: 1D histogram; 1: joint (distance x value) histogram */
+    sfb200_bins value;   /* joint only (TABLE or LINEAR) */
+    int32_t precision;   /* sfb200_precision */
+    int32_t x_dtype;     /* sfb200_dtype of x */
+    int32_t u_dtype;     /* sfb200_dtype of u */
+} sfb200_plan_desc;
+
+/* sfb200_run flags */
+#define SFB200_RUN_DEVICE_INPUT  0x1u /* x and u are device pointers (already in HBM) */
+#define SFB200_RUN_DEVICE_OUTPUT 0x2u /* sums and counts are device pointers; the call is then
+                                         asynchronous on the stream */
+#define SFB200_RUN_ACCUMULATE    0x4u /* add into sums/counts (mutating API semantics) instead of
+                                         overwriting them */
+
+typedef struct {
+    int64_t pairs;          /* N(N-1)/2 of the last run */
+    int64_t rechecked;      /* pairs that took the FP64 recheck path (mixed precision) */
+    double kernel_ms;       /* device time of the pair kernel(s), CUDA events */
+    int32_t tile;           /* tile size the autotuner chose */
+    int32_t blocks;         /* persistent blocks launched */
+    int32_t threads;        /* threads per block */
+    int32_t kernel_launches;/* kernels launched by the last run */
+} sfb200_stats;
+
+typedef struct sfb200_ctx sfb200_ctx;
+typedef struct sfb200_plan sfb200_plan;
+
+/* Library ABI version (SFB200_ABI_VERSION). */
+SFB200_API int sfb200_abi_version(void);
+
+/* Context: one CUDA device, one stream, device workspace pool.
+ * Replaces: the GPU workspace object of ext/gpu/workspace.jl:25-56. */
+SFB200_API int sfb200_ctx_create(int device, sfb200_ctx** out);
+SFB200_API int sfb200_ctx_destroy(sfb200_ctx* ctx);
+/* Last error text of this context (never NULL). */
+SFB200_API const char* sfb200_last_error(const sfb200_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work. */
+SFB200_API void* sfb200_ctx_stream(sfb200_ctx* ctx);
+
+/* Plan: validated operator set + bin tables + precision for one input layout.
+ * Replaces: BinEdges / squared_digitize_plan construction (src/BinEdges.jl:362-469) and the
+ * operator-to-kernel mapping of the GPU route (ext/StructureFunctionsKernelAbstractionsExt.jl:385-401). */
+SFB200_API int sfb200_plan_create(sfb200_ctx* ctx, const sfb200_plan_desc* desc, sfb200_plan** out);
+SFB200_API int sfb200_plan_destroy(sfb200_plan* plan);
+/* Number of doubles in `sums` and of uint64 in `counts` that sfb200_run writes. */
+SFB200_API int sfb200_plan_output_sizes(const sfb200_plan* plan, int64_t* n_sums, int64_t* n_counts);
+
+/* Run the pair hot path over N points.
+ * Replaces: _dispatch_execution_backend(::GPUBackend, ::PointField, ...) -> gpu_calculate_structure_function
+ * (src/Calculations/dispatch.jl:537-544, ext/StructureFunctionsKernelAbstractionsExt.jl:385-401, 630-675)
+ * and, with SFB200_RUN_ACCUMULATE, _dispatch_execution_backend! (dispatch.jl:399-404, accumulate-into
+ * semantics of _accumulate_gpu_sf_host!, ext/StructureFunctionsKernelAbstractionsExt.jl:678-719).
+ * `stream` may be NULL (context stream). With host outputs the call returns after the results are
+ * copied back. */
+SFB200_API int sfb200_run(sfb200_plan* plan, const void* x, const void* u, int64_t n, uint32_t flags,
+               double* sums, uint64_t* counts, void* stream);
+
+/* Statistics of the last sfb200_run on this plan. */
+SFB200_API int sfb200_plan_last_stats(const sfb200_plan* plan, sfb200_stats* out);
+
+/* Autotuner override (0 = automatic): tile size, threads per block, blocks per SM. */
+SFB200_API int sfb200_plan_set_launch(sfb200_plan* plan, int tile, int threads, int blocks_per_sm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SFB200_H */

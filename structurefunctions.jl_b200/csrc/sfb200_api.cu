@@ -1,0 +1,834 @@
+// sfb200_api.cu -- the C ABI (include/sfb200.h): contexts, plans, device workspace, runs.
+//
+// A run is: [H2D copy of the caller's arrays] -> pack kernel (SoA + FP32 images + bounds) ->
+// [FP32 window table] -> [joint value windows] -> pair kernel -> [copy-out kernel | D2H copy].
+// Everything is queued on one stream; host outputs are returned after a stream synchronize.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/sfb200.h"
+#include "sfb200_internal.h"
+#include "sfb200_kernels.cuh"
+#include "sfb200_prep.cuh"
+
+using namespace sfb;
+
+struct sfb200_ctx {
+    int device = 0;
+    int nsm = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+};
+
+struct sfb200_plan {
+    sfb200_ctx* ctx = nullptr;
+    sfb200_plan_desc desc{};
+    bool sphere = false, mixed = false, joint = false;
+    int D = 0, W = 0, nb = 0, nv = 0, nops = 0, nops_pad = 0, opl = 0, vorder = 1;
+    GenOps gen{};
+    // exact key tables (flat: squared edges; sphere: edges with -0.0 moved just below +0.0)
+    std::vector<double> exact_tab;
+    double* d_exact = nullptr;
+    std::vector<double> vedges;
+    double* d_vedges = nullptr;
+    LinearParams dlin{}, vlin{};
+    // FP64 table
+    LutGeom lg64{};
+    LutEntry64* d_lut64 = nullptr;
+    int lut64_bytes = 0;
+    // FP32 table (mixed): edge keys, geometry, window parameters
+    std::vector<double> ck;
+    double* d_ck = nullptr;
+    LutGeom lg32{};
+    LutEntry32* d_lut32 = nullptr;
+    WindowParams wp{};
+    double* d_rowlo = nullptr;
+    float* d_vwin = nullptr;
+    // workspace
+    long long cap = 0;
+    void* d_rawx = nullptr;
+    void* d_rawu = nullptr;
+    double* d_X64 = nullptr;
+    double* d_U64 = nullptr;
+    float* d_XF = nullptr;
+    float* d_UF = nullptr;
+    long long n_sums = 0, n_counts = 0;
+    double* d_sums = nullptr;
+    unsigned long long* d_counts = nullptr;
+    unsigned long long* d_aux = nullptr;  // [0] rechecked pairs, [1] |x| bound, [2] |u| bound
+    std::vector<double> h_sums;
+    std::vector<unsigned long long> h_counts;
+    sfb200_stats stats{};
+    bool stats_pending = false;
+    int tile_ovr = 0, threads_ovr = 0, bps_ovr = 0;
+};
+
+// ------------------------------------------------------------------------------- errors
+
+static int set_err(sfb200_ctx* ctx, int code, const char* fmt, ...)
+{
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->err = buf;
+    }
+    return code;
+}
+
+static int cuda_fail(sfb200_ctx* ctx, cudaError_t e, const char* what)
+{
+    return set_err(ctx, SFB200_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+#define CK(call)                                                       \
+    do {                                                               \
+        cudaError_t e_ = (call);                                       \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);       \
+    } while (0)
+
+extern "C" int sfb200_abi_version(void) { return SFB200_ABI_VERSION; }
+
+extern "C" const char* sfb200_last_error(const sfb200_ctx* ctx)
+{
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+// ------------------------------------------------------------------------------- context
+
+extern "C" int sfb200_ctx_create(int device, sfb200_ctx** out)
+{
+    if (!out) return SFB200_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return SFB200_ERR_CUDA;
+    if (device < 0 || device >= ndev) return SFB200_ERR_INVALID_ARG;
+    sfb200_ctx* ctx = new (std::nothrow) sfb200_ctx();
+    if (!ctx) return SFB200_ERR_OOM;
+    ctx->device = device;
+    if ((e = cudaSetDevice(device)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&ctx->ev0)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) {
+        delete ctx;
+        return SFB200_ERR_CUDA;
+    }
+    *out = ctx;
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_ctx_destroy(sfb200_ctx* ctx)
+{
+    if (!ctx) return SFB200_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SFB200_OK;
+}
+
+extern "C" void* sfb200_ctx_stream(sfb200_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+// ------------------------------------------------------------------------------- plan building
+
+static int op_code(const sfb200_operator& o)
+{
+    switch (o.kind) {
+    case SFB200_OP_PROJECTED:
+        if (o.nl == 1 && o.nt == 0) return OC_L1;
+        if (o.nl == 2 && o.nt == 0) return OC_L2;
+        if (o.nl == 0 && o.nt == 2) return OC_T2;
+        if (o.nl == 3 && o.nt == 0) return OC_L3;
+        if (o.nl == 0 && o.nt == 3) return OC_T3;
+        if (o.nl == 1 && o.nt == 2) return OC_L1T2;
+        if (o.nl == 2 && o.nt == 1) return OC_L2T1;
+        return OC_GEN;
+    case SFB200_OP_S2: return OC_S2;
+    case SFB200_OP_S3: return OC_S3;
+    case SFB200_OP_FULLVEC: return o.nf == 2 ? OC_S2 : OC_GEN;
+    case SFB200_OP_T2C: return OC_T2C;
+    case SFB200_OP_L1T2C: return OC_L1T2C;
+    }
+    return OC_GEN;
+}
+
+static int op_order(const sfb200_operator& o)
+{
+    switch (o.kind) {
+    case SFB200_OP_PROJECTED: return o.nl + o.nt;
+    case SFB200_OP_S2: case SFB200_OP_T2C: return 2;
+    case SFB200_OP_S3: case SFB200_OP_L1T2C: return 3;
+    case SFB200_OP_FULLVEC: return o.nf;
+    }
+    return 1;
+}
+
+static double bits_to_double(unsigned long long b)
+{
+    double d;
+    std::memcpy(&d, &b, 8);
+    return d;
+}
+
+// Cell geometry over FP64 keys for the exact table.
+static void build_lut64(const std::vector<double>& tab, LutGeom& g, std::vector<LutEntry64>& out)
+{
+    double mn = INFINITY, mx = 0.0;
+    for (double v : tab) {
+        if (v > 0.0 && std::isfinite(v)) { mn = std::min(mn, v); mx = std::max(mx, v); }
+    }
+    int e_lo = 0, e_hi = 0;
+    if (mx > 0.0) {
+        e_lo = std::max(std::ilogb(mn) - 1, -1022);
+        e_hi = std::min(std::ilogb(mx) + 1, 1023);
+    }
+    int m = 3;
+    for (;; ++m) {
+        const long long nc = (long long)(e_hi - e_lo + 1) << m;
+        const int shift = 52 - m;
+        const long long base = (long long)(e_lo + 1023) << m;
+        bool multi = false;
+        // a cell with two distinct edge values needs a finer m
+        for (size_t k = 1; k < tab.size() && !multi; ++k) {
+            if (!(tab[k] > 0.0) || !std::isfinite(tab[k]) || tab[k] == tab[k - 1] || !(tab[k - 1] > 0.0)) continue;
+            unsigned long long ba, bb;
+            std::memcpy(&ba, &tab[k - 1], 8);
+            std::memcpy(&bb, &tab[k], 8);
+            long long ca = std::min(std::max((long long)(ba >> shift) - base, 0ll), nc - 1);
+            long long cb = std::min(std::max((long long)(bb >> shift) - base, 0ll), nc - 1);
+            if (ca == cb) multi = true;
+        }
+        if (!multi || m >= 10 || ((long long)(e_hi - e_lo + 1) << (m + 1)) > 4096) break;
+    }
+    g.shift = 52 - m;
+    g.ncell = (e_hi - e_lo + 1) << m;
+    g.base = (long long)(e_lo + 1023) << m;
+    out.assign(g.ncell, LutEntry64{});
+    for (int c = 0; c < g.ncell; ++c) {
+        const double klo = (c == 0) ? 0.0 : bits_to_double((unsigned long long)(g.base + c) << g.shift);
+        const double khi = (c == g.ncell - 1) ? INFINITY : bits_to_double((unsigned long long)(g.base + c + 1) << g.shift);
+        int below = 0, cnt = 0, distinct = 0;
+        double val = NAN;
+        for (double v : tab) {
+            if (v < klo) { ++below; continue; }
+            const bool inside = (c == g.ncell - 1) ? (v >= klo) : (v >= klo && v < khi);
+            if (inside) {
+                if (cnt == 0 || v != val) ++distinct;
+                val = v;
+                ++cnt;
+            }
+        }
+        LutEntry64 e;
+        e.base = below;
+        e.mult = cnt;
+        e.e = cnt ? val : NAN;
+        if (distinct > 1) e.mult = LUT_FLAG_SLOW;
+        out[c] = e;
+    }
+}
+
+// Cell geometry over FP32 keys for the window table; fails if the edge keys leave FP32's range.
+static bool geom_lut32(const std::vector<double>& keys, LutGeom& g)
+{
+    double mn = INFINITY, mx = 0.0;
+    for (double v : keys) {
+        if (v > 0.0 && std::isfinite(v)) { mn = std::min(mn, v); mx = std::max(mx, v); }
+    }
+    int e_lo = 0, e_hi = 0;
+    if (mx > 0.0) {
+        e_lo = std::ilogb(mn) - 2;
+        e_hi = std::ilogb(mx) + 1;
+        if (e_lo < -100 || e_hi > 100) return false;
+    }
+    int m = 3;
+    for (;; ++m) {
+        const long long nc = (long long)(e_hi - e_lo + 1) << m;
+        const int shift = 23 - m;
+        const long long base = (long long)(e_lo + 127) << m;
+        bool multi = false;
+        for (size_t k = 1; k < keys.size() && !multi; ++k) {
+            if (!(keys[k] > 0.0) || keys[k] == keys[k - 1] || !(keys[k - 1] > 0.0)) continue;
+            const float fa = (float)keys[k - 1], fb = (float)keys[k];
+            unsigned ba, bb;
+            std::memcpy(&ba, &fa, 4);
+            std::memcpy(&bb, &fb, 4);
+            long long ca = std::min(std::max((long long)(ba >> shift) - base, 0ll), nc - 1);
+            long long cb = std::min(std::max((long long)(bb >> shift) - base, 0ll), nc - 1);
+            if (ca == cb) multi = true;
+        }
+        if (!multi || m >= 10 || ((long long)(e_hi - e_lo + 1) << (m + 1)) > 2048) break;
+    }
+    g.shift = 23 - m;
+    g.ncell = (e_hi - e_lo + 1) << m;
+    g.base = (long long)(e_lo + 127) << m;
+    return true;
+}
+
+static double chord2_of(double r, double radius)
+{
+    if (r < 0.0 || (r == 0.0 && std::signbit(r))) return -1.0;
+    if (r == 0.0) return 0.0;
+    const double half = r / (2.0 * radius);
+    if (half >= 0.5 * M_PI) return 5.0;
+    const double s = 2.0 * std::sin(half);
+    return s * s;
+}
+
+static int validate_bins(sfb200_ctx* ctx, const sfb200_bins& b, const char* what, bool allow_sq)
+{
+    if (b.n_edges < 2) return set_err(ctx, SFB200_ERR_INVALID_ARG, "%s: need at least 2 edges", what);
+    if (b.n_edges > 65536) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "%s: more than 65536 edges", what);
+    if (b.kind == SFB200_BINS_LINEAR) {
+        if (!(std::isfinite(b.first) && std::isfinite(b.last) && std::isfinite(b.inv_step) &&
+              std::isfinite(b.step) && b.step > 0.0 && b.last > b.first))
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "%s: LinearBinEdges needs finite first < last and step > 0", what);
+        return SFB200_OK;
+    }
+    if (b.kind == SFB200_BINS_SQTABLE && !allow_sq)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "%s: a squared-edge table is only meaningful for Euclidean distances", what);
+    if (b.kind != SFB200_BINS_TABLE && b.kind != SFB200_BINS_SQTABLE)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "%s: unknown bin kind %d", what, b.kind);
+    if (!b.edges) return set_err(ctx, SFB200_ERR_INVALID_ARG, "%s: edges pointer is NULL", what);
+    for (int k = 0; k < b.n_edges; ++k) {
+        if (std::isnan(b.edges[k])) return set_err(ctx, SFB200_ERR_INVALID_ARG, "%s: NaN edge", what);
+        if (k && b.edges[k] < b.edges[k - 1])
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "%s: edges must be sorted (non-decreasing)", what);
+    }
+    return SFB200_OK;
+}
+
+static LinearParams linear_of(const sfb200_bins& b)
+{
+    LinearParams p;
+    p.first = b.first;
+    p.last = b.last;
+    p.inv_step = b.inv_step;
+    p.step = b.step;
+    p.neg_f_inv = -b.first * b.inv_step;
+    p.n = b.n_edges;
+    return p;
+}
+
+static void free_workspace(sfb200_plan* p)
+{
+    cudaFree(p->d_rawx); cudaFree(p->d_rawu);
+    cudaFree(p->d_X64); cudaFree(p->d_U64); cudaFree(p->d_XF); cudaFree(p->d_UF);
+    p->d_rawx = p->d_rawu = nullptr;
+    p->d_X64 = p->d_U64 = nullptr;
+    p->d_XF = p->d_UF = nullptr;
+    p->cap = 0;
+}
+
+static void free_plan_device(sfb200_plan* p)
+{
+    free_workspace(p);
+    cudaFree(p->d_exact); cudaFree(p->d_vedges); cudaFree(p->d_lut64); cudaFree(p->d_ck);
+    cudaFree(p->d_lut32); cudaFree(p->d_rowlo); cudaFree(p->d_vwin);
+    cudaFree(p->d_sums); cudaFree(p->d_counts); cudaFree(p->d_aux);
+}
+
+extern "C" int sfb200_plan_destroy(sfb200_plan* p)
+{
+    if (!p) return SFB200_ERR_INVALID_ARG;
+    cudaSetDevice(p->ctx->device);
+    cudaStreamSynchronize(p->ctx->stream);
+    free_plan_device(p);
+    delete p;
+    return SFB200_OK;
+}
+
+template <typename T>
+static cudaError_t upload(T** dst, const T* src, size_t count)
+{
+    cudaError_t e = cudaMalloc((void**)dst, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) return e;
+    if (count) e = cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+}
+
+static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
+{
+    const sfb200_plan_desc& d = p->desc;
+    if (d.geometry != SFB200_GEOM_FLAT && d.geometry != SFB200_GEOM_SPHERE)
+        return set_err(ctx, SFB200_ERR_UNSUPPORTED, "unknown geometry %d", d.geometry);
+    if (d.dim != 2 && d.dim != 3)
+        return set_err(ctx, SFB200_ERR_DIMENSION, "expected spatial/velocity dimension D=2 or D=3 on axis 1; got D=%d", d.dim);
+    p->sphere = d.geometry == SFB200_GEOM_SPHERE;
+    p->D = d.dim;
+    p->W = p->sphere ? 2 : d.dim;
+    if (p->sphere) {
+        if (d.angle_unit != SFB200_ANGLE_DEG && d.angle_unit != SFB200_ANGLE_RAD)
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "unknown angle unit %d", d.angle_unit);
+        if (!(std::isfinite(d.radius) && d.radius > 0.0))
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "sphere radius must be finite and positive");
+    }
+    if (d.precision != SFB200_PREC_FP64 && d.precision != SFB200_PREC_MIXED)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "unknown precision %d", d.precision);
+    if ((d.x_dtype != SFB200_F64 && d.x_dtype != SFB200_F32) || (d.u_dtype != SFB200_F64 && d.u_dtype != SFB200_F32))
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "x_dtype/u_dtype must be F64 or F32");
+    p->mixed = d.precision == SFB200_PREC_MIXED;
+    p->joint = d.joint != 0;
+    if (d.n_ops < 1 || d.n_ops > SFB200_MAX_OPS)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "n_ops must be in 1..%d", SFB200_MAX_OPS);
+    if (p->joint && d.n_ops != 1)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "a joint histogram takes exactly one operator");
+    for (int k = 0; k < d.n_ops; ++k) {
+        const sfb200_operator& o = d.ops[k];
+        if (o.kind < SFB200_OP_PROJECTED || o.kind > SFB200_OP_L1T2C)
+            return set_err(ctx, SFB200_ERR_UNSUPPORTED, "unknown operator kind %d", o.kind);
+        if (o.nl < 0 || o.nt < 0 || o.nf < 0 || o.nl > 16 || o.nt > 16 || o.nf > 16)
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "operator powers must be in 0..16");
+    }
+    int rc = validate_bins(ctx, d.distance, "distance_bins", !p->sphere);
+    if (rc) return rc;
+    if (p->joint && (rc = validate_bins(ctx, d.value, "value_bins", false))) return rc;
+
+    p->nb = d.distance.n_edges - 1;
+    p->nv = p->joint ? d.value.n_edges - 1 : 0;
+    p->nops = d.n_ops;
+    if (p->joint && (long long)p->nb * p->nv > (1ll << 24))
+        return set_err(ctx, SFB200_ERR_UNSUPPORTED, "joint histogram larger than 2^24 cells");
+    if (!p->joint && p->nb > 4096)
+        return set_err(ctx, SFB200_ERR_UNSUPPORTED, "more than 4096 distance bins");
+
+    // operator list -> kernel
+    int codes[SFB200_MAX_OPS];
+    for (int k = 0; k < d.n_ops; ++k) codes[k] = op_code(d.ops[k]);
+    p->opl = -1;
+    if (d.n_ops == 1 && codes[0] == OC_L2) p->opl = OPL_L2;
+    else if (d.n_ops == 1 && codes[0] == OC_L3) p->opl = OPL_L3;
+    else if (d.n_ops == 1 && codes[0] == OC_L1) p->opl = OPL_L1;
+    else if (d.n_ops == 4 && codes[0] == OC_L2 && codes[1] == OC_T2 && codes[2] == OC_L3 && codes[3] == OC_T3)
+        p->opl = OPL_QUAD;
+    p->nops_pad = d.n_ops;
+    if (p->opl < 0) {
+        if (d.n_ops == 1) p->opl = OPL_GEN1;
+        else if (d.n_ops == 2) p->opl = OPL_GEN2;
+        else if (d.n_ops <= 4) { p->opl = OPL_GEN4; p->nops_pad = 4; }
+        else { p->opl = OPL_GEN8; p->nops_pad = 8; }
+    }
+    for (int k = 0; k < SFB200_MAX_OPS; ++k) {
+        if (k < d.n_ops) p->gen.op[k] = d.ops[k];
+        else p->gen.op[k] = sfb200_operator{SFB200_OP_PROJECTED, 0, 0, 0};
+    }
+    p->vorder = op_order(d.ops[0]);
+
+    // distance tables
+    const sfb200_bins& db = d.distance;
+    const bool dlinear = db.kind == SFB200_BINS_LINEAR;
+    if (dlinear) p->dlin = linear_of(db);
+    if (!dlinear) {
+        p->exact_tab.resize(db.n_edges);
+        for (int k = 0; k < db.n_edges; ++k) {
+            const double e = db.edges[k];
+            if (p->sphere) p->exact_tab[k] = (e == 0.0 && std::signbit(e)) ? -4.9406564584124654e-324 : e;
+            else p->exact_tab[k] = (db.kind == SFB200_BINS_SQTABLE) ? e : e * e;
+        }
+        for (int k = 1; k < db.n_edges; ++k)
+            if (p->exact_tab[k] < p->exact_tab[k - 1])
+                return set_err(ctx, SFB200_ERR_INVALID_ARG,
+                               "distance_bins: Euclidean edges must be non-negative (their squares must stay sorted)");
+    }
+    // edge keys of the FP32 path
+    if (p->mixed) {
+        p->ck.resize(db.n_edges);
+        for (int k = 0; k < db.n_edges; ++k) {
+            double r = dlinear ? std::fma((double)k, db.step, db.first) : db.edges[k];
+            if (p->sphere) {
+                p->ck[k] = chord2_of(r, d.radius);
+            } else if (dlinear) {
+                p->ck[k] = r < 0.0 ? -1.0 : r * r;
+            } else {
+                p->ck[k] = p->exact_tab[k];
+            }
+        }
+        if (!geom_lut32(p->ck, p->lg32))
+            return set_err(ctx, SFB200_ERR_UNSUPPORTED,
+                           "distance edges outside the FP32 range of the mixed-precision kernel; use precision=fp64");
+        const double u32 = 0x1p-24, u64 = 0x1p-53;
+        const bool x64 = d.x_dtype == SFB200_F64, u64in = d.u_dtype == SFB200_F64;
+        if (p->sphere) {
+            p->wp.A = 5.0 * u32 * 1.1 + 1e-14;
+            p->wp.Bm = 4.0 * std::sqrt(3.0) * u32 * 1.1;
+            p->wp.Cm = 12.0 * u32 * u32 * 1.1;
+            p->wp.use_bound = 0;
+            p->wp.short_rel = 0.0;
+            p->wp.short_key = 0x1p-12;                 // chord < 1/64
+            p->wp.anti_key = 4.0 * (1.0 - 0x1p-12);    // sin^2(sigma) < 2^-10 near the antipode
+        } else {
+            p->wp.A = (p->D + 3) * u32 * 1.1 + 8.0 * p->D * u64 + (dlinear ? 1e-14 : 0.0);
+            p->wp.Bm = x64 ? 4.0 * std::sqrt((double)p->D) * u32 * 1.1 : 0.0;
+            p->wp.Cm = x64 ? 4.0 * p->D * u32 * u32 * 1.1 : 0.0;
+            p->wp.use_bound = 1;
+            p->wp.short_rel = (x64 || u64in) ? 0x1p-6 : 0.0;
+            p->wp.short_key = 0.0;
+            p->wp.anti_key = INFINITY;
+        }
+    }
+    if (p->joint) {
+        if (d.value.kind == SFB200_BINS_LINEAR) p->vlin = linear_of(d.value);
+        else p->vedges.assign(d.value.edges, d.value.edges + d.value.n_edges);
+    }
+
+    // device allocations
+    cudaError_t e;
+    if (!p->exact_tab.empty() && (e = upload(&p->d_exact, p->exact_tab.data(), p->exact_tab.size())) != cudaSuccess)
+        return cuda_fail(ctx, e, "upload distance table");
+    if (!dlinear && !p->mixed) {
+        std::vector<LutEntry64> lut;
+        build_lut64(p->exact_tab, p->lg64, lut);
+        p->lut64_bytes = (int)(lut.size() * sizeof(LutEntry64));
+        if ((e = upload(&p->d_lut64, lut.data(), lut.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload table");
+    }
+    if (p->mixed) {
+        if ((e = upload(&p->d_ck, p->ck.data(), p->ck.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload keys");
+        if ((e = cudaMalloc(&p->d_lut32, sizeof(LutEntry32) * p->lg32.ncell)) != cudaSuccess)
+            return cuda_fail(ctx, e, "alloc table");
+    }
+    if (!p->vedges.empty() && (e = upload(&p->d_vedges, p->vedges.data(), p->vedges.size())) != cudaSuccess)
+        return cuda_fail(ctx, e, "upload value edges");
+    if (p->joint && p->mixed) {
+        std::vector<double> rowlo(p->nb + 2, 0.0);
+        for (int b = 1; b <= p->nb; ++b) rowlo[b] = std::max(p->ck[b - 1], 0.0);
+        if ((e = upload(&p->d_rowlo, rowlo.data(), rowlo.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload rows");
+        if ((e = cudaMalloc(&p->d_vwin, sizeof(float) * (p->nb + 2))) != cudaSuccess) return cuda_fail(ctx, e, "alloc windows");
+    }
+    p->n_sums = p->joint ? (long long)p->nb * p->nv : (long long)p->nb * p->nops;
+    p->n_counts = p->joint ? (long long)p->nb * p->nv : (long long)p->nb;
+    if ((e = cudaMalloc(&p->d_sums, sizeof(double) * p->n_sums)) != cudaSuccess) return cuda_fail(ctx, e, "alloc sums");
+    if ((e = cudaMalloc(&p->d_counts, sizeof(unsigned long long) * p->n_counts)) != cudaSuccess)
+        return cuda_fail(ctx, e, "alloc counts");
+    if ((e = cudaMalloc(&p->d_aux, sizeof(unsigned long long) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc aux");
+    p->h_sums.resize(p->n_sums);
+    p->h_counts.resize(p->n_counts);
+
+    // the kernel exists for this combination
+    KernelChoice kc = p->joint ? pick_joint(p->sphere, p->D, p->mixed, true, p->opl)
+                               : (p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl) : pick_flat1d(p->D, p->mixed, p->opl));
+    if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this operator on the joint mixed path");
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_plan_create(sfb200_ctx* ctx, const sfb200_plan_desc* desc, sfb200_plan** out)
+{
+    if (!ctx || !desc || !out) return set_err(ctx, SFB200_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+    sfb200_plan* p = new (std::nothrow) sfb200_plan();
+    if (!p) return set_err(ctx, SFB200_ERR_OOM, "out of host memory");
+    p->ctx = ctx;
+    p->desc = *desc;
+    const int rc = plan_build(ctx, p);
+    if (rc != SFB200_OK) {
+        free_plan_device(p);
+        delete p;
+        return rc;
+    }
+    p->desc.distance.edges = nullptr;  // tables were copied
+    p->desc.value.edges = nullptr;
+    *out = p;
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_plan_output_sizes(const sfb200_plan* p, int64_t* n_sums, int64_t* n_counts)
+{
+    if (!p) return SFB200_ERR_INVALID_ARG;
+    if (n_sums) *n_sums = p->n_sums;
+    if (n_counts) *n_counts = p->n_counts;
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_plan_set_launch(sfb200_plan* p, int tile, int threads, int blocks_per_sm)
+{
+    if (!p) return SFB200_ERR_INVALID_ARG;
+    sfb200_ctx* ctx = p->ctx;
+    if (tile != 0 && tile != 64 && tile != 128 && tile != 256 && tile != 512)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile must be 0, 64, 128, 256 or 512");
+    if (threads != 0 && threads != tile)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "threads per block equal the tile size");
+    if (blocks_per_sm < 0 || blocks_per_sm > 32)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "blocks_per_sm must be in 0..32");
+    p->tile_ovr = tile;
+    p->threads_ovr = threads;
+    p->bps_ovr = blocks_per_sm;
+    return SFB200_OK;
+}
+
+// ------------------------------------------------------------------------------- run
+
+static int ensure_workspace(sfb200_plan* p, long long n)
+{
+    sfb200_ctx* ctx = p->ctx;
+    if (n <= p->cap) return SFB200_OK;
+    CK(cudaStreamSynchronize(ctx->stream));
+    free_workspace(p);
+    const long long cap = std::max<long long>(n, 1024);
+    const int nx64 = p->sphere ? 8 : p->D;
+    const int nxf = p->sphere ? (p->D == 3 ? 10 : 9) : p->D;
+    CK(cudaMalloc(&p->d_rawx, sizeof(double) * p->W * cap));
+    CK(cudaMalloc(&p->d_rawu, sizeof(double) * p->D * cap));
+    CK(cudaMalloc(&p->d_X64, sizeof(double) * nx64 * cap));
+    CK(cudaMalloc(&p->d_U64, sizeof(double) * p->D * cap));
+    if (p->mixed) {
+        CK(cudaMalloc(&p->d_XF, sizeof(float) * nxf * cap));
+        if (!p->sphere) CK(cudaMalloc(&p->d_UF, sizeof(float) * p->D * cap));
+    }
+    p->cap = cap;
+    return SFB200_OK;
+}
+
+template <typename TX, typename TU>
+static void launch_pack(sfb200_plan* p, const void* x, const void* u, int n, cudaStream_t s)
+{
+    const int tb = 256, nblk = (n + tb - 1) / tb;
+    if (p->sphere)
+        k_pack_sphere<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->desc.angle_unit,
+                                                  p->d_X64, p->d_U64, p->mixed ? p->d_XF : nullptr, p->d_aux + 1);
+    else
+        k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->d_X64, p->d_U64,
+                                                p->mixed ? p->d_XF : nullptr, p->mixed ? p->d_UF : nullptr,
+                                                p->d_aux + 1);
+}
+
+static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_hist)
+{
+    const int NW = T / 32, NBP = p->nb + 2, NV = p->nops_pad;
+    if (p->joint) {
+        const long long ncell = (long long)p->nb * p->nv;
+        if (!p->mixed) {
+            const int nx = p->sphere ? 8 : p->D;
+            return (size_t)(nx + p->D) * T * 8 + (smem_hist ? (size_t)ncell * 12 : 0);
+        }
+        const int nx = p->sphere ? (p->D == 3 ? 10 : 9) : 2 * p->D;
+        return (size_t)lut_bytes + (size_t)nx * T * 4 + (size_t)ncell * 8 + (size_t)(p->nb + 2) * 4;
+    }
+    if (!p->mixed) {
+        const int nx = p->sphere ? 8 : p->D;
+        return (size_t)lut_bytes + (size_t)(nx + p->D) * T * 8 + (size_t)NW * NV * NBP * 8 + (size_t)NW * NBP * 8;
+    }
+    const int nx = p->sphere ? (p->D == 3 ? 10 : 9) : 2 * p->D;
+    return (size_t)lut_bytes + (size_t)nx * T * 4 + (size_t)NW * NV * NBP * 8 + (size_t)NW * NBP * 4;
+}
+
+static long long tile_pairs(long long n, int T)
+{
+    const long long nt = (n + T - 1) / T;
+    return nt * (nt + 1) / 2;
+}
+
+extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t n, uint32_t flags,
+                          double* sums, uint64_t* counts, void* stream)
+{
+    if (!p) return SFB200_ERR_INVALID_ARG;
+    sfb200_ctx* ctx = p->ctx;
+    if (n < 0) return set_err(ctx, SFB200_ERR_INVALID_ARG, "negative point count");
+    if (n > (1ll << 31) - 1024) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "more than 2^31 points");
+    if (!sums || !counts) return set_err(ctx, SFB200_ERR_INVALID_ARG, "sums/counts pointer is NULL");
+    if (n > 0 && (!x || !u)) return set_err(ctx, SFB200_ERR_INVALID_ARG, "x/u pointer is NULL");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    const bool dev_in = flags & SFB200_RUN_DEVICE_INPUT;
+    const bool dev_out = flags & SFB200_RUN_DEVICE_OUTPUT;
+    const bool accumulate = flags & SFB200_RUN_ACCUMULATE;
+    int launches = 0;
+
+    CK(cudaMemsetAsync(p->d_sums, 0, sizeof(double) * p->n_sums, s));
+    CK(cudaMemsetAsync(p->d_counts, 0, sizeof(unsigned long long) * p->n_counts, s));
+    CK(cudaMemsetAsync(p->d_aux, 0, sizeof(unsigned long long) * 4, s));
+    p->stats = sfb200_stats{};
+    p->stats.pairs = n * (n - 1) / 2;
+    p->stats_pending = false;
+
+    if (n >= 2) {
+        int rc = ensure_workspace(p, n);
+        if (rc) return rc;
+        const size_t xs = p->desc.x_dtype == SFB200_F64 ? 8 : 4;
+        const size_t us = p->desc.u_dtype == SFB200_F64 ? 8 : 4;
+        const void* xin = x;
+        const void* uin = u;
+        if (!dev_in) {
+            CK(cudaMemcpyAsync(p->d_rawx, x, xs * p->W * n, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(p->d_rawu, u, us * p->D * n, cudaMemcpyHostToDevice, s));
+            xin = p->d_rawx;
+            uin = p->d_rawu;
+        }
+        const bool x64 = xs == 8, u64 = us == 8;
+        if (x64 && u64) launch_pack<double, double>(p, xin, uin, (int)n, s);
+        else if (x64) launch_pack<double, float>(p, xin, uin, (int)n, s);
+        else if (u64) launch_pack<float, double>(p, xin, uin, (int)n, s);
+        else launch_pack<float, float>(p, xin, uin, (int)n, s);
+        ++launches;
+        CK(cudaGetLastError());
+        if (p->mixed) {
+            k_build_lut32<<<(p->lg32.ncell + 127) / 128, 128, 0, s>>>(p->d_ck, (int)p->ck.size(), p->wp, p->lg32,
+                                                                    p->d_aux + 1, p->d_lut32);
+            ++launches;
+            CK(cudaGetLastError());
+            if (p->joint) {
+                ValueWindowParams vw;
+                vw.nd = p->nb;
+                vw.D = p->D;
+                vw.order = p->vorder;
+                vw.sphere = p->sphere;
+                vw.x_f64 = x64;
+                vw.u_f64 = u64;
+                vw.inv_step = p->desc.value.kind == SFB200_BINS_LINEAR ? p->vlin.inv_step : 0.0;
+                vw.neg_f_inv = p->desc.value.kind == SFB200_BINS_LINEAR ? p->vlin.neg_f_inv : 0.0;
+                k_value_windows<<<1, 128, 0, s>>>(p->d_rowlo, vw, p->d_aux + 1, p->d_vwin);
+                ++launches;
+                CK(cudaGetLastError());
+            }
+        }
+
+        // launch configuration
+        const bool dlinear = p->desc.distance.kind == SFB200_BINS_LINEAR;
+        int lut_bytes = 0;
+        if (p->mixed) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
+        else if (!dlinear && !p->joint) lut_bytes = p->lut64_bytes;
+        int T;
+        bool smem_hist = true;
+        KernelChoice kc;
+        size_t smem;
+        int dev_smem_max = 0;
+        CK(cudaDeviceGetAttribute(&dev_smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+        if (p->joint) {
+            T = p->tile_ovr ? p->tile_ovr : (n >= 32768 ? 512 : (n >= 4096 ? 256 : 64));
+            smem = smem_bytes(p, T, lut_bytes, true);
+            if (smem > (size_t)dev_smem_max) {
+                if (p->mixed)
+                    return set_err(ctx, SFB200_ERR_UNSUPPORTED,
+                                   "joint histogram of %d x %d cells does not fit shared memory on the mixed path; use fp64",
+                                   p->nb, p->nv);
+                smem_hist = false;
+                smem = smem_bytes(p, T, lut_bytes, false);
+            }
+            kc = pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->opl);
+        } else {
+            kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl) : pick_flat1d(p->D, p->mixed, p->opl);
+            if (p->tile_ovr) {
+                T = p->tile_ovr;
+            } else {
+                T = 64;
+                for (int cand : {256, 128}) {
+                    if (tile_pairs(n, cand) >= 4ll * ctx->nsm) { T = cand; break; }
+                }
+            }
+            if (T > kc.max_threads) T = kc.max_threads;
+            smem = smem_bytes(p, T, lut_bytes, true);
+            while (smem > (size_t)dev_smem_max && T > 64) {
+                T /= 2;
+                smem = smem_bytes(p, T, lut_bytes, true);
+            }
+            if (smem > (size_t)dev_smem_max)
+                return set_err(ctx, SFB200_ERR_UNSUPPORTED, "%d bins x %d operators do not fit shared memory",
+                               p->nb, p->nops);
+        }
+        if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this plan");
+        CK(cudaFuncSetAttribute(kc.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int occ = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc.fn, T, smem));
+        if (occ < 1) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "kernel does not fit on an SM (%zu bytes shared)", smem);
+        if (p->bps_ovr) occ = std::min(occ, p->bps_ovr);
+        const long long ntp = tile_pairs(n, T);
+        const long long grid = std::min<long long>(ntp, (long long)ctx->nsm * occ);
+
+        PairArgs a{};
+        a.n = (int)n;
+        a.ntiles = (int)((n + T - 1) / T);
+        a.ntp = ntp;
+        a.X64 = p->d_X64;
+        a.U64 = p->d_U64;
+        a.XF = p->d_XF;
+        a.UF = p->d_UF;
+        a.lut = p->mixed ? (const void*)p->d_lut32 : (const void*)p->d_lut64;
+        a.lg = p->mixed ? p->lg32 : p->lg64;
+        a.lut_bytes = lut_bytes;
+        a.edges = p->d_exact;
+        a.n_edges = p->desc.distance.n_edges;
+        a.dist_linear = dlinear;
+        a.dlin = p->dlin;
+        a.radius = p->desc.radius;
+        a.nb = p->nb;
+        a.nops = p->nops;
+        a.nv = p->nv;
+        a.val_linear = p->joint && p->desc.value.kind == SFB200_BINS_LINEAR;
+        a.vlin = p->vlin;
+        a.vedges = p->d_vedges;
+        a.n_vedges = p->joint ? p->desc.value.n_edges : 0;
+        a.vwin = p->d_vwin;
+        a.gen = p->gen;
+        a.g_sums = p->d_sums;
+        a.g_counts = p->d_counts;
+        a.g_stats = p->d_aux;
+        void* args[] = {&a};
+        CK(cudaEventRecord(ctx->ev0, s));
+        CK(cudaLaunchKernel(kc.fn, dim3((unsigned)grid), dim3(T), args, smem, s));
+        CK(cudaEventRecord(ctx->ev1, s));
+        ++launches;
+        CK(cudaGetLastError());
+        p->stats.tile = T;
+        p->stats.threads = T;
+        p->stats.blocks = (int)grid;
+        p->stats_pending = true;
+    }
+
+    if (dev_out) {
+        const long long m = std::max(p->n_sums, p->n_counts);
+        if (m > 0) {
+            k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(p->d_sums, p->d_counts, p->n_sums, p->n_counts,
+                                                                 sums, (unsigned long long*)counts, accumulate);
+            ++launches;
+            CK(cudaGetLastError());
+        }
+        p->stats.kernel_launches = launches;
+        return SFB200_OK;
+    }
+    CK(cudaMemcpyAsync(p->h_sums.data(), p->d_sums, sizeof(double) * p->n_sums, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(p->h_counts.data(), p->d_counts, sizeof(unsigned long long) * p->n_counts,
+                       cudaMemcpyDeviceToHost, s));
+    unsigned long long aux0 = 0;
+    CK(cudaMemcpyAsync(&aux0, p->d_aux, sizeof(aux0), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (long long k = 0; k < p->n_sums; ++k) sums[k] = (accumulate ? sums[k] : 0.0) + p->h_sums[k];
+    for (long long k = 0; k < p->n_counts; ++k) counts[k] = (accumulate ? counts[k] : 0ull) + p->h_counts[k];
+    p->stats.rechecked = (int64_t)aux0;
+    p->stats.kernel_launches = launches;
+    if (p->stats_pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) p->stats.kernel_ms = ms;
+        p->stats_pending = false;
+    }
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_plan_last_stats(const sfb200_plan* pc, sfb200_stats* out)
+{
+    if (!pc || !out) return SFB200_ERR_INVALID_ARG;
+    sfb200_plan* p = const_cast<sfb200_plan*>(pc);
+    sfb200_ctx* ctx = p->ctx;
+    if (p->stats_pending) {
+        CK(cudaEventSynchronize(ctx->ev1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        p->stats.kernel_ms = ms;
+        unsigned long long aux0 = 0;
+        CK(cudaMemcpy(&aux0, p->d_aux, sizeof(aux0), cudaMemcpyDeviceToHost));
+        p->stats.rechecked = (int64_t)aux0;
+        p->stats_pending = false;
+    }
+    *out = p->stats;
+    return SFB200_OK;
+}

@@ -1,0 +1,36 @@
+// sfb200_internal.h -- declarations shared by the API translation unit and the kernel
+// instantiation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sfb200_common.cuh"
+
+namespace sfb {
+
+struct PairArgs;
+
+// Operator lists with a dedicated (compile-time fused) kernel; anything else runs the generic
+// kernel with the operator count padded to 1, 2, 4 or 8.
+enum OpListId : int {
+    OPL_L2 = 0,        // {L2SF}
+    OPL_L3 = 1,        // {L3SF}
+    OPL_L1 = 2,        // {ProjectedStructureFunctionType{1,0}} (du_L; joint value axis)
+    OPL_QUAD = 3,      // {L2SF, T2SF, L3SF, T3SF}
+    OPL_GEN1 = 4,
+    OPL_GEN2 = 5,
+    OPL_GEN4 = 6,
+    OPL_GEN8 = 7
+};
+
+struct KernelChoice {
+    const void* fn;   // kernel entry
+    int max_threads;  // launch bound
+};
+
+// Kernel lookup: returns nullptr fn for an unsupported combination.
+KernelChoice pick_flat1d(int D, bool mixed, int opl);
+KernelChoice pick_sphere1d(int D, bool mixed, int opl);
+KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, int opl);
+
+}  // namespace sfb

@@ -1,0 +1,304 @@
+// sfb200_joint.cuh -- joint (distance x value) histogram kernels, the StructureFunction2DSumsAndCounts
+// path (src/Calculations/serial_2d.jl:49-85 Euclidean, 260-303 non-Euclidean).
+//
+// A pair contributes to cell (dbin, vbin) when both bins are in range; the operator value decides
+// vbin, so in FP64 it is computed in the reference's exact operation order (sfb200_exact.cuh).
+// The histogram (n_dist x n_val cells, column-major like the reference's matrices) lives in shared
+// memory per block when it fits and is updated with shared-memory atomics (cells are many and
+// sparsely hit, so warp aggregation buys little); otherwise the kernel adds straight into the global
+// FP64 / uint64 accumulators.
+//
+// The FP32 kernel accumulates each cell as count and the FP32 sum of (v - c_vbin), the value's
+// offset from its value-bin centre: a cell's values are within half a bin width of c_vbin, so the
+// FP32 running sum carries the small residuals only, and the merge rebuilds
+// sum = count * c_vbin + residual in FP64. Pairs whose value (or distance) lies within the FP32
+// error bound of an edge are recomputed in FP64 with the reference arithmetic.
+#pragma once
+
+#include "sfb200_kernels.cuh"
+
+namespace sfb {
+
+// ------------------------------------------------------------------------------------ FP64
+template <bool SPHERE, int D, bool SMEM>
+__global__ void __launch_bounds__(512) k_joint_fp64(const PairArgs a)
+{
+    constexpr int NX = SPHERE ? 8 : D;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x;
+    const int n = a.n;
+    const int nd = a.nb, nv = a.nv;
+    const int ncell = nd * nv;
+    double* sx = reinterpret_cast<double*>(smem);  // NX * T
+    double* su = sx + NX * T;                       // D * T
+    double* hs = su + D * T;                        // ncell (SMEM)
+    unsigned* hc = reinterpret_cast<unsigned*>(hs + (SMEM ? ncell : 0));
+    const LutEntry64* lut = static_cast<const LutEntry64*>(a.lut);
+    const sfb200_operator op = a.gen.op[0];
+
+    if constexpr (SMEM) {
+        for (int k = threadIdx.x; k < ncell; k += T) { hs[k] = 0.0; hc[k] = 0u; }
+    }
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + threadIdx.x;
+        const bool iv = i < n;
+        double xa[NX], ua[D];
+#pragma unroll
+        for (int c = 0; c < NX; ++c) xa[c] = iv ? a.X64[(size_t)c * n + i] : 0.0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) ua[d] = iv ? a.U64[(size_t)d * n + i] : 0.0;
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+#pragma unroll
+            for (int c = 0; c < NX; ++c) sx[c * T + threadIdx.x] = a.X64[(size_t)c * n + j0 + threadIdx.x];
+#pragma unroll
+            for (int d = 0; d < D; ++d) su[d * T + threadIdx.x] = a.U64[(size_t)d * n + j0 + threadIdx.x];
+        }
+        __syncthreads();
+        if (!iv) continue;
+        const int jbeg = (ti == tj) ? (int)threadIdx.x + 1 : 0;
+        for (int jj = jbeg; jj < jn; ++jj) {
+            double ub[D], du[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) ub[d] = su[d * T + jj];
+            int db;
+            double v;
+            if constexpr (!SPHERE) {
+                double dx[D];
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    dx[d] = SFB_SUB(sx[d * T + jj], xa[d]);
+                    du[d] = SFB_SUB(ub[d], ua[d]);
+                }
+                const double r2 = x_dot<D>(dx, dx);
+                if (a.dist_linear) db = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
+                else db = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+                if (db < 1 || db > nd) continue;
+                v = x_sf_raw<D>(op, du, dx, r2);
+            } else {
+                SphPoint A, B;
+                A.p[0] = xa[0]; A.p[1] = xa[1]; A.p[2] = xa[2]; A.E[0] = xa[3]; A.E[1] = xa[4];
+                A.N[0] = xa[5]; A.N[1] = xa[6]; A.N[2] = xa[7];
+                B.p[0] = sx[0 * T + jj]; B.p[1] = sx[1 * T + jj]; B.p[2] = sx[2 * T + jj];
+                B.E[0] = sx[3 * T + jj]; B.E[1] = sx[4 * T + jj];
+                B.N[0] = sx[5 * T + jj]; B.N[1] = sx[6 * T + jj]; B.N[2] = sx[7 * T + jj];
+                double r, tA[2], tB[2];
+                const bool ok = x_sphere_frame(A, B, a.radius, r, tA, tB);
+                if (a.dist_linear) db = linear_bin(a.dlin, r);
+                else db = (r != r) ? a.n_edges : lut64_bin(lut, a, r);
+                if (!ok || db < 1 || db > nd) continue;
+                x_sphere_delta<D>(tA, tB, ua, ub, du);
+                v = x_sphere_value<D>(op, du);
+            }
+            const int vb = value_exact_bin(a, v);
+            if (vb < 1 || vb > nv) continue;
+            const int cell = (db - 1) + nd * (vb - 1);
+            if constexpr (SMEM) {
+                atomicAdd(&hs[cell], v);
+                atomicAdd(&hc[cell], 1u);
+            } else {
+                atomicAdd(&a.g_sums[cell], v);
+                atomicAdd(&a.g_counts[cell], 1ull);
+            }
+        }
+    }
+    if constexpr (SMEM) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < ncell; k += T) {
+            if (hc[k]) {
+                atomicAdd(&a.g_sums[k], hs[k]);
+                atomicAdd(&a.g_counts[k], (unsigned long long)hc[k]);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------ mixed
+// Value-bin centre (FP32) of value bin vb in [1, nv].
+__device__ __forceinline__ float value_center(const PairArgs& a, int vb)
+{
+    if (a.val_linear) return (float)(a.vlin.first + ((double)vb - 0.5) * a.vlin.step);
+    return (float)(0.5 * (a.vedges[vb - 1] + a.vedges[vb]));
+}
+
+template <bool SPHERE, int D, class OPS>
+__global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
+{
+    constexpr int NX = SPHERE ? ((D == 3) ? 10 : 9) : D;
+    constexpr int NV = 1;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const int n = a.n;
+    const int nd = a.nb, nv = a.nv;
+    const int ncell = nd * nv;
+    LutEntry32* lut = reinterpret_cast<LutEntry32*>(smem);
+    float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);  // NX * T
+    float* su = sx + NX * T;                                    // D * T (flat)
+    float* hres = su + (SPHERE ? 0 : D * T);                    // ncell
+    unsigned* hc = reinterpret_cast<unsigned*>(hres + ncell);   // ncell
+    float* swin = reinterpret_cast<float*>(hc + ncell);         // nd + 2
+    __shared__ unsigned long long s_recheck;
+
+    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry32); k += T)
+        lut[k] = static_cast<const LutEntry32*>(a.lut)[k];
+    for (int k = threadIdx.x; k < ncell; k += T) { hres[k] = 0.f; hc[k] = 0u; }
+    for (int k = threadIdx.x; k < nd + 2; k += T) swin[k] = a.vwin[k];
+    if (threadIdx.x == 0) s_recheck = 0ull;
+    unsigned long long my_recheck = 0;
+    const float vinv = (float)a.vlin.inv_step;
+    const float vnegf = (float)a.vlin.neg_f_inv;
+    const float tmax = (float)(a.vlin.n - 1);
+
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + threadIdx.x;
+        const bool iv = i < n;
+        float xa[NX], ua[D];
+#pragma unroll
+        for (int c = 0; c < NX; ++c) xa[c] = iv ? a.XF[(size_t)c * n + i] : 0.f;
+        if constexpr (!SPHERE) {
+#pragma unroll
+            for (int d = 0; d < D; ++d) ua[d] = iv ? a.UF[(size_t)d * n + i] : 0.f;
+        }
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+#pragma unroll
+            for (int c = 0; c < NX; ++c) sx[c * T + threadIdx.x] = a.XF[(size_t)c * n + j0 + threadIdx.x];
+            if constexpr (!SPHERE) {
+#pragma unroll
+                for (int d = 0; d < D; ++d) su[d * T + threadIdx.x] = a.UF[(size_t)d * n + j0 + threadIdx.x];
+            }
+        }
+        __syncthreads();
+        const bool diag = ti == tj;
+        for (int jj = 0; jj < jn; ++jj) {
+            const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+            float key, L, Tt, Q;
+            if constexpr (!SPHERE) {
+                float dx[D], du[D];
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    dx[d] = sx[d * T + jj] - xa[d];
+                    du[d] = su[d * T + jj] - ua[d];
+                }
+                const float h2 = fmaf(dx[1], dx[1], dx[0] * dx[0]);
+                float r2 = h2;
+                if constexpr (D == 3) r2 = fmaf(dx[2], dx[2], h2);
+                key = r2;
+                const float rs = rsqrtf(r2);
+                float pp = dx[0] * du[0];
+#pragma unroll
+                for (int d = 1; d < D; ++d) pp = fmaf(dx[d], du[d], pp);
+                L = pp * rs;
+                const float t = fmaf(du[1], dx[0], -du[0] * dx[1]);
+                Tt = (D == 2) ? t * rs : t * rsqrtf(h2);
+                Q = du[0] * du[0];
+#pragma unroll
+                for (int d = 1; d < D; ++d) Q = fmaf(du[d], du[d], Q);
+            } else {
+                const float d0 = sx[0 * T + jj] - xa[0];
+                const float d1 = sx[1 * T + jj] - xa[1];
+                const float d2 = sx[2 * T + jj] - xa[2];
+                const float ch2 = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+                key = ch2;
+                const float inv_s = rsqrtf(ch2 * fmaf(-0.25f, ch2, 1.0f));
+                L = fmaf(d2, sx[5 * T + jj] - xa[5], fmaf(d1, sx[4 * T + jj] - xa[4], d0 * (sx[3 * T + jj] - xa[3]))) * inv_s;
+                Tt = fmaf(d2, sx[8 * T + jj] - xa[8], fmaf(d1, sx[7 * T + jj] - xa[7], d0 * (sx[6 * T + jj] - xa[6]))) * inv_s;
+                Q = fmaf(Tt, Tt, L * L);
+                if constexpr (D == 3) {
+                    const float dw = sx[9 * T + jj] - xa[9];
+                    Q = fmaf(dw, dw, Q);
+                }
+            }
+            const LutEntry32 e = lut[lut_cell32(key, a.lg)];
+            int db = e.base + (key > e.hi ? (e.mult & 0xffff) : 0);
+            bool slow = (e.mult & LUT_FLAG_SLOW) || (key >= e.lo && key <= e.hi);
+            float v[NV];
+            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
+            float val = v[0];
+            int vb;
+            {
+                float t;
+                if (a.val_linear) {
+                    t = fmaf(val, vinv, vnegf);
+                } else {
+                    t = 0.f;
+                }
+                if (a.val_linear) {
+                    const float fl = floorf(t);
+                    const float fr = t - fl;
+                    const float wt = swin[min(max(db, 0), nd + 1)] + fabsf(t) * 2.4e-7f;
+                    vb = (t <= 0.f) ? 0 : ((t > tmax) ? a.vlin.n : (int)fl + 1);
+                    slow = slow || fr < wt || fr > 1.f - wt || fabsf(t) < wt || fabsf(t - tmax) < wt || !(t == t);
+                } else {
+                    slow = true;  // vector value edges: exact FP64 search
+                    vb = 0;
+                }
+            }
+            slow = slow && valid;
+            bool ok = true;
+            if (__any_sync(FULL, slow)) {
+                if (slow) {
+                    const int j = j0 + jj;
+                    double du64[D];
+                    double v64;
+                    if constexpr (!SPHERE) {
+                        double dx64[D];
+#pragma unroll
+                        for (int d = 0; d < D; ++d) {
+                            dx64[d] = SFB_SUB(a.X64[(size_t)d * n + j], a.X64[(size_t)d * n + i]);
+                            du64[d] = SFB_SUB(a.U64[(size_t)d * n + j], a.U64[(size_t)d * n + i]);
+                        }
+                        const double r264 = x_dot<D>(dx64, dx64);
+                        db = flat_exact_bin(a, r264);
+                        v64 = x_sf_raw<D>(a.gen.op[0], du64, dx64, r264);
+                    } else {
+                        SphPoint A, B;
+                        load_sph64(a.X64, n, i, A);
+                        load_sph64(a.X64, n, j, B);
+                        double r, tA[2], tB[2], uA[D], uB[D];
+                        ok = x_sphere_frame(A, B, a.radius, r, tA, tB);
+                        db = sphere_exact_bin(a, r);
+#pragma unroll
+                        for (int d = 0; d < D; ++d) {
+                            uA[d] = a.U64[(size_t)d * n + i];
+                            uB[d] = a.U64[(size_t)d * n + j];
+                        }
+                        x_sphere_delta<D>(tA, tB, uA, uB, du64);
+                        v64 = x_sphere_value<D>(a.gen.op[0], du64);
+                    }
+                    vb = value_exact_bin(a, v64);
+                    val = (float)v64;
+                }
+                const unsigned sb = __ballot_sync(FULL, slow);
+                if (lane == 0) my_recheck += __popc(sb);
+            }
+            if (valid && ok && db >= 1 && db <= nd && vb >= 1 && vb <= nv) {
+                const int cell = (db - 1) + nd * (vb - 1);
+                atomicAdd(&hres[cell], val - value_center(a, vb));
+                atomicAdd(&hc[cell], 1u);
+            }
+        }
+    }
+    if (lane == 0 && my_recheck) atomicAdd(&s_recheck, my_recheck);
+    __syncthreads();
+    for (int k = threadIdx.x; k < ncell; k += T) {
+        if (hc[k]) {
+            const int vb = k / nd + 1;
+            const double s = (double)hc[k] * (double)value_center(a, vb) + (double)hres[k];
+            atomicAdd(&a.g_sums[k], s);
+            atomicAdd(&a.g_counts[k], (unsigned long long)hc[k]);
+        }
+    }
+    if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
+}
+
+}  // namespace sfb

@@ -1,0 +1,610 @@
+// sfb200_kernels.cuh -- the pair kernels.
+//
+// Layout in HBM (per run, built by the pack kernels from the caller's column-major arrays):
+//   FP64 SoA  X64[c * n + i]: flat: D coordinates; sphere: p(3), E(2), N(3) of the local basis.
+//             U64[c * n + i]: D velocity components.
+//   FP32 SoA  XF[c * n + i]:  flat: D coordinates; sphere: p(3), U(3), W(3)[, up] (ambient tangent
+//             velocity U = u_e E + u_n N and its quarter turn W = u_n E - u_e N).
+//             UF[c * n + i]:  flat: D velocity components.
+// Every point set is tiny next to HBM (N = 200k sphere points: 8.8 MB FP64 + 8 MB FP32) and stays
+// L2-resident; the kernels are FP32/FP64 issue-bound, not bandwidth-bound.
+//
+// Schedule: the N points are cut into tiles of T = blockDim.x points. A block owns an upper-
+// triangle tile pair (ti <= tj) at a time (persistent grid, stride gridDim.x): thread t holds point
+// ti*T + t in registers, the J tile is staged in shared memory and broadcast, so each thread walks
+// the T pairs of its row. Diagonal tiles keep j > i only.
+//
+// Accumulation: each warp owns a private histogram in shared memory (rows 0..nb+1; rows 0 and nb+1
+// collect out-of-range pairs and are dropped). Per pair step the warp groups its 32 lanes by bin
+// with __match_any_sync, reduces each group's values with a shuffle tree, and the group leader adds
+// the sum and the group size into the warp's histogram. Leaders of one step hold distinct bins and a
+// histogram belongs to one warp, so the update needs no atomics. FP32 kernels keep each bin as an
+// FP32 (hi, lo) two-sum pair; at the end every block merges its warps' histograms in FP64 and adds
+// them to the global FP64 sums / uint64 counts with one atomic per bin.
+#pragma once
+
+#include "sfb200_common.cuh"
+#include "sfb200_exact.cuh"
+#include "sfb200_ops.cuh"
+
+namespace sfb {
+
+struct PairArgs {
+    int n;             // points
+    int ntiles;        // ceil(n / T)
+    long long ntp;     // ntiles (ntiles + 1) / 2
+    const double* X64; // FP64 SoA positions / sphere basis
+    const double* U64; // FP64 SoA velocities
+    const float* XF;   // FP32 SoA (mixed)
+    const float* UF;
+    const void* lut;   // LutEntry64 (FP64 kernels) or LutEntry32 (mixed)
+    LutGeom lg;
+    int lut_bytes;     // bytes of the table copied to shared memory (0: no table)
+    const double* edges; // exact edge table in key space: flat squared edges, sphere raw edges
+    int n_edges;
+    int dist_linear;   // 1: LinearBinEdges search on r (flat: sqrt(r^2))
+    LinearParams dlin;
+    double radius;     // sphere
+    int nb;            // distance bins
+    int nops;          // operators (1D)
+    // joint
+    int nv;            // value bins
+    int val_linear;
+    LinearParams vlin;
+    const double* vedges;
+    int n_vedges;
+    const float* vwin; // per distance row: half-width of the value ambiguity window (mixed), value units
+    GenOps gen;
+    double* g_sums;
+    unsigned long long* g_counts;
+    unsigned long long* g_stats; // [0] rechecked pairs
+};
+
+// Exact FP64 bin of a flat pair from r^2 (src/BinEdges.jl:515-517).
+__device__ __forceinline__ int flat_exact_bin(const PairArgs& a, double r2)
+{
+    if (r2 != r2) return a.n_edges;
+    if (a.dist_linear) return linear_bin(a.dlin, SFB_SQRT(r2));
+    return count_below(a.edges, a.n_edges, r2);
+}
+
+// Exact FP64 bin of a sphere pair from r (digitize(r, edges), src/Calculations/serial.jl:258).
+__device__ __forceinline__ int sphere_exact_bin(const PairArgs& a, double r)
+{
+    if (r != r) return a.n_edges;
+    if (a.dist_linear) return linear_bin(a.dlin, r);
+    return count_below(a.edges, a.n_edges, r);
+}
+
+__device__ __forceinline__ int lut64_bin(const LutEntry64* lut, const PairArgs& a, double key)
+{
+    const LutEntry64 e = lut[lut_cell64(key, a.lg)];
+    if (e.mult & LUT_FLAG_SLOW) return count_below(a.edges, a.n_edges, key);
+    return e.base + (key > e.e ? e.mult : 0);
+}
+
+// Value bin of the joint histogram (digitize(val, value_bins)), exact FP64.
+__device__ __forceinline__ int value_exact_bin(const PairArgs& a, double v)
+{
+    if (a.val_linear) return linear_bin(a.vlin, v);
+    // searchsortedfirst with isless: NaN sorts above every edge.
+    if (v != v) return a.n_vedges;
+    int lo = 0, hi = a.n_vedges;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const double e = a.vedges[mid];
+        const bool less = e < v || (e == v && e == 0.0 && signbit(e) && !signbit(v));
+        if (less) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// ================================================================================================
+// Flat (Euclidean) 1D, FP64
+// ================================================================================================
+template <int D, class OPS>
+__global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
+{
+    constexpr int NV = OPS::n;
+    using Needs = ListNeeds<OPS>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x, NW = T >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int NBP = a.nb + 2;
+    const int n = a.n;
+    LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
+    double* sx = reinterpret_cast<double*>(smem + a.lut_bytes);
+    double* su = sx + D * T;
+    double* hs = su + D * T;
+    unsigned long long* hc = reinterpret_cast<unsigned long long*>(hs + NW * NV * NBP);
+
+    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
+        lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
+    for (int k = threadIdx.x; k < NW * NV * NBP; k += T) hs[k] = 0.0;
+    for (int k = threadIdx.x; k < NW * NBP; k += T) hc[k] = 0ull;
+    double* whs = hs + warp * NV * NBP;
+    unsigned long long* whc = hc + warp * NBP;
+
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + threadIdx.x;
+        const bool iv = i < n;
+        double xi[D], ui[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            xi[d] = iv ? a.X64[(size_t)d * n + i] : 0.0;
+            ui[d] = iv ? a.U64[(size_t)d * n + i] : 0.0;
+        }
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                sx[d * T + threadIdx.x] = a.X64[(size_t)d * n + j0 + threadIdx.x];
+                su[d * T + threadIdx.x] = a.U64[(size_t)d * n + j0 + threadIdx.x];
+            }
+        }
+        __syncthreads();
+        const bool diag = ti == tj;
+        for (int jj = 0; jj < jn; ++jj) {
+            const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+            double dx[D], du[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                dx[d] = SFB_SUB(sx[d * T + jj], xi[d]);
+                du[d] = su[d * T + jj] - ui[d];
+            }
+            // r^2 exactly as the reference: left-to-right, no contraction (decides the bin)
+            double h2 = SFB_ADD(SFB_MUL(dx[0], dx[0]), SFB_MUL(dx[1], dx[1]));
+            double r2 = h2;
+            if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
+            int bin;
+            if (a.dist_linear) bin = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
+            else bin = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+            const int key = valid ? bin : a.nb + 1;
+
+            double L = 0.0, Tt = 0.0, Q = 0.0;
+            const double rs = rsqrt(r2);
+            if constexpr (Needs::L) {
+                double pp = dx[0] * du[0];
+#pragma unroll
+                for (int d = 1; d < D; ++d) pp = fma(dx[d], du[d], pp);
+                L = pp * rs;
+            }
+            if constexpr (Needs::T) {
+                const double t = fma(du[1], dx[0], -du[0] * dx[1]);
+                Tt = (D == 2) ? t * rs : t * rsqrt(h2);
+            }
+            if constexpr (Needs::Q) {
+                Q = du[0] * du[0];
+#pragma unroll
+                for (int d = 1; d < D; ++d) Q = fma(du[d], du[d], Q);
+            }
+            double v[NV];
+            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
+
+            const unsigned peers = __match_any_sync(FULL, key);
+            reduce_peers<NV>(peers, lane, v);
+            if (lane == __ffs(peers) - 1) {
+                whc[key] += (unsigned long long)__popc(peers);
+#pragma unroll
+                for (int o = 0; o < NV; ++o) whs[o * NBP + key] += v[o];
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // only the caller's operators are written out (NV may include padding of the generic kernels)
+    for (int k = threadIdx.x; k < min(NV, a.nops) * a.nb; k += T) {
+        const int o = k / a.nb, b = k - o * a.nb + 1;
+        double s = 0.0;
+        for (int w = 0; w < NW; ++w) s += hs[(w * NV + o) * NBP + b];
+        if (s != 0.0) atomicAdd(&a.g_sums[(size_t)o * a.nb + b - 1], s);
+    }
+    for (int b = threadIdx.x + 1; b <= a.nb; b += T) {
+        unsigned long long c = 0;
+        for (int w = 0; w < NW; ++w) c += hc[w * NBP + b];
+        if (c) atomicAdd(&a.g_counts[b - 1], c);
+    }
+}
+
+// ================================================================================================
+// Flat (Euclidean) 1D, FP32 bulk + FP64 recheck
+// ================================================================================================
+template <int D, class OPS>
+__global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
+{
+    constexpr int NV = OPS::n;
+    using Needs = ListNeeds<OPS>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x, NW = T >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int NBP = a.nb + 2;
+    const int n = a.n;
+    LutEntry32* lut = reinterpret_cast<LutEntry32*>(smem);
+    float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);
+    float* su = sx + D * T;
+    float* hhi = su + D * T;                    // NW * NV * NBP
+    float* hlo = hhi + NW * NV * NBP;           // NW * NV * NBP
+    unsigned* hc = reinterpret_cast<unsigned*>(hlo + NW * NV * NBP);  // NW * NBP
+    __shared__ unsigned long long s_recheck;
+
+    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry32); k += T)
+        lut[k] = static_cast<const LutEntry32*>(a.lut)[k];
+    for (int k = threadIdx.x; k < NW * NV * NBP; k += T) { hhi[k] = 0.f; hlo[k] = 0.f; }
+    for (int k = threadIdx.x; k < NW * NBP; k += T) hc[k] = 0u;
+    if (threadIdx.x == 0) s_recheck = 0ull;
+    float* whi = hhi + warp * NV * NBP;
+    float* wlo = hlo + warp * NV * NBP;
+    unsigned* whc = hc + warp * NBP;
+    unsigned long long my_recheck = 0;
+
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + threadIdx.x;
+        const bool iv = i < n;
+        float xi[D], ui[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            xi[d] = iv ? a.XF[(size_t)d * n + i] : 0.f;
+            ui[d] = iv ? a.UF[(size_t)d * n + i] : 0.f;
+        }
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                sx[d * T + threadIdx.x] = a.XF[(size_t)d * n + j0 + threadIdx.x];
+                su[d * T + threadIdx.x] = a.UF[(size_t)d * n + j0 + threadIdx.x];
+            }
+        }
+        __syncthreads();
+        const bool diag = ti == tj;
+        for (int jj = 0; jj < jn; ++jj) {
+            const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+            float dx[D], du[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                dx[d] = sx[d * T + jj] - xi[d];
+                du[d] = su[d * T + jj] - ui[d];
+            }
+            const float h2 = fmaf(dx[1], dx[1], dx[0] * dx[0]);
+            float r2 = h2;
+            if constexpr (D == 3) r2 = fmaf(dx[2], dx[2], h2);
+            const LutEntry32 e = lut[lut_cell32(r2, a.lg)];
+            int bin = e.base + (r2 > e.hi ? (e.mult & 0xffff) : 0);
+            bool slow = (e.mult & LUT_FLAG_SLOW) || (r2 >= e.lo && r2 <= e.hi);
+
+            float L = 0.f, Tt = 0.f, Q = 0.f;
+            const float rs = rsqrtf(r2);
+            if constexpr (Needs::L) {
+                float pp = dx[0] * du[0];
+#pragma unroll
+                for (int d = 1; d < D; ++d) pp = fmaf(dx[d], du[d], pp);
+                L = pp * rs;
+            }
+            if constexpr (Needs::T) {
+                const float t = fmaf(du[1], dx[0], -du[0] * dx[1]);
+                Tt = (D == 2) ? t * rs : t * rsqrtf(h2);
+            }
+            if constexpr (Needs::Q) {
+                Q = du[0] * du[0];
+#pragma unroll
+                for (int d = 1; d < D; ++d) Q = fmaf(du[d], du[d], Q);
+            }
+            float v[NV];
+            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
+
+            slow = slow && valid;
+            if (__any_sync(FULL, slow)) {
+                if (slow) {
+                    // FP64 recheck from the original inputs (reference arithmetic for the bin).
+                    const int j = j0 + jj;
+                    double dx64[D], du64[D];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        dx64[d] = SFB_SUB(a.X64[(size_t)d * n + j], a.X64[(size_t)d * n + i]);
+                        du64[d] = a.U64[(size_t)d * n + j] - a.U64[(size_t)d * n + i];
+                    }
+                    const double h264 = SFB_ADD(SFB_MUL(dx64[0], dx64[0]), SFB_MUL(dx64[1], dx64[1]));
+                    double r264 = h264;
+                    if constexpr (D == 3) r264 = SFB_ADD(h264, SFB_MUL(dx64[2], dx64[2]));
+                    bin = flat_exact_bin(a, r264);
+                    const double rs64 = rsqrt(r264);
+                    double L64 = 0.0, T64 = 0.0, Q64 = 0.0;
+                    if constexpr (Needs::L) {
+                        double pp = dx64[0] * du64[0];
+#pragma unroll
+                        for (int d = 1; d < D; ++d) pp = fma(dx64[d], du64[d], pp);
+                        L64 = pp * rs64;
+                    }
+                    if constexpr (Needs::T) {
+                        const double t = fma(du64[1], dx64[0], -du64[0] * dx64[1]);
+                        T64 = (D == 2) ? t * rs64 : t * rsqrt(h264);
+                    }
+                    if constexpr (Needs::Q) {
+                        Q64 = du64[0] * du64[0];
+#pragma unroll
+                        for (int d = 1; d < D; ++d) Q64 = fma(du64[d], du64[d], Q64);
+                    }
+                    double v64[NV];
+                    eval_ops(OPS{}, L64, T64, Q64, D, a.gen, v64);
+#pragma unroll
+                    for (int o = 0; o < NV; ++o) v[o] = (float)v64[o];
+                }
+                const unsigned sb = __ballot_sync(FULL, slow);
+                if (lane == 0) my_recheck += __popc(sb);
+            }
+            const int key = valid ? bin : a.nb + 1;
+            const unsigned peers = __match_any_sync(FULL, key);
+            reduce_peers<NV>(peers, lane, v);
+            if (lane == __ffs(peers) - 1) {
+                whc[key] += (unsigned)__popc(peers);
+#pragma unroll
+                for (int o = 0; o < NV; ++o) two_sum_acc(whi[o * NBP + key], wlo[o * NBP + key], v[o]);
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0 && my_recheck) atomicAdd(&s_recheck, my_recheck);
+    __syncthreads();
+    // only the caller's operators are written out (NV may include padding of the generic kernels)
+    for (int k = threadIdx.x; k < min(NV, a.nops) * a.nb; k += T) {
+        const int o = k / a.nb, b = k - o * a.nb + 1;
+        double s = 0.0;
+        for (int w = 0; w < NW; ++w) {
+            const int idx = (w * NV + o) * NBP + b;
+            s += (double)hhi[idx] + (double)hlo[idx];
+        }
+        if (s != 0.0) atomicAdd(&a.g_sums[(size_t)o * a.nb + b - 1], s);
+    }
+    for (int b = threadIdx.x + 1; b <= a.nb; b += T) {
+        unsigned long long c = 0;
+        for (int w = 0; w < NW; ++w) c += hc[w * NBP + b];
+        if (c) atomicAdd(&a.g_counts[b - 1], c);
+    }
+    if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
+}
+
+// ================================================================================================
+// Sphere 1D, FP64 (reference geodesic frame per pair)
+// ================================================================================================
+__device__ __forceinline__ void load_sph64(const double* X, int n, int i, SphPoint& P)
+{
+    P.p[0] = X[(size_t)0 * n + i]; P.p[1] = X[(size_t)1 * n + i]; P.p[2] = X[(size_t)2 * n + i];
+    P.E[0] = X[(size_t)3 * n + i]; P.E[1] = X[(size_t)4 * n + i];
+    P.N[0] = X[(size_t)5 * n + i]; P.N[1] = X[(size_t)6 * n + i]; P.N[2] = X[(size_t)7 * n + i];
+}
+
+template <int D, class OPS>
+__global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
+{
+    constexpr int NV = OPS::n;
+    constexpr int NX = 8;  // p(3), E(2), N(3)
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x, NW = T >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int NBP = a.nb + 2;
+    const int n = a.n;
+    LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
+    double* sx = reinterpret_cast<double*>(smem + a.lut_bytes);  // NX * T
+    double* su = sx + NX * T;                                     // D * T
+    double* hs = su + D * T;
+    unsigned long long* hc = reinterpret_cast<unsigned long long*>(hs + NW * NV * NBP);
+
+    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
+        lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
+    for (int k = threadIdx.x; k < NW * NV * NBP; k += T) hs[k] = 0.0;
+    for (int k = threadIdx.x; k < NW * NBP; k += T) hc[k] = 0ull;
+    double* whs = hs + warp * NV * NBP;
+    unsigned long long* whc = hc + warp * NBP;
+
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + threadIdx.x;
+        const bool iv = i < n;
+        SphPoint A;
+        double uA[D];
+        if (iv) load_sph64(a.X64, n, i, A);
+        else { for (int k = 0; k < 3; ++k) { A.p[k] = 0.0; A.N[k] = 0.0; } A.E[0] = A.E[1] = 0.0; }
+#pragma unroll
+        for (int d = 0; d < D; ++d) uA[d] = iv ? a.U64[(size_t)d * n + i] : 0.0;
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+#pragma unroll
+            for (int c = 0; c < NX; ++c) sx[c * T + threadIdx.x] = a.X64[(size_t)c * n + j0 + threadIdx.x];
+#pragma unroll
+            for (int d = 0; d < D; ++d) su[d * T + threadIdx.x] = a.U64[(size_t)d * n + j0 + threadIdx.x];
+        }
+        __syncthreads();
+        const bool diag = ti == tj;
+        for (int jj = 0; jj < jn; ++jj) {
+            SphPoint B;
+            B.p[0] = sx[0 * T + jj]; B.p[1] = sx[1 * T + jj]; B.p[2] = sx[2 * T + jj];
+            B.E[0] = sx[3 * T + jj]; B.E[1] = sx[4 * T + jj];
+            B.N[0] = sx[5 * T + jj]; B.N[1] = sx[6 * T + jj]; B.N[2] = sx[7 * T + jj];
+            double r, tA[2], tB[2];
+            const bool ok = x_sphere_frame(A, B, a.radius, r, tA, tB);
+            int bin;
+            if (a.dist_linear) bin = linear_bin(a.dlin, r);
+            else bin = (r != r) ? a.n_edges : lut64_bin(lut, a, r);
+            const bool valid = iv && ok && (!diag || jj > (int)threadIdx.x);
+            const int key = valid ? bin : a.nb + 1;
+            double uB[D], du[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) uB[d] = su[d * T + jj];
+            x_sphere_delta<D>(tA, tB, uA, uB, du);
+            const double L = du[0], Tt = du[1];
+            double Q = du[0] * du[0] + du[1] * du[1];
+            if constexpr (D == 3) Q = fma(du[2], du[2], Q);
+            double v[NV];
+            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
+            const unsigned peers = __match_any_sync(FULL, key);
+            reduce_peers<NV>(peers, lane, v);
+            if (lane == __ffs(peers) - 1) {
+                whc[key] += (unsigned long long)__popc(peers);
+#pragma unroll
+                for (int o = 0; o < NV; ++o) whs[o * NBP + key] += v[o];
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // only the caller's operators are written out (NV may include padding of the generic kernels)
+    for (int k = threadIdx.x; k < min(NV, a.nops) * a.nb; k += T) {
+        const int o = k / a.nb, b = k - o * a.nb + 1;
+        double s = 0.0;
+        for (int w = 0; w < NW; ++w) s += hs[(w * NV + o) * NBP + b];
+        if (s != 0.0) atomicAdd(&a.g_sums[(size_t)o * a.nb + b - 1], s);
+    }
+    for (int b = threadIdx.x + 1; b <= a.nb; b += T) {
+        unsigned long long c = 0;
+        for (int w = 0; w < NW; ++w) c += hc[w * NBP + b];
+        if (c) atomicAdd(&a.g_counts[b - 1], c);
+    }
+}
+
+// ================================================================================================
+// Sphere 1D, FP32 bulk + FP64 recheck.
+//
+// With d = q - p (chord vector), the reference's transported increments reduce to
+//   du_L = d . (U_B - U_A) / sin(sigma),  du_T = d . (W_B - W_A) / sin(sigma),
+//   sin^2(sigma) = |d|^2 (1 - |d|^2 / 4),
+// because t_A = d - (d.p) p and t_B = (d.p) q + d differ from d only along p and q, which are
+// orthogonal to the tangent vectors U, W at their own point. The bin is decided on the chord
+// |d|^2, which is monotone in the arc length, against the chord images of the edges. Short,
+// near-antipodal and near-edge pairs are recomputed with the reference frame in FP64.
+// ================================================================================================
+template <int D, class OPS>
+__global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
+{
+    constexpr int NV = OPS::n;
+    constexpr int NF = (D == 3) ? 10 : 9;  // p(3), U(3), W(3)[, up]
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x, NW = T >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int NBP = a.nb + 2;
+    const int n = a.n;
+    LutEntry32* lut = reinterpret_cast<LutEntry32*>(smem);
+    float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);  // NF * T
+    float* hhi = sx + NF * T;
+    float* hlo = hhi + NW * NV * NBP;
+    unsigned* hc = reinterpret_cast<unsigned*>(hlo + NW * NV * NBP);
+    __shared__ unsigned long long s_recheck;
+
+    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry32); k += T)
+        lut[k] = static_cast<const LutEntry32*>(a.lut)[k];
+    for (int k = threadIdx.x; k < NW * NV * NBP; k += T) { hhi[k] = 0.f; hlo[k] = 0.f; }
+    for (int k = threadIdx.x; k < NW * NBP; k += T) hc[k] = 0u;
+    if (threadIdx.x == 0) s_recheck = 0ull;
+    float* whi = hhi + warp * NV * NBP;
+    float* wlo = hlo + warp * NV * NBP;
+    unsigned* whc = hc + warp * NBP;
+    unsigned long long my_recheck = 0;
+
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + threadIdx.x;
+        const bool iv = i < n;
+        float fa[NF];
+#pragma unroll
+        for (int c = 0; c < NF; ++c) fa[c] = iv ? a.XF[(size_t)c * n + i] : 0.f;
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+#pragma unroll
+            for (int c = 0; c < NF; ++c) sx[c * T + threadIdx.x] = a.XF[(size_t)c * n + j0 + threadIdx.x];
+        }
+        __syncthreads();
+        const bool diag = ti == tj;
+        for (int jj = 0; jj < jn; ++jj) {
+            const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+            const float d0 = sx[0 * T + jj] - fa[0];
+            const float d1 = sx[1 * T + jj] - fa[1];
+            const float d2 = sx[2 * T + jj] - fa[2];
+            const float ch2 = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+            const LutEntry32 e = lut[lut_cell32(ch2, a.lg)];
+            int bin = e.base + (ch2 > e.hi ? (e.mult & 0xffff) : 0);
+            bool slow = (e.mult & LUT_FLAG_SLOW) || (ch2 >= e.lo && ch2 <= e.hi);
+            const float s2 = ch2 * fmaf(-0.25f, ch2, 1.0f);
+            const float inv_s = rsqrtf(s2);
+            const float dU0 = sx[3 * T + jj] - fa[3], dU1 = sx[4 * T + jj] - fa[4], dU2 = sx[5 * T + jj] - fa[5];
+            const float dW0 = sx[6 * T + jj] - fa[6], dW1 = sx[7 * T + jj] - fa[7], dW2 = sx[8 * T + jj] - fa[8];
+            const float L = fmaf(d2, dU2, fmaf(d1, dU1, d0 * dU0)) * inv_s;
+            const float Tt = fmaf(d2, dW2, fmaf(d1, dW1, d0 * dW0)) * inv_s;
+            float Q = fmaf(Tt, Tt, L * L);
+            if constexpr (D == 3) {
+                const float dw = sx[9 * T + jj] - fa[9];
+                Q = fmaf(dw, dw, Q);
+            }
+            float v[NV];
+            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
+
+            slow = slow && valid;
+            bool ok = true;
+            if (__any_sync(FULL, slow)) {
+                if (slow) {
+                    const int j = j0 + jj;
+                    SphPoint A, B;
+                    load_sph64(a.X64, n, i, A);
+                    load_sph64(a.X64, n, j, B);
+                    double r, tA[2], tB[2], uA[D], uB[D], du[D];
+                    ok = x_sphere_frame(A, B, a.radius, r, tA, tB);
+                    bin = sphere_exact_bin(a, r);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        uA[d] = a.U64[(size_t)d * n + i];
+                        uB[d] = a.U64[(size_t)d * n + j];
+                    }
+                    x_sphere_delta<D>(tA, tB, uA, uB, du);
+                    double Q64 = du[0] * du[0] + du[1] * du[1];
+                    if constexpr (D == 3) Q64 = fma(du[2], du[2], Q64);
+                    double v64[NV];
+                    eval_ops(OPS{}, du[0], du[1], Q64, D, a.gen, v64);
+#pragma unroll
+                    for (int o = 0; o < NV; ++o) v[o] = (float)v64[o];
+                }
+                const unsigned sb = __ballot_sync(FULL, slow);
+                if (lane == 0) my_recheck += __popc(sb);
+            }
+            const int key = (valid && ok) ? bin : a.nb + 1;
+            const unsigned peers = __match_any_sync(FULL, key);
+            reduce_peers<NV>(peers, lane, v);
+            if (lane == __ffs(peers) - 1) {
+                whc[key] += (unsigned)__popc(peers);
+#pragma unroll
+                for (int o = 0; o < NV; ++o) two_sum_acc(whi[o * NBP + key], wlo[o * NBP + key], v[o]);
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0 && my_recheck) atomicAdd(&s_recheck, my_recheck);
+    __syncthreads();
+    // only the caller's operators are written out (NV may include padding of the generic kernels)
+    for (int k = threadIdx.x; k < min(NV, a.nops) * a.nb; k += T) {
+        const int o = k / a.nb, b = k - o * a.nb + 1;
+        double s = 0.0;
+        for (int w = 0; w < NW; ++w) {
+            const int idx = (w * NV + o) * NBP + b;
+            s += (double)hhi[idx] + (double)hlo[idx];
+        }
+        if (s != 0.0) atomicAdd(&a.g_sums[(size_t)o * a.nb + b - 1], s);
+    }
+    for (int b = threadIdx.x + 1; b <= a.nb; b += T) {
+        unsigned long long c = 0;
+        for (int w = 0; w < NW; ++w) c += hc[w * NBP + b];
+        if (c) atomicAdd(&a.g_counts[b - 1], c);
+    }
+    if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
+}
+
+}  // namespace sfb

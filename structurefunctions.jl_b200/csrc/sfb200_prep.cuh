@@ -1,0 +1,216 @@
+// sfb200_prep.cuh -- per-run preparation kernels: input packing (column-major caller arrays ->
+// SoA, FP32 images, spherical bases), the coordinate bound, the FP32 window table, and the copy of
+// the accumulated histogram into caller device buffers.
+#pragma once
+
+#include "sfb200_common.cuh"
+#include "sfb200_sphmath.h"
+
+namespace sfb {
+
+// Block maxima of two non-negative doubles, folded into bound[0], bound[1] with integer atomicMax
+// (non-negative IEEE doubles order like their bit patterns). Call once per block, all threads.
+__device__ __forceinline__ void block_max2_to(double vx, double vu, unsigned long long* bound)
+{
+    __shared__ double red[2][32];
+    for (int o = 16; o > 0; o >>= 1) {
+        vx = fmax(vx, __shfl_xor_sync(FULL, vx, o));
+        vu = fmax(vu, __shfl_xor_sync(FULL, vu, o));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { red[0][warp] = vx; red[1][warp] = vu; }
+    __syncthreads();
+    if (warp == 0) {
+        const bool in = lane < (int)(blockDim.x >> 5);
+        vx = in ? red[0][lane] : 0.0;
+        vu = in ? red[1][lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            vx = fmax(vx, __shfl_xor_sync(FULL, vx, o));
+            vu = fmax(vu, __shfl_xor_sync(FULL, vu, o));
+        }
+        if (lane == 0 && vx > 0.0) atomicMax(&bound[0], (unsigned long long)__double_as_longlong(vx));
+        if (lane == 0 && vu > 0.0) atomicMax(&bound[1], (unsigned long long)__double_as_longlong(vu));
+    }
+}
+
+template <typename TX, typename TU>
+__global__ void k_pack_flat(const TX* __restrict__ x, const TU* __restrict__ u, int n, int D,
+                            double* X64, double* U64, float* XF, float* UF, unsigned long long* bound)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mx = 0.0, mu = 0.0;
+    if (i < n) {
+        for (int d = 0; d < D; ++d) {
+            const double xv = (double)x[(size_t)D * i + d];
+            const double uv = (double)u[(size_t)D * i + d];
+            X64[(size_t)d * n + i] = xv;
+            U64[(size_t)d * n + i] = uv;
+            if (XF) {
+                XF[(size_t)d * n + i] = (float)xv;
+                UF[(size_t)d * n + i] = (float)uv;
+            }
+            mx = fmax(mx, fabs(xv));  // fmax ignores NaN coordinates
+            mu = fmax(mu, fabs(uv));
+        }
+    }
+    block_max2_to(mx, mu, bound);
+}
+
+// Sphere: lon/lat -> p, E, N in FP64 with the shared degree-exact sincos (identical to the CPU
+// check), velocities as given; FP32 images p, U = u_e E + u_n N, W = u_n E - u_e N, [up].
+template <typename TX, typename TU>
+__global__ void k_pack_sphere(const TX* __restrict__ x, const TU* __restrict__ u, int n, int D,
+                              int unit, double* X64, double* U64, float* XF, unsigned long long* bound)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mu = 0.0;
+    if (i < n) {
+        for (int d = 0; d < D; ++d) mu = fmax(mu, fabs((double)u[(size_t)D * i + d]));
+    }
+    block_max2_to(1.0, mu, bound);
+    if (i >= n) return;
+    const double lon = (double)x[(size_t)2 * i], lat = (double)x[(size_t)2 * i + 1];
+    double sl, cl, sp, cp;
+    if (unit == SFB200_ANGLE_DEG) {
+        sfb_sincosd(lon, &sl, &cl);
+        sfb_sincosd(lat, &sp, &cp);
+    } else {
+        sfb_sincos(lon, &sl, &cl);
+        sfb_sincos(lat, &sp, &cp);
+    }
+    const double p0 = SFB_MUL(cp, cl), p1 = SFB_MUL(cp, sl), p2 = sp;
+    const double E0 = -sl, E1 = cl;
+    const double N0 = SFB_MUL(-sp, cl), N1 = SFB_MUL(-sp, sl), N2 = cp;
+    const double c[8] = {p0, p1, p2, E0, E1, N0, N1, N2};
+    for (int k = 0; k < 8; ++k) X64[(size_t)k * n + i] = c[k];
+    double uv[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < D; ++d) {
+        uv[d] = (double)u[(size_t)D * i + d];
+        U64[(size_t)d * n + i] = uv[d];
+    }
+    if (XF) {
+        const double ue = uv[0], un = uv[1];
+        const double U[3] = {ue * E0 + un * N0, ue * E1 + un * N1, un * N2};
+        const double W[3] = {un * E0 - ue * N0, un * E1 - ue * N1, -ue * N2};
+        XF[(size_t)0 * n + i] = (float)p0;
+        XF[(size_t)1 * n + i] = (float)p1;
+        XF[(size_t)2 * n + i] = (float)p2;
+        for (int k = 0; k < 3; ++k) {
+            XF[(size_t)(3 + k) * n + i] = (float)U[k];
+            XF[(size_t)(6 + k) * n + i] = (float)W[k];
+        }
+        if (D == 3) XF[(size_t)9 * n + i] = (float)uv[2];
+    }
+}
+
+// Window parameters of the FP32 key: |key32 - key64| <= A |c| + B sqrt|c| + C near an edge key c.
+// B and C carry the rounding of FP64 coordinates to FP32 and scale with the coordinate bound M
+// (from the pack kernel) as B = Bm * M, C = Cm * M^2; `short_rel` marks keys below (short_rel*M)^2
+// (flat) or below `short_key` (sphere) for FP64 recomputation; keys above `anti_key` likewise.
+struct WindowParams {
+    double A, Bm, Cm;
+    int use_bound;       // 1: M from the pack kernel; 0: M = 1
+    double short_rel;    // flat: short pairs have r < short_rel * M (0: none)
+    double short_key;    // sphere: absolute key threshold
+    double anti_key;     // keys above this are recomputed (sphere near-antipodal); +inf: none
+};
+
+// One thread per cell: certain-below count, the single overlapping edge interval, slow flags.
+__global__ void k_build_lut32(const double* __restrict__ ck, int nk, WindowParams wp, LutGeom g,
+                              const unsigned long long* bound_bits, LutEntry32* out)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.ncell) return;
+    const double M = wp.use_bound ? __longlong_as_double((long long)*bound_bits) : 1.0;
+    const double B = wp.Bm * M, C = wp.Cm * M * M;
+    auto lo_of = [&](int k) {
+        const double v = ck[k];
+        const double w = 2.0 * (wp.A * fabs(v) + B * sqrt(fabs(v)) + C);
+        return v - w;
+    };
+    auto hi_of = [&](int k) {
+        const double v = ck[k];
+        const double w = 2.0 * (wp.A * fabs(v) + B * sqrt(fabs(v)) + C);
+        return v + w;
+    };
+    const int sh = g.shift;
+    const double Klo = (c == 0) ? 0.0
+        : (double)__uint_as_float((unsigned)((g.base + c) << sh));
+    const double Khi = (c == g.ncell - 1) ? __longlong_as_double(0x7ff0000000000000ll)
+        : (double)__uint_as_float((unsigned)((g.base + c + 1) << sh));
+    // first k with hi_k >= Klo  (intervals before it are certainly below the cell)
+    int lo = 0, hi = nk;
+    while (lo < hi) { const int m = (lo + hi) >> 1; if (hi_of(m) < Klo) lo = m + 1; else hi = m; }
+    const int k0 = lo;
+    // first k with lo_k >= Khi (intervals from it on are certainly above the cell)
+    lo = k0; hi = nk;
+    while (lo < hi) { const int m = (lo + hi) >> 1; if (lo_of(m) < Khi) lo = m + 1; else hi = m; }
+    const int k1 = lo;
+    LutEntry32 e;
+    e.base = k0;
+    e.mult = 0;
+    e.lo = __int_as_float(0x7fc00000);
+    e.hi = __int_as_float(0x7fc00000);
+    if (k1 > k0) {
+        if (ck[k0] == ck[k1 - 1]) {
+            e.mult = k1 - k0;
+            e.lo = __double2float_rd(lo_of(k0));
+            e.hi = __double2float_ru(hi_of(k0));
+        } else {
+            e.mult = LUT_FLAG_SLOW;
+        }
+    }
+    double short_key = wp.short_key;
+    if (wp.short_rel > 0.0) short_key = (wp.short_rel * M) * (wp.short_rel * M);
+    if (Klo < short_key || Khi > wp.anti_key) e.mult |= LUT_FLAG_SLOW;
+    out[c] = e;
+}
+
+// Joint FP32 kernels: half-width, in value-bin index units, of the band around a value edge inside
+// which the FP32 value may sit on the other side of the FP64 value. Per distance row b the pair
+// separation is at least sqrt(row_key_lo[b]) (r for flat, chord for sphere), which bounds the
+// direction error; |du| is bounded by 2 sqrt(3) max|u|. For an operator of order k the value error
+// is k |du|_max^(k-1) times the increment error. Rows 0 and nd+1 are out of range.
+struct ValueWindowParams {
+    int nd;
+    int D;
+    int order;
+    int sphere;
+    int x_f64;
+    int u_f64;
+    double inv_step;  // value bins: 1/step
+    double neg_f_inv; // -first/step
+};
+
+__global__ void k_value_windows(const double* __restrict__ row_key_lo, ValueWindowParams p,
+                                const unsigned long long* bound, float* out)
+{
+    const double u32 = 0x1p-24;
+    const double M = p.sphere ? 1.0 : __longlong_as_double((long long)bound[0]);
+    const double U = __longlong_as_double((long long)bound[1]);
+    for (int b = threadIdx.x; b < p.nd + 2; b += blockDim.x) {
+        if (b == 0 || b == p.nd + 1) { out[b] = 3.0e38f; continue; }
+        const double rlo = sqrt(fmax(row_key_lo[b], 0.0));
+        const double pos_err = (p.x_f64 || p.sphere) ? 2.0 * sqrt((double)p.D) * M * u32 : 0.0;
+        const double eps_dir = (rlo > 0.0 ? pos_err / rlo : (pos_err > 0.0 ? 1e30 : 0.0)) + (p.D + 8) * u32;
+        const double U2 = 2.0 * sqrt(3.0) * U;
+        const double eps_L = U2 * eps_dir + (p.u_f64 ? 2.0 * sqrt(3.0) * U * u32 : 0.0) + U2 * 8.0 * u32;
+        double scale = 1.0;
+        for (int k = 1; k < p.order; ++k) scale *= U2;
+        const double wv = 4.0 * (p.order > 0 ? p.order : 1) * scale * eps_L;
+        const double wt = wv * fabs(p.inv_step) + 4.0 * fabs(p.neg_f_inv) * u32 + 1e-6;
+        out[b] = (float)fmin(wt, 3.0e38);
+    }
+}
+
+// Device outputs: out = (accumulate ? out : 0) + accumulated histogram.
+__global__ void k_finalize(const double* __restrict__ s, const unsigned long long* __restrict__ c,
+                           long long ns, long long nc, double* out_s, unsigned long long* out_c,
+                           int accumulate)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < ns) out_s[k] = (accumulate ? out_s[k] : 0.0) + s[k];
+    if (k < nc) out_c[k] = (accumulate ? out_c[k] : 0ull) + c[k];
+}
+
+}  // namespace sfb

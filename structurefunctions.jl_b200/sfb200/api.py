@@ -1,0 +1,377 @@
+"""Public entry points, mirroring src/Calculations/dispatch.jl of the reference.
+
+    calculate_structure_function(sf, x, u, distance_bins[, value_bins][, count_eltype];
+                                 backend=B200Backend(), output_type=..., distance_metric=Euclidean())
+    calculate_structure_function_inplace(sums, counts, sf, x, u, distance_bins[, value_bins]; ...)
+
+`x` is (W, N) and `u` is (D, N), with W = D for Euclidean geometry and W = 2 (lon, lat) on the
+sphere, as in the reference. NumPy arrays (host) and CUDA torch tensors (device-resident) are
+accepted. Validation, error types and result containers follow the reference; the O(N^2) pair loop
+runs in libsfb200.so on the GPU (no CPU fallback).
+
+Extension beyond the reference: `sf` may be a tuple/list of operators; the pair loop is then run
+once and a tuple of results (one per operator) is returned.
+"""
+import ctypes as C
+import weakref
+
+import numpy as np
+
+from . import _abi, _lib
+from .bins import AbstractBinEdges, as_bin_edges
+from .errors import ArgumentError, DimensionMismatch
+from .metrics import Euclidean, pair_geometry_for
+from .operators import AbstractDerivedStructureFunctionType, AbstractPairwiseStructureFunctionType
+from .results import (StructureFunction, StructureFunction2DSumsAndCounts, StructureFunctionSumsAndCounts,
+                      bin_average)
+
+try:  # torch is optional: only used to accept device-resident tensors
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+# ----------------------------------------------------------------------------------- backend
+
+_CONTEXTS = {}
+
+
+def _context(device):
+    ctx = _CONTEXTS.get(device)
+    if ctx is None:
+        ctx = _lib.Context(device)
+        _CONTEXTS[device] = ctx
+    return ctx
+
+
+class B200Backend:
+    """Execution backend that runs the pair loop on a B200 through libsfb200.so.
+
+    precision: "mixed" (FP32 bulk, FP64 recheck near bin edges, FP64 merge) or "fp64" (every
+    pair in FP64). Plans are cached per (operator set, bins, metric, dtypes).
+    """
+
+    def __init__(self, device=0, precision="mixed", tile=0):
+        if precision not in ("mixed", "fp64"):
+            raise ArgumentError("precision must be 'mixed' or 'fp64'")
+        self.device = int(device)
+        self.precision = precision
+        self.tile = int(tile)
+        self._plans = {}
+
+    def __repr__(self):
+        return f"B200Backend(device={self.device}, precision={self.precision!r})"
+
+    @property
+    def context(self):
+        return _context(self.device)
+
+    def plan(self, key, desc, keep):
+        p = self._plans.get(key)
+        if p is None:
+            p = _lib.Plan(self.context, desc, keep)
+            if self.tile:
+                p.set_launch(self.tile, self.tile, 0)
+            self._plans[key] = p
+        return p
+
+
+_DEFAULT_BACKEND = None
+
+
+def default_backend():
+    global _DEFAULT_BACKEND
+    if _DEFAULT_BACKEND is None:
+        _DEFAULT_BACKEND = B200Backend()
+    return _DEFAULT_BACKEND
+
+
+# ----------------------------------------------------------------------------------- validation
+
+class PointField:
+    """u is (D, N) (src/Calculations/shapes.jl:18)."""
+
+    def __init__(self, D):
+        self.D = D
+
+
+def _shape_of(a):
+    return tuple(a.shape)
+
+
+def _validate_spatial_dimension(D):
+    if D not in (2, 3):
+        raise DimensionMismatch(f"expected spatial/velocity dimension D=2 or D=3 on axis 1; got D={D}")
+
+
+def validate_array_shape(x, u, distance_metric):
+    """_validate_array_shape (src/Calculations/shapes.jl:67-105)."""
+    xs, us = _shape_of(x), _shape_of(u)
+    if len(xs) < 2:
+        raise DimensionMismatch(f"x must have shape (Dx, N) or (Dx, N, auxiliary...); got ndims(x)={len(xs)}")
+    if len(us) < 2:
+        raise DimensionMismatch(f"u must have shape (D, N) or (D, N, auxiliary...); got ndims(u)={len(us)}")
+    D = us[0]
+    _validate_spatial_dimension(D)
+    W = pair_geometry_for(distance_metric, D).coordinate_width()
+    if xs[0] != W:
+        raise DimensionMismatch(
+            f"this geometry locates a point with {W} coordinate(s) on axis 1 of x, but got size(x,1)={xs[0]} "
+            f"(velocity dimension D={D} from size(u,1))")
+    if us[1] != xs[1]:
+        raise DimensionMismatch(
+            f"x and u must share axis-2 point count N; got size(x,2)={xs[1]} and size(u,2)={us[1]}")
+    if len(xs) == 2 and len(us) == 2:
+        return PointField(D)
+    aux = ArgumentError("auxiliary-axis (batched) inputs are not implemented for B200Backend; "
+                        "pass (Dx, N)/(D, N) arrays")
+    if len(xs) == 2 and len(us) >= 3:  # SharedPositionField in the reference
+        raise aux
+    if len(xs) >= 3 and len(us) >= 3:  # VaryingPositionField in the reference
+        if len(xs) != len(us):
+            raise DimensionMismatch(
+                f"varying-position inputs must have the same rank; got ndims(x)={len(xs)} and ndims(u)={len(us)}")
+        if xs[2:] != us[2:]:
+            raise DimensionMismatch(f"varying-position inputs must share auxiliary axes; got {xs[2:]} and {us[2:]}")
+        raise aux
+    raise DimensionMismatch(
+        f"unsupported shape combination: x has shape {xs}, u has shape {us}; valid forms are (Dx,N)/(D,N), "
+        "(Dx,N)/(D,N,auxiliary...), or matched (Dx,N,auxiliary...) arrays")
+
+
+def assert_counts_representable(count_eltype, n_points):
+    """_assert_counts_representable (src/Calculations/serial.jl:111-120)."""
+    ct = np.dtype(count_eltype)
+    if ct.kind not in "iu":
+        raise ArgumentError(f"count_eltype must be an integer type; got {ct}")
+    n_pairs = (int(n_points) * (int(n_points) - 1)) // 2
+    if n_pairs > int(np.iinfo(ct).max):
+        raise ArgumentError(
+            f"count_eltype={ct} cannot represent the worst-case pair count {n_pairs} for N={n_points} "
+            f"(typemax({ct}) = {np.iinfo(ct).max}); pass count_eltype=np.uint64 or np.int64.")
+
+
+def _derived_error(sf):
+    raise ArgumentError(
+        f"{type(sf).__name__} is a derived structure-function quantity, not a pairwise operator. Use "
+        "helmholtz_decompose_2d for 2D Helmholtz rotational/divergent quantities.")
+
+
+# ----------------------------------------------------------------------------------- arrays
+
+def _is_torch(a):
+    return torch is not None and isinstance(a, torch.Tensor)
+
+
+def _dtype_code(dt):
+    if dt == np.float64:
+        return _abi.F64
+    if dt == np.float32:
+        return _abi.F32
+    raise ArgumentError(f"inputs must be Float32 or Float64; got {dt}")
+
+
+def _prepare(a):
+    """(W, N) array -> (pointer, keepalive, dtype code, on_device) with column-major memory."""
+    if _is_torch(a):
+        if a.dtype not in (torch.float32, torch.float64):
+            raise ArgumentError(f"inputs must be Float32 or Float64; got {a.dtype}")
+        t = a.t().contiguous()  # (N, W) row-major == (W, N) column-major
+        code = _abi.F64 if a.dtype == torch.float64 else _abi.F32
+        if t.is_cuda:
+            return t.data_ptr(), t, code, True
+        arr = t.numpy()
+        return arr.ctypes.data, arr, code, False
+    arr = np.asarray(a)
+    if arr.dtype not in (np.float32, np.float64):
+        if arr.dtype.kind in "iu":
+            arr = arr.astype(np.float64)
+        else:
+            raise ArgumentError(f"inputs must be Float32 or Float64; got {arr.dtype}")
+    arr = np.asfortranarray(arr)
+    return arr.ctypes.data, arr, _dtype_code(arr.dtype), False
+
+
+def _output_float_type(x_code, u_code):
+    """promote_type(float(FTx), float(FTu)) (src/Calculations/batch.jl:179)."""
+    return np.float64 if (x_code == _abi.F64 or u_code == _abi.F64) else np.float32
+
+
+# ----------------------------------------------------------------------------------- core
+
+def _ops_of(sf):
+    if isinstance(sf, (list, tuple)):
+        ops = list(sf)
+        multi = True
+    else:
+        ops = [sf]
+        multi = False
+    for o in ops:
+        if isinstance(o, AbstractDerivedStructureFunctionType):
+            _derived_error(o)
+        if not isinstance(o, AbstractPairwiseStructureFunctionType):
+            raise ArgumentError(f"not a structure-function operator: {o!r}")
+    if not 1 <= len(ops) <= _abi.MAX_OPS:
+        raise ArgumentError(f"between 1 and {_abi.MAX_OPS} operators per call")
+    return ops, multi
+
+
+def plan_description(ops, D, distance_bins, value_bins=None, distance_metric=None, precision="mixed",
+                     x_dtype=np.float64, u_dtype=np.float64):
+    """The C-ABI plan description (and the arrays it points to) for a call of the public API."""
+    distance_metric = Euclidean() if distance_metric is None else distance_metric
+    geom = pair_geometry_for(distance_metric, D)
+    keep = []
+    dbins = as_bin_edges(distance_bins)
+    desc = _abi.PlanDesc()
+    desc.geometry = geom.kind
+    desc.dim = geom.dim
+    desc.angle_unit = geom.angle_unit
+    desc.radius = geom.radius
+    desc.n_ops = len(ops)
+    for k, o in enumerate(ops):
+        desc.ops[k] = o.as_abi()
+    desc.distance = dbins.distance_abi(geom.kind, keep)
+    desc.joint = 1 if value_bins is not None else 0
+    if value_bins is not None:
+        desc.value = as_bin_edges(value_bins).value_abi(keep)
+    desc.precision = _abi.PREC_MIXED if precision == "mixed" else _abi.PREC_FP64
+    desc.x_dtype = _dtype_code(np.dtype(x_dtype))
+    desc.u_dtype = _dtype_code(np.dtype(u_dtype))
+    return desc, keep
+
+
+def _run(backend, ops, x, u, distance_bins, value_bins, distance_metric):
+    """Run the pair loop; returns (sums (float64), counts (uint64), plan, x_code, u_code)."""
+    shape = validate_array_shape(x, u, distance_metric)
+    geom = pair_geometry_for(distance_metric, shape.D)
+    xp, xkeep, xcode, xdev = _prepare(x)
+    up, ukeep, ucode, udev = _prepare(u)
+    if xdev != udev:
+        raise ArgumentError("x and u must both be host arrays or both be device tensors")
+    n = _shape_of(x)[1]
+    dt = {_abi.F64: np.float64, _abi.F32: np.float32}
+    desc, keep = plan_description(ops, shape.D, distance_bins, value_bins, distance_metric, backend.precision,
+                                  dt[xcode], dt[ucode])
+    key = (tuple(ops), as_bin_edges(distance_bins), value_bins is not None and as_bin_edges(value_bins), geom,
+           xcode, ucode)
+    plan = backend.plan(key, desc, keep)
+    sums = np.zeros(plan.n_sums, dtype=np.float64)
+    counts = np.zeros(plan.n_counts, dtype=np.uint64)
+    flags = _abi.RUN_DEVICE_INPUT if xdev else 0
+    plan.run(xp, up, n, flags, sums.ctypes.data, counts.ctypes.data)
+    return sums, counts, plan, xcode, ucode
+
+
+def _split_args(args):
+    """(value_bins?, count_eltype?) from the positional tail, as the reference's methods take them."""
+    value_bins, count_eltype = None, np.uint32
+    rest = list(args)
+    if rest and not _is_dtype_like(rest[0]):
+        value_bins = rest.pop(0)
+    if rest:
+        count_eltype = rest.pop(0)
+    if rest:
+        raise ArgumentError("too many positional arguments")
+    return value_bins, count_eltype
+
+
+def _is_dtype_like(v):
+    if isinstance(v, (AbstractBinEdges, list, tuple, np.ndarray)):
+        return False
+    try:
+        np.dtype(v)
+        return True
+    except TypeError:
+        return False
+
+
+def calculate_structure_function(structure_function_type, x, u, distance_bins, *args, backend=None,
+                                 output_type=None, distance_metric=None, count_eltype=None, verbose=False,
+                                 show_progress=False):
+    """The reference's `calculate_structure_function` (src/Calculations/dispatch.jl:64-91, 108-136)."""
+    if isinstance(x, tuple) or isinstance(u, tuple):
+        raise ArgumentError("tuple-of-component-vector inputs are not part of the stabilized public API; "
+                            "pass arrays with shape (D, N) or (D, N, auxiliary...) instead")
+    ops, multi = _ops_of(structure_function_type)
+    value_bins, ct = _split_args(args)
+    if count_eltype is not None:
+        ct = count_eltype
+    if isinstance(distance_bins, (int, np.integer)):
+        raise ArgumentError("automatic distance binning (distance_bins::Int) is not implemented for "
+                            "B200Backend; pass bin edges")
+    distance_metric = Euclidean() if distance_metric is None else distance_metric
+    backend = default_backend() if backend is None else backend
+    if not isinstance(backend, B200Backend):
+        raise ArgumentError(f"backend {backend!r} is not a B200Backend")
+    joint = value_bins is not None
+    if joint and multi:
+        raise ArgumentError("a joint (distance x value) histogram takes exactly one operator")
+    if output_type is None:
+        output_type = StructureFunction2DSumsAndCounts if joint else StructureFunction
+    validate_array_shape(x, u, distance_metric)
+    assert_counts_representable(ct, _shape_of(x)[1])
+    sums, counts, plan, xcode, ucode = _run(backend, ops, x, u, distance_bins, value_bins, distance_metric)
+    ot = _output_float_type(xcode, ucode)
+    ct = np.dtype(ct)
+    if joint:
+        nd = len(distance_bins) - 1
+        nv = len(value_bins) - 1
+        s2 = sums.reshape((nd, nv), order="F").astype(ot)
+        c2 = counts.reshape((nd, nv), order="F").astype(ct)
+        raw = StructureFunction2DSumsAndCounts(ops[0], distance_bins, value_bins, s2, c2)
+        if output_type is not StructureFunction2DSumsAndCounts:
+            raise ArgumentError(f"Cannot produce a {getattr(output_type, '__name__', output_type)} from this "
+                                f"calculation (got a StructureFunction2DSumsAndCounts). Check the `output_type` keyword.")
+        return raw
+    nb = len(distance_bins) - 1
+    c1 = counts.astype(ct)
+    results = []
+    for k, o in enumerate(ops):
+        raw = StructureFunctionSumsAndCounts(o, distance_bins, sums[k * nb:(k + 1) * nb].astype(ot), c1.copy())
+        results.append(_finalize(raw, output_type))
+    return tuple(results) if multi else results[0]
+
+
+def _finalize(raw, output_type):
+    """_finalize (src/Calculations/dispatch.jl:20-29)."""
+    if output_type is StructureFunctionSumsAndCounts:
+        return raw
+    if output_type is StructureFunction:
+        return StructureFunction(raw.operator, raw.distance, bin_average(raw.sums, raw.counts))
+    raise ArgumentError(f"Cannot produce a {getattr(output_type, '__name__', output_type)} from this calculation "
+                        f"(got a {type(raw).__name__}). Check the `output_type` keyword.")
+
+
+def calculate_structure_function_inplace(sums, counts, structure_function_type, x, u, distance_bins,
+                                         value_bins=None, *, backend=None, distance_metric=None, verbose=False,
+                                         show_progress=False):
+    """The reference's mutating `calculate_structure_function!` (src/Calculations/dispatch.jl:346-373):
+    adds this call's sums and counts into the caller's arrays."""
+    if isinstance(x, tuple) or isinstance(u, tuple):
+        raise ArgumentError("tuple-of-component-vector inputs are not part of the stabilized public API; "
+                            "pass arrays with shape (D, N) or (D, N, auxiliary...) instead")
+    ops, multi = _ops_of(structure_function_type)
+    if multi:
+        raise ArgumentError("the mutating entry takes one operator")
+    distance_metric = Euclidean() if distance_metric is None else distance_metric
+    backend = default_backend() if backend is None else backend
+    validate_array_shape(x, u, distance_metric)
+    counts_arr = np.asarray(counts)
+    assert_counts_representable(counts_arr.dtype, _shape_of(x)[1])
+    s, c, plan, _, _ = _run(backend, ops, x, u, distance_bins, value_bins, distance_metric)
+    if value_bins is not None:
+        nd, nv = len(distance_bins) - 1, len(value_bins) - 1
+        s = s.reshape((nd, nv), order="F")
+        c = c.reshape((nd, nv), order="F")
+    if sums.shape != s.shape or counts_arr.shape != c.shape:
+        raise DimensionMismatch(f"sums/counts must have shape {s.shape}; got {sums.shape} and {counts_arr.shape}")
+    sums += s.astype(sums.dtype)
+    counts += c.astype(counts_arr.dtype)
+    return None
+
+
+def last_stats(backend=None):
+    """Statistics of the most recent run of each cached plan of `backend`."""
+    backend = default_backend() if backend is None else backend
+    return [p.stats() for p in backend._plans.values()]

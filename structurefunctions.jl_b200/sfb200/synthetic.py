@@ -1,0 +1,161 @@
+"""Seeded synthetic workloads with the shapes and value distributions of the benchmark configs.
+
+No public dataset is involved: every input is generated here from a fixed seed (NumPy PCG64).
+
+  c0  2D planar, N=4096, Float64, 32 Fourier modes (|k| in [1,64], amplitude |k|^-5/6) + N(0, 0.01^2)
+      noise; L2SF; 32 log distance bins 1e-3..sqrt(2).
+  c1  3D unit cube, N=65536, Float64, 64 solenoidal modes (|k| in [1,128], amplitude |k|^-11/6);
+      L2SF, T2SF, L3SF, T3SF fused; 64 log bins 1e-4..sqrt(3).
+  c2  sphere, N=200000 (lon, lat) degrees, Float32, radius 6371 km; 48 zonal/meridional modes
+      (degree l in [1,200], amplitude l^-5/6, each component scaled to unit variance); L2SF along
+      the arc; 48 log bins 1..20000 km.
+  c3  2D planar, N=131072, Float32, field as c0; joint du_L histogram, 64 log distance bins
+      1e-3..sqrt(2) x 256 linear value bins over [-5 sigma, 5 sigma], sigma = sqrt(2) std(u).
+Log edges are materialized once as e_k = exp(ln(lo) + k (ln(hi) - ln(lo)) / nb) with the end points
+set exactly.
+"""
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import operators as OP
+from .bins import BinEdges, LinearBinEdges
+from .metrics import Euclidean, Haversine
+
+
+def log_edges(lo, hi, nb):
+    k = np.arange(nb + 1, dtype=np.float64)
+    e = np.exp(math.log(lo) + k * (math.log(hi) - math.log(lo)) / nb)
+    e[0] = lo
+    e[-1] = hi
+    return e
+
+
+def planar_field(x, n_modes, kmax, rng, noise_std):
+    """Sum of random Fourier modes on [0,1)^2 (amplitude |k|^-5/6) plus Gaussian noise; x is (2, N)."""
+    N = x.shape[1]
+    kmag = rng.uniform(1.0, kmax, n_modes)
+    th_k = rng.uniform(0.0, 2 * np.pi, n_modes)
+    th_e = rng.uniform(0.0, 2 * np.pi, n_modes)
+    phi = rng.uniform(0.0, 2 * np.pi, n_modes)
+    amp = kmag ** (-5.0 / 6.0)
+    kvec = np.stack([kmag * np.cos(th_k), kmag * np.sin(th_k)])  # (2, M)
+    evec = np.stack([np.cos(th_e), np.sin(th_e)])                # (2, M)
+    phase = 2 * np.pi * (kvec.T @ x) + phi[:, None]              # (M, N)
+    u = evec @ (amp[:, None] * np.cos(phase))                    # (2, N)
+    u += rng.normal(0.0, noise_std, size=(2, N))
+    return u
+
+
+def solenoidal_field(x, n_modes, kmax, rng):
+    """64 random divergence-free modes in 3D (a_m perpendicular to k_m, |a_m| = |k|^-11/6)."""
+    kmag = rng.uniform(1.0, kmax, n_modes)
+    khat = rng.normal(size=(3, n_modes))
+    khat /= np.linalg.norm(khat, axis=0)
+    # an orthonormal pair perpendicular to k-hat, then a random angle in that plane
+    ref = np.where(np.abs(khat[2]) < 0.9, np.array([[0.0], [0.0], [1.0]]), np.array([[1.0], [0.0], [0.0]]))
+    e1 = np.cross(khat.T, ref.T).T
+    e1 /= np.linalg.norm(e1, axis=0)
+    e2 = np.cross(khat.T, e1.T).T
+    ang = rng.uniform(0.0, 2 * np.pi, n_modes)
+    avec = (np.cos(ang) * e1 + np.sin(ang) * e2) * kmag ** (-11.0 / 6.0)
+    phi = rng.uniform(0.0, 2 * np.pi, n_modes)
+    phase = 2 * np.pi * ((kmag * khat).T @ x) + phi[:, None]  # (M, N)
+    return avec @ np.cos(phase)                                # (3, N)
+
+
+def sphere_points(N, rng):
+    lon = rng.uniform(-180.0, 180.0, N)
+    lat = np.degrees(np.arcsin(rng.uniform(-1.0, 1.0, N)))
+    return np.stack([lon, lat])
+
+
+def sphere_field(x, n_modes, lmax, rng):
+    """Zonal (u_east ~ cos(l lat)) and meridional (u_north ~ cos(l lon)) modes, unit variance."""
+    lon = np.radians(x[0])
+    lat = np.radians(x[1])
+    N = x.shape[1]
+    u = np.zeros((2, N))
+    ls = rng.integers(1, lmax + 1, n_modes)
+    phi = rng.uniform(0.0, 2 * np.pi, n_modes)
+    for m in range(n_modes):
+        a = float(ls[m]) ** (-5.0 / 6.0)
+        if m % 2 == 0:
+            u[0] += a * np.cos(ls[m] * lat + phi[m])
+        else:
+            u[1] += a * np.cos(ls[m] * lon + phi[m])
+    u[0] /= u[0].std()
+    u[1] /= u[1].std()
+    return u
+
+
+@dataclass
+class Workload:
+    name: str
+    x: np.ndarray
+    u: np.ndarray
+    ops: tuple
+    distance_bins: object
+    metric: object = field(default_factory=Euclidean)
+    value_bins: object = None
+    flops_per_pair: int = 0
+    sigma: float = float("nan")
+
+    @property
+    def n(self):
+        return self.x.shape[1]
+
+    @property
+    def pairs(self):
+        return self.n * (self.n - 1) // 2
+
+
+def config(name, n=None):
+    """Workload `name` in {"c0", "c1", "c2", "c3"}; `n` truncates to the first n points (same seed)."""
+    if name == "c0":
+        N = 4096 if n is None else n
+        rng = np.random.default_rng(0)
+        x = rng.random((2, max(N, 4096)))
+        u = planar_field(x, 32, 64.0, rng, 0.01)
+        return Workload("c0 2D N=%d L2SF 32 log bins F64" % N, x[:, :N].copy(), u[:, :N].copy(), (OP.L2SF,),
+                        BinEdges(log_edges(1e-3, math.sqrt(2.0), 32)), flops_per_pair=FLOPS["c0"])
+    if name == "c1":
+        N = 65536 if n is None else n
+        rng = np.random.default_rng(1)
+        x = rng.random((3, 65536))
+        u = solenoidal_field(x, 64, 128.0, rng)
+        return Workload("c1 3D N=%d L2/T2/L3/T3 64 log bins F64" % N, x[:, :N].copy(), u[:, :N].copy(),
+                        (OP.L2SF, OP.T2SF, OP.L3SF, OP.T3SF), BinEdges(log_edges(1e-4, math.sqrt(3.0), 64)),
+                        flops_per_pair=FLOPS["c1"])
+    if name == "c2":
+        N = 200000 if n is None else n
+        rng = np.random.default_rng(2)
+        x = sphere_points(200000, rng)
+        u = sphere_field(x, 48, 200, rng)
+        return Workload("c2 sphere N=%d L2SF 48 log bins 1..20000 km F32" % N,
+                        x[:, :N].astype(np.float32), u[:, :N].astype(np.float32), (OP.L2SF,),
+                        BinEdges(log_edges(1.0, 20000.0, 48)), metric=Haversine(6371.0),
+                        flops_per_pair=FLOPS["c2"])
+    if name == "c3":
+        N = 131072 if n is None else n
+        rng = np.random.default_rng(3)
+        x = rng.random((2, 131072))
+        u = planar_field(x, 32, 64.0, rng, 0.01)
+        sigma = math.sqrt(2.0) * float(np.std(u.astype(np.float32).astype(np.float64).ravel()))
+        vb = LinearBinEdges(-5.0 * sigma, 5.0 * sigma, 257)
+        return Workload("c3 2D N=%d joint du_L 64x256 F32" % N, x[:, :N].astype(np.float32),
+                        u[:, :N].astype(np.float32), (OP.ProjectedStructureFunctionType(1, 0),),
+                        BinEdges(log_edges(1e-3, math.sqrt(2.0), 64)), value_bins=vb,
+                        flops_per_pair=FLOPS["c3"], sigma=sigma)
+    raise KeyError(name)
+
+
+# Algorithmic FP32/FP64 operations per pair of the FP32 kernel's formulation (+, -, *, sqrt/rsqrt,
+# rcp = 1 each, FMA = 2; binning compares and rechecks not counted; one add per accumulated sum).
+#   c0 (2D L2):  dx 2, r^2 3 (mul + fma), du 2, p 3, rsqrt 1, L 1, L^2 1, acc 1            = 14
+#   c1 (3D L2,T2,L3,T3): dx 3, h^2 3, r^2 2, du 3, p 5, |du|^2 5, rsqrt 1, L 1, L2 1, T2 1,
+#        L3 2, t 3, rsqrt(h^2) 1, T 1, T3 2, acc 4                                       = 38
+#   c2 (sphere L2): d 3, |d|^2 5, s^2 3, rsqrt 1, dU 3, d.dU 5, scale 1, L^2 1, acc 1       = 23
+#   c3 (2D joint du_L): dx 2, r^2 3, du 2, p 3, rsqrt 1, L 1, t 2, centre 1, acc 1         = 16
+FLOPS = {"c0": 14, "c1": 38, "c2": 23, "c3": 16}

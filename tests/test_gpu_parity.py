@@ -1,0 +1,176 @@
+"""GPU parity: libsfb200.so through the C ABI against the CPU oracle on the same seeded inputs.
+
+Counts must be identical (bit-exact, joint cells included); sums must agree per bin within
+TOL_FP64 (FP64 kernels) or TOL_MIXED (FP32 kernels) times the oracle's per-bin sum of |value|.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle_py
+from helpers import TOL_FP64, TOL_MIXED, compare
+import sfb200 as SF
+from sfb200 import _lib, synthetic
+from sfb200.api import plan_description
+
+pytestmark = pytest.mark.gpu
+
+PRECISIONS = [("fp64", TOL_FP64), ("mixed", TOL_MIXED)]
+
+
+def run_gpu(ops, x, u, bins, metric=None, value_bins=None, precision="mixed", tile=0):
+    be = SF.B200Backend(precision=precision, tile=tile)
+    desc, keep = plan_description(ops, u.shape[0], bins, value_bins, metric, precision, x.dtype, u.dtype)
+    plan = _lib.Plan(be.context, desc, keep)
+    if tile:
+        plan.set_launch(tile, tile, 0)
+    sums = np.zeros(plan.n_sums)
+    counts = np.zeros(plan.n_counts, dtype=np.uint64)
+    xa = np.asfortranarray(x)
+    ua = np.asfortranarray(u)
+    plan.run(xa.ctypes.data, ua.ctypes.data, x.shape[1], 0, sums.ctypes.data, counts.ctypes.data)
+    st = plan.stats()
+    plan.close()
+    return sums, counts, st
+
+
+def run_oracle(ops, x, u, bins, metric=None, value_bins=None):
+    desc, keep = plan_description(ops, u.shape[0], bins, value_bins, metric, "fp64", x.dtype, u.dtype)
+    return oracle_py.run(desc, x, u, with_abs=True)
+
+
+def check(ops, x, u, bins, metric=None, value_bins=None, precision="mixed", tol=TOL_MIXED, tile=0):
+    gs, gc, st = run_gpu(ops, x, u, bins, metric, value_bins, precision, tile)
+    rs, rc, ra = run_oracle(ops, x, u, bins, metric, value_bins)
+    nb = len(bins) - 1
+    if value_bins is None:
+        scale = ra
+        for k in range(len(ops)):
+            compare(gs[k * nb:(k + 1) * nb], gc, rs[k * nb:(k + 1) * nb], rc, ra[k * nb:(k + 1) * nb], tol)
+    else:
+        compare(gs, gc, rs, rc, ra, tol)
+    return st
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+@pytest.mark.parametrize("D", [2, 3])
+def test_flat_l2_random(precision, tol, D):
+    rng = np.random.default_rng(10 + D)
+    x = rng.random((D, 1500))
+    u = rng.standard_normal((D, 1500))
+    bins = synthetic.log_edges(1e-3, math.sqrt(D), 24)
+    check((SF.L2SF,), x, u, bins, precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_flat_quad_3d(precision, tol):
+    w = synthetic.config("c1", n=2048)
+    check(w.ops, w.x, w.u, w.distance_bins.edges, precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_c0_full(precision, tol):
+    w = synthetic.config("c0")
+    check(w.ops, w.x, w.u, w.distance_bins.edges, precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+@pytest.mark.parametrize("opset", [
+    (SF.S2SF,), (SF.T2SF,), (SF.L3SF,), (SF.T3SF,), (SF.S3SF,), (SF.L1T2SF,), (SF.L2T1SF,), (SF.T2ComponentSF,),
+    (SF.L1T2ComponentSF,), (SF.FullVectorStructureFunctionType(3),), (SF.ProjectedStructureFunctionType(1, 1),),
+    (SF.L2SF, SF.T2SF), (SF.S2SF, SF.L2SF, SF.T2SF, SF.S3SF, SF.L3SF, SF.L1T2SF),
+])
+@pytest.mark.parametrize("D", [2, 3])
+def test_flat_operator_matrix(precision, tol, opset, D):
+    rng = np.random.default_rng(100 + D)
+    x = rng.random((D, 700))
+    u = rng.standard_normal((D, 700))
+    bins = np.linspace(0.0, math.sqrt(D), 17)
+    check(opset, x, u, bins, precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_flat_linear_bins(precision, tol):
+    rng = np.random.default_rng(7)
+    x = rng.random((2, 1200))
+    u = rng.standard_normal((2, 1200))
+    bins = SF.LinearBinEdges(0.0, 1.4, 11)
+    check((SF.L2SF,), x, u, bins, precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_flat_float32_inputs(precision, tol):
+    rng = np.random.default_rng(8)
+    x = rng.random((2, 1500)).astype(np.float32)
+    u = rng.standard_normal((2, 1500)).astype(np.float32)
+    bins = np.linspace(0.0, 1.4, 11).astype(np.float32)
+    check((SF.L2SF,), x, u, bins, precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+@pytest.mark.parametrize("D", [2, 3])
+def test_sphere_l2(precision, tol, D):
+    w = synthetic.config("c2", n=1500)
+    u = w.u
+    if D == 3:
+        u = np.vstack([w.u, np.random.default_rng(5).standard_normal((1, w.n)).astype(np.float32)])
+    check((SF.L2SF, SF.T2SF, SF.S2SF) if D == 3 else w.ops, w.x, u, w.distance_bins.edges, metric=w.metric,
+          precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_sphere_radians_and_odd_ops(precision, tol):
+    rng = np.random.default_rng(9)
+    lon = rng.uniform(-math.pi, math.pi, 900)
+    lat = np.arcsin(rng.uniform(-1, 1, 900))
+    x = np.stack([lon, lat])
+    u = rng.standard_normal((2, 900))
+    bins = np.linspace(0.0, math.pi, 13)
+    check((SF.L3SF, SF.T3SF, SF.L2T1SF), x, u, bins, metric=SF.SphericalAngle(), precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_joint_c3_subset(precision, tol):
+    w = synthetic.config("c3", n=3000)
+    check(w.ops, w.x, w.u, w.distance_bins.edges, value_bins=w.value_bins, precision=precision, tol=tol)
+
+
+def test_joint_fp64_vector_value_bins():
+    rng = np.random.default_rng(11)
+    x = rng.random((2, 800))
+    u = rng.standard_normal((2, 800))
+    check((SF.L2SF,), x, u, np.linspace(0, 1.4, 9), value_bins=np.linspace(0.0, 4.0, 11), precision="fp64",
+          tol=TOL_FP64)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_joint_sphere(precision, tol):
+    w = synthetic.config("c2", n=1200)
+    vb = SF.LinearBinEdges(-3.0, 3.0, 61)
+    check((SF.ProjectedStructureFunctionType(1, 0),), w.x, w.u, w.distance_bins.edges, metric=w.metric,
+          value_bins=vb, precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tiny_and_empty(precision):
+    be = SF.B200Backend(precision=precision)
+    for n in (0, 1, 2, 3):
+        x = np.arange(2 * n, dtype=np.float64).reshape(2, n) / 10.0
+        u = np.ones((2, n))
+        r = SF.calculate_structure_function(SF.L2SF, x, u, [0.0, 3.0], backend=be,
+                                            output_type=SF.StructureFunctionSumsAndCounts)
+        assert int(r.counts.sum()) == n * (n - 1) // 2
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_points_on_edges_exact(precision):
+    """Pairs placed exactly on bin edges (right-inclusive) and at edge +- 1 ulp."""
+    edges = np.array([0.1, 0.2, 0.3, 0.5])
+    xs = [0.0]
+    for e in edges:
+        xs += [e, np.nextafter(e, 1.0), np.nextafter(e, 0.0)]
+    x = np.zeros((2, len(xs)))
+    x[0] = xs
+    u = np.random.default_rng(3).standard_normal((2, len(xs)))
+    check((SF.L2SF,), x, u, edges, precision=precision, tol=TOL_MIXED)
