@@ -20,3 +20,7 @@ def oracle():
 
     oracle_py.load()
     return oracle_py
+
+GOLDEN_DIR = os.path.join(ROOT, "tests", "golden")
+if GOLDEN_DIR not in sys.path:
+    sys.path.insert(0, GOLDEN_DIR)
