@@ -31,6 +31,8 @@ struct sfb200_plan {
     sfb200_ctx* ctx = nullptr;
     sfb200_plan_desc desc{};
     bool sphere = false, mixed = false, joint = false;
+    bool df = false;  // FP32 records carry (hi, lo) pairs (an input is FP64, or the sphere basis)
+    bool l_only = false;  // the joint value depends on du_L only (compensated in FP32)
     int D = 0, W = 0, nb = 0, nv = 0, nops = 0, nops_pad = 0, opl = 0, vorder = 1;
     GenOps gen{};
     // exact key tables (flat: squared edges; sphere: edges with -0.0 moved just below +0.0)
@@ -380,6 +382,7 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "x_dtype/u_dtype must be F64 or F32");
     p->mixed = d.precision == SFB200_PREC_MIXED;
     p->joint = d.joint != 0;
+    p->df = p->mixed && (p->sphere || d.x_dtype == SFB200_F64 || d.u_dtype == SFB200_F64);
     if (d.n_ops < 1 || d.n_ops > SFB200_MAX_OPS)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "n_ops must be in 1..%d", SFB200_MAX_OPS);
     if (p->joint && d.n_ops != 1)
@@ -424,6 +427,7 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         else p->gen.op[k] = sfb200_operator{SFB200_OP_PROJECTED, 0, 0, 0};
     }
     p->vorder = op_order(d.ops[0]);
+    p->l_only = d.ops[0].kind == SFB200_OP_PROJECTED && d.ops[0].nt == 0;
 
     // distance tables
     const sfb200_bins& db = d.distance;
@@ -458,21 +462,24 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
             return set_err(ctx, SFB200_ERR_UNSUPPORTED,
                            "distance edges outside the FP32 range of the mixed-precision kernel; use precision=fp64");
         const double u32 = 0x1p-24, u64 = 0x1p-53;
-        const bool x64 = d.x_dtype == SFB200_F64, u64in = d.u_dtype == SFB200_F64;
         if (p->sphere) {
-            p->wp.A = 5.0 * u32 * 1.1 + 1e-14;
-            p->wp.Bm = 4.0 * std::sqrt(3.0) * u32 * 1.1;
-            p->wp.Cm = 12.0 * u32 * u32 * 1.1;
+            // (hi, lo) records: the chord carries ~2u per component plus the FMA chain; the FP64
+            // arc length differs from the chord image of the edges by ~1e-15 relative.
+            p->wp.A = 9.0 * u32 * 1.1 + 1e-14;
+            p->wp.Bm = 4.0 * std::sqrt(3.0) * u32 * u32 * 1.1;
+            p->wp.Cm = 0.0;
             p->wp.use_bound = 0;
             p->wp.short_rel = 0.0;
-            p->wp.short_key = 0x1p-12;                 // chord < 1/64
-            p->wp.anti_key = 4.0 * (1.0 - 0x1p-12);    // sin^2(sigma) < 2^-10 near the antipode
+            p->wp.short_key = 0x1p-40;                 // (near-)coincident: frame degenerate
+            p->wp.anti_key = 4.0 - 0x1p-40;            // (near-)antipodal: frame degenerate
         } else {
-            p->wp.A = (p->D + 3) * u32 * 1.1 + 8.0 * p->D * u64 + (dlinear ? 1e-14 : 0.0);
-            p->wp.Bm = x64 ? 4.0 * std::sqrt((double)p->D) * u32 * 1.1 : 0.0;
-            p->wp.Cm = x64 ? 4.0 * p->D * u32 * u32 * 1.1 : 0.0;
+            // FP32 inputs are exact floats: differences carry u. FP64 inputs come as (hi, lo)
+            // pairs: differences carry 2u plus the u^2 |x| residual of the split.
+            p->wp.A = (p->D + (p->df ? 5 : 3)) * u32 * 1.1 + 8.0 * p->D * u64 + (dlinear ? 1e-14 : 0.0);
+            p->wp.Bm = p->df ? 4.0 * std::sqrt((double)p->D) * u32 * u32 * 1.1 : 0.0;
+            p->wp.Cm = 0.0;
             p->wp.use_bound = 1;
-            p->wp.short_rel = (x64 || u64in) ? 0x1p-6 : 0.0;
+            p->wp.short_rel = p->df ? 0x1p-20 : 0.0;
             p->wp.short_key = 0.0;
             p->wp.anti_key = INFINITY;
         }
@@ -515,8 +522,8 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
     p->h_counts.resize(p->n_counts);
 
     // the kernel exists for this combination
-    KernelChoice kc = p->joint ? pick_joint(p->sphere, p->D, p->mixed, true, p->opl)
-                               : (p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl) : pick_flat1d(p->D, p->mixed, p->opl));
+    KernelChoice kc = p->joint ? pick_joint(p->sphere, p->D, p->mixed, true, p->df, p->opl)
+                               : (p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl) : pick_flat1d(p->D, p->mixed, p->df, p->opl));
     if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this operator on the joint mixed path");
     return SFB200_OK;
 }
@@ -577,14 +584,14 @@ static int ensure_workspace(sfb200_plan* p, long long n)
     free_workspace(p);
     const long long cap = std::max<long long>(n, 1024);
     const int nx64 = p->sphere ? 8 : p->D;
-    const int nxf = p->sphere ? (p->D == 3 ? 10 : 9) : p->D;
+    const int nxf = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 2 * p->D : p->D);
     CK(cudaMalloc(&p->d_rawx, sizeof(double) * p->W * cap));
     CK(cudaMalloc(&p->d_rawu, sizeof(double) * p->D * cap));
     CK(cudaMalloc(&p->d_X64, sizeof(double) * nx64 * cap));
     CK(cudaMalloc(&p->d_U64, sizeof(double) * p->D * cap));
     if (p->mixed) {
         CK(cudaMalloc(&p->d_XF, sizeof(float) * nxf * cap));
-        if (!p->sphere) CK(cudaMalloc(&p->d_UF, sizeof(float) * p->D * cap));
+        if (!p->sphere) CK(cudaMalloc(&p->d_UF, sizeof(float) * (p->df ? 2 : 1) * p->D * cap));
     }
     p->cap = cap;
     return SFB200_OK;
@@ -598,7 +605,7 @@ static void launch_pack(sfb200_plan* p, const void* x, const void* u, int n, cud
         k_pack_sphere<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->desc.angle_unit,
                                                   p->d_X64, p->d_U64, p->mixed ? p->d_XF : nullptr, p->d_aux + 1);
     else
-        k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->d_X64, p->d_U64,
+        k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->df, p->d_X64, p->d_U64,
                                                 p->mixed ? p->d_XF : nullptr, p->mixed ? p->d_UF : nullptr,
                                                 p->d_aux + 1);
 }
@@ -612,14 +619,14 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
             const int nx = p->sphere ? 8 : p->D;
             return (size_t)(nx + p->D) * T * 8 + (smem_hist ? (size_t)ncell * 12 : 0);
         }
-        const int nx = p->sphere ? (p->D == 3 ? 10 : 9) : 2 * p->D;
+        const int nx = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 4 : 2) * p->D;
         return (size_t)lut_bytes + (size_t)nx * T * 4 + (size_t)ncell * 8 + (size_t)(p->nb + 2) * 4;
     }
     if (!p->mixed) {
         const int nx = p->sphere ? 8 : p->D;
         return (size_t)lut_bytes + (size_t)(nx + p->D) * T * 8 + (size_t)NW * NV * NBP * 8 + (size_t)NW * NBP * 8;
     }
-    const int nx = p->sphere ? (p->D == 3 ? 10 : 9) : 2 * p->D;
+    const int nx = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 4 : 2) * p->D;
     return (size_t)lut_bytes + (size_t)nx * T * 4 + (size_t)NW * NV * NBP * 8 + (size_t)NW * NBP * 4;
 }
 
@@ -685,6 +692,8 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
                 vw.sphere = p->sphere;
                 vw.x_f64 = x64;
                 vw.u_f64 = u64;
+                vw.df = p->df;
+                vw.l_only = p->l_only;
                 vw.inv_step = p->desc.value.kind == SFB200_BINS_LINEAR ? p->vlin.inv_step : 0.0;
                 vw.neg_f_inv = p->desc.value.kind == SFB200_BINS_LINEAR ? p->vlin.neg_f_inv : 0.0;
                 k_value_windows<<<1, 128, 0, s>>>(p->d_rowlo, vw, p->d_aux + 1, p->d_vwin);
@@ -715,9 +724,9 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
                 smem_hist = false;
                 smem = smem_bytes(p, T, lut_bytes, false);
             }
-            kc = pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->opl);
+            kc = pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->df, p->opl);
         } else {
-            kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl) : pick_flat1d(p->D, p->mixed, p->opl);
+            kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl) : pick_flat1d(p->D, p->mixed, p->df, p->opl);
             if (p->tile_ovr) {
                 T = p->tile_ovr;
             } else {
@@ -769,6 +778,9 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         a.vedges = p->d_vedges;
         a.n_vedges = p->joint ? p->desc.value.n_edges : 0;
         a.vwin = p->d_vwin;
+        // per-pair relative value error: compensated du_L carries ~(6 order + 6) u; otherwise only
+        // the rounding of t itself (the rest is in the per-row absolute window)
+        a.vrel = (float)((p->l_only ? (6.0 * p->vorder + 6.0) * 1.25 : 4.0) * 0x1p-24);
         a.gen = p->gen;
         a.g_sums = p->d_sums;
         a.g_counts = p->d_counts;

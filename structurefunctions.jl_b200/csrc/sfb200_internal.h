@@ -28,9 +28,10 @@ struct KernelChoice {
     int max_threads;  // launch bound
 };
 
-// Kernel lookup: returns nullptr fn for an unsupported combination.
-KernelChoice pick_flat1d(int D, bool mixed, int opl);
+// Kernel lookup: returns nullptr fn for an unsupported combination. `df`: FP32 records carry
+// (hi, lo) pairs because an input is FP64.
+KernelChoice pick_flat1d(int D, bool mixed, bool df, int opl);
 KernelChoice pick_sphere1d(int D, bool mixed, int opl);
-KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, int opl);
+KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, bool df, int opl);
 
 }  // namespace sfb

@@ -125,10 +125,33 @@ __device__ __forceinline__ float value_center(const PairArgs& a, int vb)
     return (float)(0.5 * (a.vedges[vb - 1] + a.vedges[vb]));
 }
 
-template <bool SPHERE, int D, class OPS>
+// Compensated dot product (Ogita-Rump-Oishi Dot2): the exact product errors come from fma and the
+// sum errors from a two-sum, so the result is as accurate as if computed in twice the precision.
+// Used for the joint value axis, where cells near du_L = 0 hold values that a plain FP32 dot product
+// (with cancellation) would get wrong in the leading digits.
+template <int K>
+__device__ __forceinline__ float dot2(const float* x, const float* y)
+{
+    float p = __fmul_rn(x[0], y[0]);
+    float e = __fmaf_rn(x[0], y[0], -p);
+#pragma unroll
+    for (int k = 1; k < K; ++k) {
+        const float q = __fmul_rn(x[k], y[k]);
+        const float eq = __fmaf_rn(x[k], y[k], -q);
+        const float s = __fadd_rn(p, q);
+        const float bp = __fsub_rn(s, p);
+        const float es = __fadd_rn(__fsub_rn(p, __fsub_rn(s, bp)), __fsub_rn(q, bp));
+        p = s;
+        e = __fadd_rn(e, __fadd_rn(eq, es));
+    }
+    return __fadd_rn(p, e);
+}
+
+template <bool SPHERE, int D, bool DFX, bool DFU, class OPS>
 __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
 {
-    constexpr int NX = SPHERE ? ((D == 3) ? 10 : 9) : D;
+    constexpr int NXF = SPHERE ? ((D == 3) ? 20 : 18) : (DFX ? 2 * D : D);
+    constexpr int NUF = SPHERE ? 0 : (DFU ? 2 * D : D);
     constexpr int NV = 1;
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = blockDim.x;
@@ -137,9 +160,9 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
     const int nd = a.nb, nv = a.nv;
     const int ncell = nd * nv;
     LutEntry32* lut = reinterpret_cast<LutEntry32*>(smem);
-    float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);  // NX * T
-    float* su = sx + NX * T;                                    // D * T (flat)
-    float* hres = su + (SPHERE ? 0 : D * T);                    // ncell
+    float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);  // NXF * T
+    float* su = sx + NXF * T;                                   // NUF * T (flat)
+    float* hres = su + NUF * T;                                 // ncell
     unsigned* hc = reinterpret_cast<unsigned*>(hres + ncell);   // ncell
     float* swin = reinterpret_cast<float*>(hc + ncell);         // nd + 2
     __shared__ unsigned long long s_recheck;
@@ -159,23 +182,19 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
         decode_tile_pair(p, a.ntiles, ti, tj);
         const int i = ti * T + threadIdx.x;
         const bool iv = i < n;
-        float xa[NX], ua[D];
+        float xa[NXF], ua[NUF > 0 ? NUF : 1];
 #pragma unroll
-        for (int c = 0; c < NX; ++c) xa[c] = iv ? a.XF[(size_t)c * n + i] : 0.f;
-        if constexpr (!SPHERE) {
+        for (int c = 0; c < NXF; ++c) xa[c] = iv ? a.XF[(size_t)c * n + i] : 0.f;
 #pragma unroll
-            for (int d = 0; d < D; ++d) ua[d] = iv ? a.UF[(size_t)d * n + i] : 0.f;
-        }
+        for (int c = 0; c < NUF; ++c) ua[c] = iv ? a.UF[(size_t)c * n + i] : 0.f;
         __syncthreads();
         const int j0 = tj * T;
         const int jn = min(T, n - j0);
         if ((int)threadIdx.x < jn) {
 #pragma unroll
-            for (int c = 0; c < NX; ++c) sx[c * T + threadIdx.x] = a.XF[(size_t)c * n + j0 + threadIdx.x];
-            if constexpr (!SPHERE) {
+            for (int c = 0; c < NXF; ++c) sx[c * T + threadIdx.x] = a.XF[(size_t)c * n + j0 + threadIdx.x];
 #pragma unroll
-                for (int d = 0; d < D; ++d) su[d * T + threadIdx.x] = a.UF[(size_t)d * n + j0 + threadIdx.x];
-            }
+            for (int c = 0; c < NUF; ++c) su[c * T + threadIdx.x] = a.UF[(size_t)c * n + j0 + threadIdx.x];
         }
         __syncthreads();
         const bool diag = ti == tj;
@@ -186,35 +205,38 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
                 float dx[D], du[D];
 #pragma unroll
                 for (int d = 0; d < D; ++d) {
-                    dx[d] = sx[d * T + jj] - xa[d];
-                    du[d] = su[d * T + jj] - ua[d];
+                    dx[d] = df_diff<DFX>(sx, d, D, T, jj, xa);
+                    du[d] = df_diff<DFU>(su, d, D, T, jj, ua);
                 }
                 const float h2 = fmaf(dx[1], dx[1], dx[0] * dx[0]);
                 float r2 = h2;
                 if constexpr (D == 3) r2 = fmaf(dx[2], dx[2], h2);
                 key = r2;
                 const float rs = rsqrtf(r2);
-                float pp = dx[0] * du[0];
-#pragma unroll
-                for (int d = 1; d < D; ++d) pp = fmaf(dx[d], du[d], pp);
-                L = pp * rs;
+                L = dot2<D>(dx, du) * rs;
                 const float t = fmaf(du[1], dx[0], -du[0] * dx[1]);
                 Tt = (D == 2) ? t * rs : t * rsqrtf(h2);
                 Q = du[0] * du[0];
 #pragma unroll
                 for (int d = 1; d < D; ++d) Q = fmaf(du[d], du[d], Q);
             } else {
-                const float d0 = sx[0 * T + jj] - xa[0];
-                const float d1 = sx[1 * T + jj] - xa[1];
-                const float d2 = sx[2 * T + jj] - xa[2];
-                const float ch2 = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+                float d[3], sv[3], dU[3], dW[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    d[c] = df_diff<true>(sx, c, 3, T, jj, xa);
+                    sv[c] = __fadd_rn(__fadd_rn(sx[c * T + jj], xa[c]), __fadd_rn(sx[(3 + c) * T + jj], xa[3 + c]));
+                    dU[c] = df_diff<true>(sx + 6 * T, c, 3, T, jj, xa + 6);
+                    dW[c] = df_diff<true>(sx + 12 * T, c, 3, T, jj, xa + 12);
+                }
+                const float ch2 = fmaf(d[2], d[2], fmaf(d[1], d[1], d[0] * d[0]));
                 key = ch2;
-                const float inv_s = rsqrtf(ch2 * fmaf(-0.25f, ch2, 1.0f));
-                L = fmaf(d2, sx[5 * T + jj] - xa[5], fmaf(d1, sx[4 * T + jj] - xa[4], d0 * (sx[3 * T + jj] - xa[3]))) * inv_s;
-                Tt = fmaf(d2, sx[8 * T + jj] - xa[8], fmaf(d1, sx[7 * T + jj] - xa[7], d0 * (sx[6 * T + jj] - xa[6]))) * inv_s;
+                const float ss = fmaf(sv[2], sv[2], fmaf(sv[1], sv[1], sv[0] * sv[0]));
+                const float inv_s = rsqrtf(0.25f * ch2 * ss);
+                L = dot2<3>(d, dU) * inv_s;
+                Tt = fmaf(d[2], dW[2], fmaf(d[1], dW[1], d[0] * dW[0])) * inv_s;
                 Q = fmaf(Tt, Tt, L * L);
                 if constexpr (D == 3) {
-                    const float dw = sx[9 * T + jj] - xa[9];
+                    const float dw = df_diff<true>(sx + 18 * T, 0, 1, T, jj, xa + 18);
                     Q = fmaf(dw, dw, Q);
                 }
             }
@@ -235,7 +257,8 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
                 if (a.val_linear) {
                     const float fl = floorf(t);
                     const float fr = t - fl;
-                    const float wt = swin[min(max(db, 0), nd + 1)] + fabsf(t) * 2.4e-7f;
+                    // absolute part per distance row + relative part (|t| + |first/step|) * vrel
+                    const float wt = swin[min(max(db, 0), nd + 1)] + (fabsf(t) + fabsf(vnegf)) * a.vrel;
                     vb = (t <= 0.f) ? 0 : ((t > tmax) ? a.vlin.n : (int)fl + 1);
                     slow = slow || fr < wt || fr > 1.f - wt || fabsf(t) < wt || fabsf(t - tmax) < wt || !(t == t);
                 } else {

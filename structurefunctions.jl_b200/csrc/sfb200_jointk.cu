@@ -11,26 +11,27 @@ static KernelChoice joint_fp64(bool smem)
     return {reinterpret_cast<const void*>(&k_joint_fp64<SPHERE, D, false>), 512};
 }
 
-template <bool SPHERE, int D>
+template <bool SPHERE, int D, bool DF>
 static KernelChoice joint_mixed(int opl)
 {
     switch (opl) {
-    case OPL_L1: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, OpList<OC_L1>>), 512};
-    case OPL_L2: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, OpList<OC_L2>>), 512};
-    case OPL_L3: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, OpList<OC_L3>>), 512};
-    case OPL_GEN1: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, OpList<OC_GEN>>), 512};
+    case OPL_L1: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_L1>>), 512};
+    case OPL_L2: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_L2>>), 512};
+    case OPL_L3: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_L3>>), 512};
+    case OPL_GEN1: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_GEN>>), 512};
     }
     return {nullptr, 0};
 }
 
-KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, int opl)
+KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, bool df, int opl)
 {
     if (!mixed) {
         if (sphere) return D == 2 ? joint_fp64<true, 2>(smem_hist) : joint_fp64<true, 3>(smem_hist);
         return D == 2 ? joint_fp64<false, 2>(smem_hist) : joint_fp64<false, 3>(smem_hist);
     }
-    if (sphere) return D == 2 ? joint_mixed<true, 2>(opl) : joint_mixed<true, 3>(opl);
-    return D == 2 ? joint_mixed<false, 2>(opl) : joint_mixed<false, 3>(opl);
+    if (sphere) return D == 2 ? joint_mixed<true, 2, true>(opl) : joint_mixed<true, 3, true>(opl);
+    if (df) return D == 2 ? joint_mixed<false, 2, true>(opl) : joint_mixed<false, 3, true>(opl);
+    return D == 2 ? joint_mixed<false, 2, false>(opl) : joint_mixed<false, 3, false>(opl);
 }
 
 }  // namespace sfb

@@ -53,7 +53,9 @@ struct PairArgs {
     LinearParams vlin;
     const double* vedges;
     int n_vedges;
-    const float* vwin; // per distance row: half-width of the value ambiguity window (mixed), value units
+    const float* vwin; // per distance row: absolute half-width of the value ambiguity window in
+                       // value-bin index units (mixed)
+    float vrel;        // relative half-width: window += (|t| + |first/step|) * vrel
     GenOps gen;
     double* g_sums;
     unsigned long long* g_counts;
@@ -212,11 +214,25 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
 
 // ================================================================================================
 // Flat (Euclidean) 1D, FP32 bulk + FP64 recheck
+//
+// FP64 inputs are carried as FP32 (hi, lo) pairs with hi + lo equal to the FP64 value to ~2^-48
+// relative, and differences are formed as (b_hi - a_hi) + (b_lo - a_lo): the difference of two
+// nearby coordinates (or velocities) then keeps full FP32 relative accuracy instead of inheriting
+// the rounding error of the coordinates themselves. FP32 inputs are exact in one float.
 // ================================================================================================
-template <int D, class OPS>
+template <bool DF>
+__device__ __forceinline__ float df_diff(const float* s, int c, int D, int T, int jj, const float* a)
+{
+    if constexpr (DF) return __fadd_rn(__fsub_rn(s[c * T + jj], a[c]), __fsub_rn(s[(D + c) * T + jj], a[D + c]));
+    else return __fsub_rn(s[c * T + jj], a[c]);
+}
+
+template <int D, bool DFX, bool DFU, class OPS>
 __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
 {
     constexpr int NV = OPS::n;
+    constexpr int NXF = DFX ? 2 * D : D;
+    constexpr int NUF = DFU ? 2 * D : D;
     using Needs = ListNeeds<OPS>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = blockDim.x, NW = T >> 5;
@@ -225,8 +241,8 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
     const int n = a.n;
     LutEntry32* lut = reinterpret_cast<LutEntry32*>(smem);
     float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);
-    float* su = sx + D * T;
-    float* hhi = su + D * T;                    // NW * NV * NBP
+    float* su = sx + NXF * T;
+    float* hhi = su + NUF * T;                  // NW * NV * NBP
     float* hlo = hhi + NW * NV * NBP;           // NW * NV * NBP
     unsigned* hc = reinterpret_cast<unsigned*>(hlo + NW * NV * NBP);  // NW * NBP
     __shared__ unsigned long long s_recheck;
@@ -246,21 +262,19 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
         decode_tile_pair(p, a.ntiles, ti, tj);
         const int i = ti * T + threadIdx.x;
         const bool iv = i < n;
-        float xi[D], ui[D];
+        float xi[NXF], ui[NUF];
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-            xi[d] = iv ? a.XF[(size_t)d * n + i] : 0.f;
-            ui[d] = iv ? a.UF[(size_t)d * n + i] : 0.f;
-        }
+        for (int c = 0; c < NXF; ++c) xi[c] = iv ? a.XF[(size_t)c * n + i] : 0.f;
+#pragma unroll
+        for (int c = 0; c < NUF; ++c) ui[c] = iv ? a.UF[(size_t)c * n + i] : 0.f;
         __syncthreads();
         const int j0 = tj * T;
         const int jn = min(T, n - j0);
         if ((int)threadIdx.x < jn) {
 #pragma unroll
-            for (int d = 0; d < D; ++d) {
-                sx[d * T + threadIdx.x] = a.XF[(size_t)d * n + j0 + threadIdx.x];
-                su[d * T + threadIdx.x] = a.UF[(size_t)d * n + j0 + threadIdx.x];
-            }
+            for (int c = 0; c < NXF; ++c) sx[c * T + threadIdx.x] = a.XF[(size_t)c * n + j0 + threadIdx.x];
+#pragma unroll
+            for (int c = 0; c < NUF; ++c) su[c * T + threadIdx.x] = a.UF[(size_t)c * n + j0 + threadIdx.x];
         }
         __syncthreads();
         const bool diag = ti == tj;
@@ -269,8 +283,8 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
             float dx[D], du[D];
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                dx[d] = sx[d * T + jj] - xi[d];
-                du[d] = su[d * T + jj] - ui[d];
+                dx[d] = df_diff<DFX>(sx, d, D, T, jj, xi);
+                du[d] = df_diff<DFU>(su, d, D, T, jj, ui);
             }
             const float h2 = fmaf(dx[1], dx[1], dx[0] * dx[0]);
             float r2 = h2;
@@ -474,19 +488,23 @@ __global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
 // ================================================================================================
 // Sphere 1D, FP32 bulk + FP64 recheck.
 //
-// With d = q - p (chord vector), the reference's transported increments reduce to
+// With d = q - p (chord vector) and s = p + q, the reference's transported increments reduce to
 //   du_L = d . (U_B - U_A) / sin(sigma),  du_T = d . (W_B - W_A) / sin(sigma),
-//   sin^2(sigma) = |d|^2 (1 - |d|^2 / 4),
+//   sin^2(sigma) = |d|^2 |s|^2 / 4,
 // because t_A = d - (d.p) p and t_B = (d.p) q + d differ from d only along p and q, which are
 // orthogonal to the tangent vectors U, W at their own point. The bin is decided on the chord
-// |d|^2, which is monotone in the arc length, against the chord images of the edges. Short,
-// near-antipodal and near-edge pairs are recomputed with the reference frame in FP64.
+// |d|^2, which is monotone in the arc length, against the chord images of the edges. Per-point
+// records are FP32 (hi, lo) pairs of the FP64 basis and velocities (p, U, W[, up]), so d, s and the
+// velocity differences keep FP32 relative accuracy at every separation, including the antipode
+// (|s| -> 0). Coincident, antipodal and near-edge pairs are recomputed with the reference frame in
+// FP64.
 // ================================================================================================
 template <int D, class OPS>
 __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
 {
     constexpr int NV = OPS::n;
-    constexpr int NF = (D == 3) ? 10 : 9;  // p(3), U(3), W(3)[, up]
+    using Needs = ListNeeds<OPS>;
+    constexpr int NF = (D == 3) ? 20 : 18;  // (hi, lo) of p(3), U(3), W(3)[, up]
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -528,23 +546,35 @@ __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
         const bool diag = ti == tj;
         for (int jj = 0; jj < jn; ++jj) {
             const bool valid = iv && (!diag || jj > (int)threadIdx.x);
-            const float d0 = sx[0 * T + jj] - fa[0];
-            const float d1 = sx[1 * T + jj] - fa[1];
-            const float d2 = sx[2 * T + jj] - fa[2];
-            const float ch2 = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+            float d[3], sv[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                d[c] = df_diff<true>(sx, c, 3, T, jj, fa);
+                sv[c] = __fadd_rn(__fadd_rn(sx[c * T + jj], fa[c]), __fadd_rn(sx[(3 + c) * T + jj], fa[3 + c]));
+            }
+            const float ch2 = fmaf(d[2], d[2], fmaf(d[1], d[1], d[0] * d[0]));
             const LutEntry32 e = lut[lut_cell32(ch2, a.lg)];
             int bin = e.base + (ch2 > e.hi ? (e.mult & 0xffff) : 0);
             bool slow = (e.mult & LUT_FLAG_SLOW) || (ch2 >= e.lo && ch2 <= e.hi);
-            const float s2 = ch2 * fmaf(-0.25f, ch2, 1.0f);
-            const float inv_s = rsqrtf(s2);
-            const float dU0 = sx[3 * T + jj] - fa[3], dU1 = sx[4 * T + jj] - fa[4], dU2 = sx[5 * T + jj] - fa[5];
-            const float dW0 = sx[6 * T + jj] - fa[6], dW1 = sx[7 * T + jj] - fa[7], dW2 = sx[8 * T + jj] - fa[8];
-            const float L = fmaf(d2, dU2, fmaf(d1, dU1, d0 * dU0)) * inv_s;
-            const float Tt = fmaf(d2, dW2, fmaf(d1, dW1, d0 * dW0)) * inv_s;
-            float Q = fmaf(Tt, Tt, L * L);
-            if constexpr (D == 3) {
-                const float dw = sx[9 * T + jj] - fa[9];
-                Q = fmaf(dw, dw, Q);
+            const float ss = fmaf(sv[2], sv[2], fmaf(sv[1], sv[1], sv[0] * sv[0]));
+            const float inv_s = rsqrtf(0.25f * ch2 * ss);
+            float L = 0.f, Tt = 0.f, Q = 0.f;
+            {
+                float dU[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) dU[c] = df_diff<true>(sx + 6 * T, c, 3, T, jj, fa + 6);
+                L = fmaf(d[2], dU[2], fmaf(d[1], dU[1], d[0] * dU[0])) * inv_s;
+            }
+            if constexpr (Needs::T || Needs::Q) {
+                float dW[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) dW[c] = df_diff<true>(sx + 12 * T, c, 3, T, jj, fa + 12);
+                Tt = fmaf(d[2], dW[2], fmaf(d[1], dW[1], d[0] * dW[0])) * inv_s;
+                Q = fmaf(Tt, Tt, L * L);
+                if constexpr (D == 3) {
+                    const float dw = df_diff<true>(sx + 18 * T, 0, 1, T, jj, fa + 18);
+                    Q = fmaf(dw, dw, Q);
+                }
             }
             float v[NV];
             eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);

@@ -33,10 +33,19 @@ __device__ __forceinline__ void block_max2_to(double vx, double vu, unsigned lon
     }
 }
 
+// FP32 image of an FP64 value as (hi, lo): hi = fl32(v), lo = fl32(v - hi); hi + lo equals v to
+// about 2^-48 relative.
+__device__ __forceinline__ void split_df(double v, float& hi, float& lo)
+{
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
+}
+
 template <typename TX, typename TU>
-__global__ void k_pack_flat(const TX* __restrict__ x, const TU* __restrict__ u, int n, int D,
+__global__ void k_pack_flat(const TX* __restrict__ x, const TU* __restrict__ u, int n, int D, int df,
                             double* X64, double* U64, float* XF, float* UF, unsigned long long* bound)
 {
+    // with df, every FP32 value is stored as (hi, lo) (lo = 0 for FP32 inputs)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double mx = 0.0, mu = 0.0;
     if (i < n) {
@@ -46,8 +55,13 @@ __global__ void k_pack_flat(const TX* __restrict__ x, const TU* __restrict__ u, 
             X64[(size_t)d * n + i] = xv;
             U64[(size_t)d * n + i] = uv;
             if (XF) {
-                XF[(size_t)d * n + i] = (float)xv;
-                UF[(size_t)d * n + i] = (float)uv;
+                float h, l;
+                split_df(xv, h, l);
+                XF[(size_t)d * n + i] = h;
+                if (df) XF[(size_t)(D + d) * n + i] = l;
+                split_df(uv, h, l);
+                UF[(size_t)d * n + i] = h;
+                if (df) UF[(size_t)(D + d) * n + i] = l;
             }
             mx = fmax(mx, fabs(xv));  // fmax ignores NaN coordinates
             mu = fmax(mu, fabs(uv));
@@ -89,17 +103,29 @@ __global__ void k_pack_sphere(const TX* __restrict__ x, const TU* __restrict__ u
         U64[(size_t)d * n + i] = uv[d];
     }
     if (XF) {
+        // records of (hi, lo) pairs: p at 0..5, U at 6..11, W at 12..17, up at 18..19
         const double ue = uv[0], un = uv[1];
+        const double P[3] = {p0, p1, p2};
         const double U[3] = {ue * E0 + un * N0, ue * E1 + un * N1, un * N2};
         const double W[3] = {un * E0 - ue * N0, un * E1 - ue * N1, -ue * N2};
-        XF[(size_t)0 * n + i] = (float)p0;
-        XF[(size_t)1 * n + i] = (float)p1;
-        XF[(size_t)2 * n + i] = (float)p2;
         for (int k = 0; k < 3; ++k) {
-            XF[(size_t)(3 + k) * n + i] = (float)U[k];
-            XF[(size_t)(6 + k) * n + i] = (float)W[k];
+            float h, l;
+            split_df(P[k], h, l);
+            XF[(size_t)k * n + i] = h;
+            XF[(size_t)(3 + k) * n + i] = l;
+            split_df(U[k], h, l);
+            XF[(size_t)(6 + k) * n + i] = h;
+            XF[(size_t)(9 + k) * n + i] = l;
+            split_df(W[k], h, l);
+            XF[(size_t)(12 + k) * n + i] = h;
+            XF[(size_t)(15 + k) * n + i] = l;
         }
-        if (D == 3) XF[(size_t)9 * n + i] = (float)uv[2];
+        if (D == 3) {
+            float h, l;
+            split_df(uv[2], h, l);
+            XF[(size_t)18 * n + i] = h;
+            XF[(size_t)19 * n + i] = l;
+        }
     }
 }
 
@@ -178,6 +204,8 @@ struct ValueWindowParams {
     int sphere;
     int x_f64;
     int u_f64;
+    int df;           // (hi, lo) records: input rounding is u^2, not u
+    int l_only;       // value depends on du_L only, computed with a compensated dot product
     double inv_step;  // value bins: 1/step
     double neg_f_inv; // -first/step
 };
@@ -191,10 +219,12 @@ __global__ void k_value_windows(const double* __restrict__ row_key_lo, ValueWind
     for (int b = threadIdx.x; b < p.nd + 2; b += blockDim.x) {
         if (b == 0 || b == p.nd + 1) { out[b] = 3.0e38f; continue; }
         const double rlo = sqrt(fmax(row_key_lo[b], 0.0));
-        const double pos_err = (p.x_f64 || p.sphere) ? 2.0 * sqrt((double)p.D) * M * u32 : 0.0;
-        const double eps_dir = (rlo > 0.0 ? pos_err / rlo : (pos_err > 0.0 ? 1e30 : 0.0)) + (p.D + 8) * u32;
+        const double rin = p.df ? u32 * u32 : u32;  // rounding of the stored inputs
+        const double pos_err = (p.x_f64 || p.sphere) ? 2.0 * sqrt((double)p.D) * M * rin : 0.0;
+        const double arith = p.l_only ? 0.0 : (p.D + 8) * u32;  // relative part handled per pair when l_only
+        const double eps_dir = (rlo > 0.0 ? pos_err / rlo : (pos_err > 0.0 ? 1e30 : 0.0)) + arith;
         const double U2 = 2.0 * sqrt(3.0) * U;
-        const double eps_L = U2 * eps_dir + (p.u_f64 ? 2.0 * sqrt(3.0) * U * u32 : 0.0) + U2 * 8.0 * u32;
+        const double eps_L = U2 * eps_dir + (p.u_f64 ? 2.0 * sqrt(3.0) * U * rin : 0.0) + (p.l_only ? 0.0 : U2 * 8.0 * u32);
         double scale = 1.0;
         for (int k = 1; k < p.order; ++k) scale *= U2;
         const double wv = 4.0 * (p.order > 0 ? p.order : 1) * scale * eps_L;
