@@ -147,6 +147,7 @@ typedef struct {
     int32_t blocks;         /* persistent blocks launched */
     int32_t threads;        /* threads per block */
     int32_t kernel_launches;/* kernels launched by the last run */
+    int32_t privatization;  /* histogram privatization depth used (-1: joint kernel) */
 } sfb200_stats;
 
 typedef struct sfb200_ctx sfb200_ctx;
@@ -185,8 +186,11 @@ SFB200_API int sfb200_run(sfb200_plan* plan, const void* x, const void* u, int64
 /* Statistics of the last sfb200_run on this plan. */
 SFB200_API int sfb200_plan_last_stats(const sfb200_plan* plan, sfb200_stats* out);
 
-/* Autotuner override (0 = automatic): tile size, threads per block, blocks per SM. */
-SFB200_API int sfb200_plan_set_launch(sfb200_plan* plan, int tile, int threads, int blocks_per_sm);
+/* Autotuner override of the 1D kernels' launch: tile size (points per tile = threads per block; 0 =
+ * automatic), histogram privatization depth (-1 = automatic; 0 = one warp-aggregated histogram per
+ * warp; 1, 4, 8 = copies per warp updated with shared-memory atomics; 32 = one column per lane), and a
+ * cap on resident blocks per SM (0 = occupancy limit). */
+SFB200_API int sfb200_plan_set_launch(sfb200_plan* plan, int tile, int privatization, int blocks_per_sm);
 
 #ifdef __cplusplus
 }

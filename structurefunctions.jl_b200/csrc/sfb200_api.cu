@@ -69,7 +69,7 @@ struct sfb200_plan {
     std::vector<unsigned long long> h_counts;
     sfb200_stats stats{};
     bool stats_pending = false;
-    int tile_ovr = 0, threads_ovr = 0, bps_ovr = 0;
+    int tile_ovr = 0, priv_ovr = -1, bps_ovr = 0;
 };
 
 // ------------------------------------------------------------------------------- errors
@@ -523,7 +523,8 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
 
     // the kernel exists for this combination
     KernelChoice kc = p->joint ? pick_joint(p->sphere, p->D, p->mixed, true, p->df, p->opl)
-                               : (p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl) : pick_flat1d(p->D, p->mixed, p->df, p->opl));
+                               : (p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, 0)
+                                            : pick_flat1d(p->D, p->mixed, p->df, p->opl, 0));
     if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this operator on the joint mixed path");
     return SFB200_OK;
 }
@@ -558,18 +559,19 @@ extern "C" int sfb200_plan_output_sizes(const sfb200_plan* p, int64_t* n_sums, i
     return SFB200_OK;
 }
 
-extern "C" int sfb200_plan_set_launch(sfb200_plan* p, int tile, int threads, int blocks_per_sm)
+extern "C" int sfb200_plan_set_launch(sfb200_plan* p, int tile, int privatization, int blocks_per_sm)
 {
     if (!p) return SFB200_ERR_INVALID_ARG;
     sfb200_ctx* ctx = p->ctx;
-    if (tile != 0 && tile != 64 && tile != 128 && tile != 256 && tile != 512)
-        return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile must be 0, 64, 128, 256 or 512");
-    if (threads != 0 && threads != tile)
-        return set_err(ctx, SFB200_ERR_INVALID_ARG, "threads per block equal the tile size");
+    if (tile != 0 && tile != 32 && tile != 64 && tile != 128 && tile != 256 && tile != 512)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile must be 0, 32, 64, 128, 256 or 512");
+    if (privatization != -1 && privatization != 0 && privatization != 1 && privatization != 4 &&
+        privatization != 8 && privatization != 32)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "privatization must be -1 (auto), 0, 1, 4, 8 or 32");
     if (blocks_per_sm < 0 || blocks_per_sm > 32)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "blocks_per_sm must be in 0..32");
     p->tile_ovr = tile;
-    p->threads_ovr = threads;
+    p->priv_ovr = privatization;
     p->bps_ovr = blocks_per_sm;
     return SFB200_OK;
 }
@@ -610,7 +612,20 @@ static void launch_pack(sfb200_plan* p, const void* x, const void* u, int n, cud
                                                 p->d_aux + 1);
 }
 
-static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_hist)
+// Host mirror of BlockHist<R, NV, PRIV>::bytes (sfb200_acc.cuh).
+static size_t hist_bytes(bool fp32, int NV, int priv, int NW, int NBP)
+{
+    const size_t rs = fp32 ? 4 : 8;
+    size_t b;
+    if (priv == 0) {
+        b = (size_t)NW * NV * NBP * rs * (fp32 ? 2 : 1) + (size_t)NW * NBP * (fp32 ? 4 : 8);
+    } else {
+        b = (size_t)NV * NBP * 8 + (size_t)NBP * 8 + (size_t)NW * NV * NBP * priv * rs + (size_t)NW * NBP * priv * 4;
+    }
+    return (b + 15) & ~(size_t)15;
+}
+
+static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_hist, int priv)
 {
     const int NW = T / 32, NBP = p->nb + 2, NV = p->nops_pad;
     if (p->joint) {
@@ -624,10 +639,17 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
     }
     if (!p->mixed) {
         const int nx = p->sphere ? 8 : p->D;
-        return (size_t)lut_bytes + (size_t)(nx + p->D) * T * 8 + (size_t)NW * NV * NBP * 8 + (size_t)NW * NBP * 8;
+        return (size_t)lut_bytes + (size_t)(nx + p->D) * T * 8 + hist_bytes(false, NV, priv, NW, NBP);
     }
     const int nx = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 4 : 2) * p->D;
-    return (size_t)lut_bytes + (size_t)nx * T * 4 + (size_t)NW * NV * NBP * 8 + (size_t)NW * NBP * 4;
+    return (size_t)lut_bytes + (((size_t)nx * T * 4 + 15) & ~(size_t)15) + hist_bytes(true, NV, priv, NW, NBP);
+}
+
+// Autotuner default for the histogram privatization depth (overridable per plan).
+static int default_privatization(const sfb200_plan* p)
+{
+    (void)p;
+    return 0;
 }
 
 static long long tile_pairs(long long n, int T)
@@ -713,20 +735,23 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         size_t smem;
         int dev_smem_max = 0;
         CK(cudaDeviceGetAttribute(&dev_smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+        int flush_every = 0;
         if (p->joint) {
             T = p->tile_ovr ? p->tile_ovr : (n >= 32768 ? 512 : (n >= 4096 ? 256 : 64));
-            smem = smem_bytes(p, T, lut_bytes, true);
+            smem = smem_bytes(p, T, lut_bytes, true, 0);
             if (smem > (size_t)dev_smem_max) {
                 if (p->mixed)
                     return set_err(ctx, SFB200_ERR_UNSUPPORTED,
                                    "joint histogram of %d x %d cells does not fit shared memory on the mixed path; use fp64",
                                    p->nb, p->nv);
                 smem_hist = false;
-                smem = smem_bytes(p, T, lut_bytes, false);
+                smem = smem_bytes(p, T, lut_bytes, false, 0);
             }
             kc = pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->df, p->opl);
         } else {
-            kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl) : pick_flat1d(p->D, p->mixed, p->df, p->opl);
+            const int want = p->priv_ovr >= 0 ? p->priv_ovr : default_privatization(p);
+            kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, want)
+                           : pick_flat1d(p->D, p->mixed, p->df, p->opl, want);
             if (p->tile_ovr) {
                 T = p->tile_ovr;
             } else {
@@ -736,14 +761,16 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
                 }
             }
             if (T > kc.max_threads) T = kc.max_threads;
-            smem = smem_bytes(p, T, lut_bytes, true);
-            while (smem > (size_t)dev_smem_max && T > 64) {
+            smem = smem_bytes(p, T, lut_bytes, true, kc.priv);
+            while (smem > (size_t)dev_smem_max && T > 32) {
                 T /= 2;
-                smem = smem_bytes(p, T, lut_bytes, true);
+                smem = smem_bytes(p, T, lut_bytes, true, kc.priv);
             }
             if (smem > (size_t)dev_smem_max)
                 return set_err(ctx, SFB200_ERR_UNSUPPORTED, "%d bins x %d operators do not fit shared memory",
                                p->nb, p->nops);
+            // FP32 copies are folded into FP64 before any lane-bin cell can hold more than ~512 terms
+            if (kc.priv > 0) flush_every = p->mixed ? std::max(1, 512 * kc.priv / (32 * T)) : 64;
         }
         if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this plan");
         CK(cudaFuncSetAttribute(kc.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -778,6 +805,7 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         a.vedges = p->d_vedges;
         a.n_vedges = p->joint ? p->desc.value.n_edges : 0;
         a.vwin = p->d_vwin;
+        a.flush_every = flush_every;
         // per-pair relative value error: compensated du_L carries ~(6 order + 6) u; otherwise only
         // the rounding of t itself (the rest is in the per-row absolute window)
         a.vrel = (float)((p->l_only ? (6.0 * p->vorder + 6.0) * 1.25 : 4.0) * 0x1p-24);
@@ -793,6 +821,7 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         CK(cudaGetLastError());
         p->stats.tile = T;
         p->stats.threads = T;
+        p->stats.privatization = p->joint ? -1 : kc.priv;
         p->stats.blocks = (int)grid;
         p->stats_pending = true;
     }

@@ -26,12 +26,13 @@ enum OpListId : int {
 struct KernelChoice {
     const void* fn;   // kernel entry
     int max_threads;  // launch bound
+    int priv;         // histogram privatization depth the kernel was built with (1D kernels)
 };
 
 // Kernel lookup: returns nullptr fn for an unsupported combination. `df`: FP32 records carry
 // (hi, lo) pairs because an input is FP64.
-KernelChoice pick_flat1d(int D, bool mixed, bool df, int opl);
-KernelChoice pick_sphere1d(int D, bool mixed, int opl);
+KernelChoice pick_flat1d(int D, bool mixed, bool df, int opl, int priv);
+KernelChoice pick_sphere1d(int D, bool mixed, int opl, int priv);
 KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, bool df, int opl);
 
 }  // namespace sfb

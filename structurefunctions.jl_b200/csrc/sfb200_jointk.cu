@@ -7,20 +7,20 @@ namespace sfb {
 template <bool SPHERE, int D>
 static KernelChoice joint_fp64(bool smem)
 {
-    if (smem) return {reinterpret_cast<const void*>(&k_joint_fp64<SPHERE, D, true>), 512};
-    return {reinterpret_cast<const void*>(&k_joint_fp64<SPHERE, D, false>), 512};
+    if (smem) return {reinterpret_cast<const void*>(&k_joint_fp64<SPHERE, D, true>), 512, 0};
+    return {reinterpret_cast<const void*>(&k_joint_fp64<SPHERE, D, false>), 512, 0};
 }
 
 template <bool SPHERE, int D, bool DF>
 static KernelChoice joint_mixed(int opl)
 {
     switch (opl) {
-    case OPL_L1: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_L1>>), 512};
-    case OPL_L2: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_L2>>), 512};
-    case OPL_L3: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_L3>>), 512};
-    case OPL_GEN1: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_GEN>>), 512};
+    case OPL_L1: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_L1>>), 512, 0};
+    case OPL_L2: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_L2>>), 512, 0};
+    case OPL_L3: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_L3>>), 512, 0};
+    case OPL_GEN1: return {reinterpret_cast<const void*>(&k_joint_mixed<SPHERE, D, DF, DF, OpList<OC_GEN>>), 512, 0};
     }
-    return {nullptr, 0};
+    return {nullptr, 0, 0};
 }
 
 KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, bool df, int opl)

@@ -14,18 +14,16 @@
 // ti*T + t in registers, the J tile is staged in shared memory and broadcast, so each thread walks
 // the T pairs of its row. Diagonal tiles keep j > i only.
 //
-// Accumulation: each warp owns a private histogram in shared memory (rows 0..nb+1; rows 0 and nb+1
-// collect out-of-range pairs and are dropped). Per pair step the warp groups its 32 lanes by bin
-// with __match_any_sync, reduces each group's values with a shuffle tree, and the group leader adds
-// the sum and the group size into the warp's histogram. Leaders of one step hold distinct bins and a
-// histogram belongs to one warp, so the update needs no atomics. FP32 kernels keep each bin as an
-// FP32 (hi, lo) two-sum pair; at the end every block merges its warps' histograms in FP64 and adds
-// them to the global FP64 sums / uint64 counts with one atomic per bin.
+// Accumulation (sfb200_acc.cuh): per-warp private histograms in shared memory at a selectable
+// privatization depth -- warp-aggregated (__match_any_sync + shuffle tree, leader update, FP32
+// two-sum cells) or C copies per warp up to one column per lane -- merged per block in FP64 and
+// added to the global FP64 sums / uint64 counts with one atomic per bin.
 #pragma once
 
 #include "sfb200_common.cuh"
 #include "sfb200_exact.cuh"
 #include "sfb200_ops.cuh"
+#include "sfb200_acc.cuh"
 
 namespace sfb {
 
@@ -56,6 +54,7 @@ struct PairArgs {
     const float* vwin; // per distance row: absolute half-width of the value ambiguity window in
                        // value-bin index units (mixed)
     float vrel;        // relative half-width: window += (|t| + |first/step|) * vrel
+    int flush_every;   // privatized histograms: fold copies into FP64 every this many tile pairs
     GenOps gen;
     double* g_sums;
     unsigned long long* g_counts;
@@ -104,30 +103,27 @@ __device__ __forceinline__ int value_exact_bin(const PairArgs& a, double v)
 // ================================================================================================
 // Flat (Euclidean) 1D, FP64
 // ================================================================================================
-template <int D, class OPS>
+template <int D, class OPS, int PRIV>
 __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
 {
     constexpr int NV = OPS::n;
     using Needs = ListNeeds<OPS>;
+    using Hist = BlockHist<double, NV, PRIV>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int NBP = a.nb + 2;
     const int n = a.n;
     LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
     double* sx = reinterpret_cast<double*>(smem + a.lut_bytes);
     double* su = sx + D * T;
-    double* hs = su + D * T;
-    unsigned long long* hc = reinterpret_cast<unsigned long long*>(hs + NW * NV * NBP);
-
+    Hist hist;
+    hist.init(reinterpret_cast<unsigned char*>(su + D * T), NW, a.nb + 2);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
-    for (int k = threadIdx.x; k < NW * NV * NBP; k += T) hs[k] = 0.0;
-    for (int k = threadIdx.x; k < NW * NBP; k += T) hc[k] = 0ull;
-    double* whs = hs + warp * NV * NBP;
-    unsigned long long* whc = hc + warp * NBP;
 
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+    int iter = 0;
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
         const int i = ti * T + threadIdx.x;
@@ -159,7 +155,7 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
                 du[d] = su[d * T + jj] - ui[d];
             }
             // r^2 exactly as the reference: left-to-right, no contraction (decides the bin)
-            double h2 = SFB_ADD(SFB_MUL(dx[0], dx[0]), SFB_MUL(dx[1], dx[1]));
+            const double h2 = SFB_ADD(SFB_MUL(dx[0], dx[0]), SFB_MUL(dx[1], dx[1]));
             double r2 = h2;
             if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
             int bin;
@@ -186,30 +182,10 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
             }
             double v[NV];
             eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
-
-            const unsigned peers = __match_any_sync(FULL, key);
-            reduce_peers<NV>(peers, lane, v);
-            if (lane == __ffs(peers) - 1) {
-                whc[key] += (unsigned long long)__popc(peers);
-#pragma unroll
-                for (int o = 0; o < NV; ++o) whs[o * NBP + key] += v[o];
-            }
-            __syncwarp();
+            hist.add(key, v, lane, warp);
         }
     }
-    __syncthreads();
-    // only the caller's operators are written out (NV may include padding of the generic kernels)
-    for (int k = threadIdx.x; k < min(NV, a.nops) * a.nb; k += T) {
-        const int o = k / a.nb, b = k - o * a.nb + 1;
-        double s = 0.0;
-        for (int w = 0; w < NW; ++w) s += hs[(w * NV + o) * NBP + b];
-        if (s != 0.0) atomicAdd(&a.g_sums[(size_t)o * a.nb + b - 1], s);
-    }
-    for (int b = threadIdx.x + 1; b <= a.nb; b += T) {
-        unsigned long long c = 0;
-        for (int w = 0; w < NW; ++w) c += hc[w * NBP + b];
-        if (c) atomicAdd(&a.g_counts[b - 1], c);
-    }
+    hist.merge(a.g_sums, a.g_counts, a.nops, a.nb);
 }
 
 // ================================================================================================
@@ -227,37 +203,32 @@ __device__ __forceinline__ float df_diff(const float* s, int c, int D, int T, in
     else return __fsub_rn(s[c * T + jj], a[c]);
 }
 
-template <int D, bool DFX, bool DFU, class OPS>
+template <int D, bool DFX, bool DFU, class OPS, int PRIV>
 __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
 {
     constexpr int NV = OPS::n;
     constexpr int NXF = DFX ? 2 * D : D;
     constexpr int NUF = DFU ? 2 * D : D;
     using Needs = ListNeeds<OPS>;
+    using Hist = BlockHist<float, NV, PRIV>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int NBP = a.nb + 2;
     const int n = a.n;
     LutEntry32* lut = reinterpret_cast<LutEntry32*>(smem);
     float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);
     float* su = sx + NXF * T;
-    float* hhi = su + NUF * T;                  // NW * NV * NBP
-    float* hlo = hhi + NW * NV * NBP;           // NW * NV * NBP
-    unsigned* hc = reinterpret_cast<unsigned*>(hlo + NW * NV * NBP);  // NW * NBP
     __shared__ unsigned long long s_recheck;
-
+    Hist hist;
+    hist.init(smem + a.lut_bytes + (((size_t)(NXF + NUF) * T * 4 + 15) & ~(size_t)15), NW, a.nb + 2);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry32); k += T)
         lut[k] = static_cast<const LutEntry32*>(a.lut)[k];
-    for (int k = threadIdx.x; k < NW * NV * NBP; k += T) { hhi[k] = 0.f; hlo[k] = 0.f; }
-    for (int k = threadIdx.x; k < NW * NBP; k += T) hc[k] = 0u;
     if (threadIdx.x == 0) s_recheck = 0ull;
-    float* whi = hhi + warp * NV * NBP;
-    float* wlo = hlo + warp * NV * NBP;
-    unsigned* whc = hc + warp * NBP;
     unsigned long long my_recheck = 0;
 
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+    int iter = 0;
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
         const int i = ti * T + threadIdx.x;
@@ -354,33 +325,11 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
                 if (lane == 0) my_recheck += __popc(sb);
             }
             const int key = valid ? bin : a.nb + 1;
-            const unsigned peers = __match_any_sync(FULL, key);
-            reduce_peers<NV>(peers, lane, v);
-            if (lane == __ffs(peers) - 1) {
-                whc[key] += (unsigned)__popc(peers);
-#pragma unroll
-                for (int o = 0; o < NV; ++o) two_sum_acc(whi[o * NBP + key], wlo[o * NBP + key], v[o]);
-            }
-            __syncwarp();
+            hist.add(key, v, lane, warp);
         }
     }
     if (lane == 0 && my_recheck) atomicAdd(&s_recheck, my_recheck);
-    __syncthreads();
-    // only the caller's operators are written out (NV may include padding of the generic kernels)
-    for (int k = threadIdx.x; k < min(NV, a.nops) * a.nb; k += T) {
-        const int o = k / a.nb, b = k - o * a.nb + 1;
-        double s = 0.0;
-        for (int w = 0; w < NW; ++w) {
-            const int idx = (w * NV + o) * NBP + b;
-            s += (double)hhi[idx] + (double)hlo[idx];
-        }
-        if (s != 0.0) atomicAdd(&a.g_sums[(size_t)o * a.nb + b - 1], s);
-    }
-    for (int b = threadIdx.x + 1; b <= a.nb; b += T) {
-        unsigned long long c = 0;
-        for (int w = 0; w < NW; ++w) c += hc[w * NBP + b];
-        if (c) atomicAdd(&a.g_counts[b - 1], c);
-    }
+    hist.merge(a.g_sums, a.g_counts, a.nops, a.nb);
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 
@@ -394,30 +343,27 @@ __device__ __forceinline__ void load_sph64(const double* X, int n, int i, SphPoi
     P.N[0] = X[(size_t)5 * n + i]; P.N[1] = X[(size_t)6 * n + i]; P.N[2] = X[(size_t)7 * n + i];
 }
 
-template <int D, class OPS>
+template <int D, class OPS, int PRIV>
 __global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
 {
     constexpr int NV = OPS::n;
     constexpr int NX = 8;  // p(3), E(2), N(3)
+    using Hist = BlockHist<double, NV, PRIV>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int NBP = a.nb + 2;
     const int n = a.n;
     LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
     double* sx = reinterpret_cast<double*>(smem + a.lut_bytes);  // NX * T
     double* su = sx + NX * T;                                     // D * T
-    double* hs = su + D * T;
-    unsigned long long* hc = reinterpret_cast<unsigned long long*>(hs + NW * NV * NBP);
-
+    Hist hist;
+    hist.init(reinterpret_cast<unsigned char*>(su + D * T), NW, a.nb + 2);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
-    for (int k = threadIdx.x; k < NW * NV * NBP; k += T) hs[k] = 0.0;
-    for (int k = threadIdx.x; k < NW * NBP; k += T) hc[k] = 0ull;
-    double* whs = hs + warp * NV * NBP;
-    unsigned long long* whc = hc + warp * NBP;
 
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+    int iter = 0;
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
         const int i = ti * T + threadIdx.x;
@@ -460,29 +406,10 @@ __global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
             if constexpr (D == 3) Q = fma(du[2], du[2], Q);
             double v[NV];
             eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
-            const unsigned peers = __match_any_sync(FULL, key);
-            reduce_peers<NV>(peers, lane, v);
-            if (lane == __ffs(peers) - 1) {
-                whc[key] += (unsigned long long)__popc(peers);
-#pragma unroll
-                for (int o = 0; o < NV; ++o) whs[o * NBP + key] += v[o];
-            }
-            __syncwarp();
+            hist.add(key, v, lane, warp);
         }
     }
-    __syncthreads();
-    // only the caller's operators are written out (NV may include padding of the generic kernels)
-    for (int k = threadIdx.x; k < min(NV, a.nops) * a.nb; k += T) {
-        const int o = k / a.nb, b = k - o * a.nb + 1;
-        double s = 0.0;
-        for (int w = 0; w < NW; ++w) s += hs[(w * NV + o) * NBP + b];
-        if (s != 0.0) atomicAdd(&a.g_sums[(size_t)o * a.nb + b - 1], s);
-    }
-    for (int b = threadIdx.x + 1; b <= a.nb; b += T) {
-        unsigned long long c = 0;
-        for (int w = 0; w < NW; ++w) c += hc[w * NBP + b];
-        if (c) atomicAdd(&a.g_counts[b - 1], c);
-    }
+    hist.merge(a.g_sums, a.g_counts, a.nops, a.nb);
 }
 
 // ================================================================================================
@@ -499,35 +426,30 @@ __global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
 // (|s| -> 0). Coincident, antipodal and near-edge pairs are recomputed with the reference frame in
 // FP64.
 // ================================================================================================
-template <int D, class OPS>
+template <int D, class OPS, int PRIV>
 __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
 {
     constexpr int NV = OPS::n;
     using Needs = ListNeeds<OPS>;
+    using Hist = BlockHist<float, NV, PRIV>;
     constexpr int NF = (D == 3) ? 20 : 18;  // (hi, lo) of p(3), U(3), W(3)[, up]
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int NBP = a.nb + 2;
     const int n = a.n;
     LutEntry32* lut = reinterpret_cast<LutEntry32*>(smem);
     float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);  // NF * T
-    float* hhi = sx + NF * T;
-    float* hlo = hhi + NW * NV * NBP;
-    unsigned* hc = reinterpret_cast<unsigned*>(hlo + NW * NV * NBP);
     __shared__ unsigned long long s_recheck;
-
+    Hist hist;
+    hist.init(smem + a.lut_bytes + (((size_t)NF * T * 4 + 15) & ~(size_t)15), NW, a.nb + 2);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry32); k += T)
         lut[k] = static_cast<const LutEntry32*>(a.lut)[k];
-    for (int k = threadIdx.x; k < NW * NV * NBP; k += T) { hhi[k] = 0.f; hlo[k] = 0.f; }
-    for (int k = threadIdx.x; k < NW * NBP; k += T) hc[k] = 0u;
     if (threadIdx.x == 0) s_recheck = 0ull;
-    float* whi = hhi + warp * NV * NBP;
-    float* wlo = hlo + warp * NV * NBP;
-    unsigned* whc = hc + warp * NBP;
     unsigned long long my_recheck = 0;
 
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+    int iter = 0;
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
         const int i = ti * T + threadIdx.x;
@@ -591,9 +513,9 @@ __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
                     ok = x_sphere_frame(A, B, a.radius, r, tA, tB);
                     bin = sphere_exact_bin(a, r);
 #pragma unroll
-                    for (int d = 0; d < D; ++d) {
-                        uA[d] = a.U64[(size_t)d * n + i];
-                        uB[d] = a.U64[(size_t)d * n + j];
+                    for (int dd = 0; dd < D; ++dd) {
+                        uA[dd] = a.U64[(size_t)dd * n + i];
+                        uB[dd] = a.U64[(size_t)dd * n + j];
                     }
                     x_sphere_delta<D>(tA, tB, uA, uB, du);
                     double Q64 = du[0] * du[0] + du[1] * du[1];
@@ -607,33 +529,11 @@ __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
                 if (lane == 0) my_recheck += __popc(sb);
             }
             const int key = (valid && ok) ? bin : a.nb + 1;
-            const unsigned peers = __match_any_sync(FULL, key);
-            reduce_peers<NV>(peers, lane, v);
-            if (lane == __ffs(peers) - 1) {
-                whc[key] += (unsigned)__popc(peers);
-#pragma unroll
-                for (int o = 0; o < NV; ++o) two_sum_acc(whi[o * NBP + key], wlo[o * NBP + key], v[o]);
-            }
-            __syncwarp();
+            hist.add(key, v, lane, warp);
         }
     }
     if (lane == 0 && my_recheck) atomicAdd(&s_recheck, my_recheck);
-    __syncthreads();
-    // only the caller's operators are written out (NV may include padding of the generic kernels)
-    for (int k = threadIdx.x; k < min(NV, a.nops) * a.nb; k += T) {
-        const int o = k / a.nb, b = k - o * a.nb + 1;
-        double s = 0.0;
-        for (int w = 0; w < NW; ++w) {
-            const int idx = (w * NV + o) * NBP + b;
-            s += (double)hhi[idx] + (double)hlo[idx];
-        }
-        if (s != 0.0) atomicAdd(&a.g_sums[(size_t)o * a.nb + b - 1], s);
-    }
-    for (int b = threadIdx.x + 1; b <= a.nb; b += T) {
-        unsigned long long c = 0;
-        for (int w = 0; w < NW; ++w) c += hc[w * NBP + b];
-        if (c) atomicAdd(&a.g_counts[b - 1], c);
-    }
+    hist.merge(a.g_sums, a.g_counts, a.nops, a.nb);
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 

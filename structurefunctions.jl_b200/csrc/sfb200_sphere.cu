@@ -4,35 +4,47 @@
 
 namespace sfb {
 
-template <int D, bool MIXED, class OPS>
-static KernelChoice sphere_entry()
+template <int D, bool MIXED, class OPS, int PRIV>
+static KernelChoice sphere_kernel()
 {
-    if constexpr (MIXED) return {reinterpret_cast<const void*>(&k_sphere1d_mixed<D, OPS>), 256};
-    else return {reinterpret_cast<const void*>(&k_sphere1d_fp64<D, OPS>), 256};
+    if constexpr (MIXED) return {reinterpret_cast<const void*>(&k_sphere1d_mixed<D, OPS, PRIV>), 256, PRIV};
+    else return {reinterpret_cast<const void*>(&k_sphere1d_fp64<D, OPS, PRIV>), 256, PRIV};
+}
+
+template <int D, bool MIXED, class OPS, bool ALL>
+static KernelChoice sphere_entry(int priv)
+{
+    switch (priv) {
+    case 32: return sphere_kernel<D, MIXED, OPS, 32>();
+    case 8: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 8>(); break;
+    case 4: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 4>(); break;
+    case 1: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 1>(); break;
+    }
+    return sphere_kernel<D, MIXED, OPS, 0>();
 }
 
 template <int D, bool MIXED>
-static KernelChoice sphere_by_list(int opl)
+static KernelChoice sphere_by_list(int opl, int priv)
 {
     switch (opl) {
-    case OPL_L2: return sphere_entry<D, MIXED, OpList<OC_L2>>();
-    case OPL_L3: return sphere_entry<D, MIXED, OpList<OC_L3>>();
-    case OPL_L1: return sphere_entry<D, MIXED, OpList<OC_L1>>();
-    case OPL_QUAD: return sphere_entry<D, MIXED, OpList<OC_L2, OC_T2, OC_L3, OC_T3>>();
-    case OPL_GEN1: return sphere_entry<D, MIXED, OpList<OC_GEN>>();
-    case OPL_GEN2: return sphere_entry<D, MIXED, OpList<OC_GEN, OC_GEN>>();
-    case OPL_GEN4: return sphere_entry<D, MIXED, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>>();
+    case OPL_L2: return sphere_entry<D, MIXED, OpList<OC_L2>, true>(priv);
+    case OPL_L3: return sphere_entry<D, MIXED, OpList<OC_L3>, true>(priv);
+    case OPL_L1: return sphere_entry<D, MIXED, OpList<OC_L1>, true>(priv);
+    case OPL_QUAD: return sphere_entry<D, MIXED, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, true>(priv);
+    case OPL_GEN1: return sphere_entry<D, MIXED, OpList<OC_GEN>, false>(priv);
+    case OPL_GEN2: return sphere_entry<D, MIXED, OpList<OC_GEN, OC_GEN>, false>(priv);
+    case OPL_GEN4: return sphere_entry<D, MIXED, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv);
     case OPL_GEN8:
-        return sphere_entry<D, MIXED, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN>>();
+        return sphere_entry<D, MIXED, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv);
     }
-    return {nullptr, 0};
+    return {nullptr, 0, 0};
 }
 
-KernelChoice pick_sphere1d(int D, bool mixed, int opl)
+KernelChoice pick_sphere1d(int D, bool mixed, int opl, int priv)
 {
-    if (D == 2) return mixed ? sphere_by_list<2, true>(opl) : sphere_by_list<2, false>(opl);
-    if (D == 3) return mixed ? sphere_by_list<3, true>(opl) : sphere_by_list<3, false>(opl);
-    return {nullptr, 0};
+    if (D == 2) return mixed ? sphere_by_list<2, true>(opl, priv) : sphere_by_list<2, false>(opl, priv);
+    if (D == 3) return mixed ? sphere_by_list<3, true>(opl, priv) : sphere_by_list<3, false>(opl, priv);
+    return {nullptr, 0, 0};
 }
 
 }  // namespace sfb

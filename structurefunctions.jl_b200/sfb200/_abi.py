@@ -87,6 +87,7 @@ class Stats(C.Structure):
         ("blocks", C.c_int32),
         ("threads", C.c_int32),
         ("kernel_launches", C.c_int32),
+        ("privatization", C.c_int32),
     ]
 
 

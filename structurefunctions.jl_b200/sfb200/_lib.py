@@ -123,8 +123,8 @@ class Plan:
         check(load().sfb200_plan_last_stats(self.ptr, C.byref(st)), self.ctx.ptr)
         return {k: getattr(st, k) for k, _ in _abi.Stats._fields_}
 
-    def set_launch(self, tile=0, threads=0, blocks_per_sm=0):
-        check(load().sfb200_plan_set_launch(self.ptr, tile, threads, blocks_per_sm), self.ctx.ptr)
+    def set_launch(self, tile=0, privatization=-1, blocks_per_sm=0):
+        check(load().sfb200_plan_set_launch(self.ptr, tile, privatization, blocks_per_sm), self.ctx.ptr)
 
     def close(self):
         if self.ptr:

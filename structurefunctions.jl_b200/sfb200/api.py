@@ -71,7 +71,7 @@ class B200Backend:
         if p is None:
             p = _lib.Plan(self.context, desc, keep)
             if self.tile:
-                p.set_launch(self.tile, self.tile, 0)
+                p.set_launch(self.tile, -1, 0)
             self._plans[key] = p
         return p
 

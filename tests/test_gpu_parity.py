@@ -19,12 +19,12 @@ pytestmark = pytest.mark.gpu
 PRECISIONS = [("fp64", TOL_FP64), ("mixed", TOL_MIXED)]
 
 
-def run_gpu(ops, x, u, bins, metric=None, value_bins=None, precision="mixed", tile=0):
+def run_gpu(ops, x, u, bins, metric=None, value_bins=None, precision="mixed", tile=0, priv=None):
     be = SF.B200Backend(precision=precision, tile=tile)
     desc, keep = plan_description(ops, u.shape[0], bins, value_bins, metric, precision, x.dtype, u.dtype)
     plan = _lib.Plan(be.context, desc, keep)
-    if tile:
-        plan.set_launch(tile, tile, 0)
+    if tile or priv is not None:
+        plan.set_launch(tile, -1 if priv is None else priv, 0)
     sums = np.zeros(plan.n_sums)
     counts = np.zeros(plan.n_counts, dtype=np.uint64)
     xa = np.asfortranarray(x)
@@ -150,6 +150,25 @@ def test_joint_sphere(precision, tol):
     vb = SF.LinearBinEdges(-3.0, 3.0, 61)
     check((SF.ProjectedStructureFunctionType(1, 0),), w.x, w.u, w.distance_bins.edges, metric=w.metric,
           value_bins=vb, precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+@pytest.mark.parametrize("priv", [0, 1, 4, 8, 32])
+@pytest.mark.parametrize("tile", [32, 64, 256])
+def test_privatization_modes(precision, tol, priv, tile):
+    """Every histogram privatization depth and tile size gives the oracle's histogram."""
+    w = synthetic.config("c1", n=1500)
+    gs, gc, st = run_gpu(w.ops, w.x, w.u, w.distance_bins.edges, precision=precision, tile=tile, priv=priv)
+    assert st["privatization"] == priv and st["tile"] <= tile
+    rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges)
+    nb = len(w.distance_bins) - 1
+    for k in range(len(w.ops)):
+        compare(gs[k * nb:(k + 1) * nb], gc, rs[k * nb:(k + 1) * nb], rc, ra[k * nb:(k + 1) * nb], tol)
+    ws = synthetic.config("c2", n=700)
+    gs, gc, st = run_gpu(ws.ops, ws.x, ws.u, ws.distance_bins.edges, metric=ws.metric, precision=precision,
+                         tile=tile, priv=priv)
+    rs, rc, ra = run_oracle(ws.ops, ws.x, ws.u, ws.distance_bins.edges, metric=ws.metric)
+    compare(gs, gc, rs, rc, ra, tol)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
