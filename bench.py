@@ -45,7 +45,39 @@ def parse():
     ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample length")
+    ap.add_argument("--profile", type=int, default=0, metavar="N",
+                    help="profiling case: run the pair kernels of --config on its first N points (a warm-up "
+                         "run then two runs per precision) and exit; sized for ncu captures")
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     return ap.parse_args()
+
+
+def run_profile_case(args):
+    """Small, self-contained case for ncu: no timing output, a handful of launches."""
+    import torch
+
+    from sfb200 import _abi, _lib, synthetic
+    from sfb200.api import plan_description
+
+    w = synthetic.config(args.config, n=args.profile)
+    ctx = _lib.Context(0)
+    xd = torch.from_numpy(np.ascontiguousarray(w.x.T)).cuda()
+    ud = torch.from_numpy(np.ascontiguousarray(w.u.T)).cuda()
+    precs = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+    for prec in precs:
+        desc, keep = plan_description(w.ops, w.u.shape[0], w.distance_bins, w.value_bins, w.metric, prec,
+                                      w.x.dtype, w.u.dtype)
+        plan = _lib.Plan(ctx, desc, keep)
+        sums = torch.zeros(plan.n_sums, dtype=torch.float64, device="cuda")
+        counts = torch.zeros(plan.n_counts, dtype=torch.int64, device="cuda")
+        flags = _abi.RUN_DEVICE_INPUT | _abi.RUN_DEVICE_OUTPUT
+        for _ in range(3):
+            plan.run(xd.data_ptr(), ud.data_ptr(), w.n, flags, sums.data_ptr(), counts.data_ptr(), ctx.stream)
+        st = plan.stats()
+        print(json.dumps({"profile_case": w.name, "precision": prec, "kernel_ms": st["kernel_ms"],
+                          "tile": st["tile"], "blocks": st["blocks"], "privatization": st["privatization"]}))
+        plan.close()
+    ctx.close()
 
 
 # ------------------------------------------------------------------------------------------ clocks
@@ -379,7 +411,9 @@ def main():
     args = parse()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -20,10 +20,14 @@
 
 namespace sfb {
 
+//   PRIV = 2  warp-aggregated as PRIV = 0, but the group leader adds into the warp's copy with a
+//             shared-memory atomic (no read-modify-write chain on the leader; FP32 cells, folded into
+//             the block FP64 histogram like the copies).
 template <typename R, int NV, int PRIV>
 struct BlockHist {
     static constexpr bool AGG = PRIV == 0;
-    static constexpr int C = PRIV == 0 ? 1 : PRIV;
+    static constexpr bool AGG_RED = PRIV == 2;
+    static constexpr int C = (PRIV == 0 || PRIV == 2) ? 1 : PRIV;
     using CountT = typename std::conditional<AGG && sizeof(R) == 8, unsigned long long, unsigned>::type;
 
     R* hv;          // values: AGG: [warp][o][bin] (+ lo plane for FP32); else [warp][o][bin][copy]
@@ -90,6 +94,15 @@ struct BlockHist {
                 }
             }
             __syncwarp();
+        } else if constexpr (AGG_RED) {
+            const unsigned peers = __match_any_sync(FULL, key);
+            reduce_peers<NV>(peers, lane, v);
+            if (lane == __ffs(peers) - 1) {
+                R* wv = hv + (size_t)warp * NV * NBP;
+#pragma unroll
+                for (int o = 0; o < NV; ++o) atomicAdd(&wv[o * NBP + key], v[o]);
+                atomicAdd(&hc[warp * NBP + key], (unsigned)__popc(peers));
+            }
         } else {
             const int col = (C == 32) ? lane : (lane % C);
             R* wv = hv + (size_t)warp * NV * NBP * C;

@@ -566,7 +566,7 @@ extern "C" int sfb200_plan_set_launch(sfb200_plan* p, int tile, int privatizatio
     if (tile != 0 && tile != 32 && tile != 64 && tile != 128 && tile != 256 && tile != 512)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile must be 0, 32, 64, 128, 256 or 512");
     if (privatization != -1 && privatization != 0 && privatization != 1 && privatization != 4 &&
-        privatization != 8 && privatization != 32)
+        privatization != 8 && privatization != 32 && privatization != 2)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "privatization must be -1 (auto), 0, 1, 4, 8 or 32");
     if (blocks_per_sm < 0 || blocks_per_sm > 32)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "blocks_per_sm must be in 0..32");
@@ -620,7 +620,8 @@ static size_t hist_bytes(bool fp32, int NV, int priv, int NW, int NBP)
     if (priv == 0) {
         b = (size_t)NW * NV * NBP * rs * (fp32 ? 2 : 1) + (size_t)NW * NBP * (fp32 ? 4 : 8);
     } else {
-        b = (size_t)NV * NBP * 8 + (size_t)NBP * 8 + (size_t)NW * NV * NBP * priv * rs + (size_t)NW * NBP * priv * 4;
+        const int C = priv == 2 ? 1 : priv;  // 2: warp-aggregated with leader atomics, one copy
+        b = (size_t)NV * NBP * 8 + (size_t)NBP * 8 + (size_t)NW * NV * NBP * C * rs + (size_t)NW * NBP * C * 4;
     }
     return (b + 15) & ~(size_t)15;
 }
@@ -641,7 +642,8 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
         const int nx = p->sphere ? 8 : p->D;
         return (size_t)lut_bytes + (size_t)(nx + p->D) * T * 8 + hist_bytes(false, NV, priv, NW, NBP);
     }
-    const int nx = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 4 : 2) * p->D;
+    // sphere: NF floats per point; flat: one record of (hi[, lo]) x and u padded to 4 floats
+    const int nx = p->sphere ? (p->D == 3 ? 20 : 18) : ((((p->df ? 4 : 2) * p->D) + 3) & ~3);
     return (size_t)lut_bytes + (((size_t)nx * T * 4 + 15) & ~(size_t)15) + hist_bytes(true, NV, priv, NW, NBP);
 }
 
@@ -770,7 +772,10 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
                 return set_err(ctx, SFB200_ERR_UNSUPPORTED, "%d bins x %d operators do not fit shared memory",
                                p->nb, p->nops);
             // FP32 copies are folded into FP64 before any lane-bin cell can hold more than ~512 terms
-            if (kc.priv > 0) flush_every = p->mixed ? std::max(1, 512 * kc.priv / (32 * T)) : 64;
+            if (kc.priv > 0) {
+                const int copies = kc.priv == 2 ? 1 : kc.priv;
+                flush_every = p->mixed ? std::max(1, 512 * copies / (32 * T)) : 64;
+            }
         }
         if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this plan");
         CK(cudaFuncSetAttribute(kc.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -21,6 +21,7 @@ static KernelChoice flat_entry(int priv)
     case 8: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 8>(); break;
     case 4: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 4>(); break;
     case 1: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 1>(); break;
+    case 2: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 2>(); break;
     }
     return flat_kernel<D, MODE, OPS, 0>();
 }

@@ -203,12 +203,36 @@ __device__ __forceinline__ float df_diff(const float* s, int c, int D, int T, in
     else return __fsub_rn(s[c * T + jj], a[c]);
 }
 
+// The J tile is staged as one record per point, [x_hi(D) u_hi(D) | x_lo(D) u_lo(D)] padded to a
+// multiple of 4 floats, and read with 128-bit broadcast loads: one shared-memory transaction per
+// 4 floats instead of one per component.
+template <int D, bool DF>
+struct FlatRec {
+    static constexpr int NRAW = (DF ? 4 : 2) * D;
+    static constexpr int NR = (NRAW + 3) & ~3;
+};
+
+template <int NR>
+__device__ __forceinline__ void load_rec4(const float* base, float (&r)[NR])
+{
+#pragma unroll
+    for (int q = 0; q < NR / 4; ++q) {
+        const float4 t = reinterpret_cast<const float4*>(base)[q];
+        r[4 * q] = t.x;
+        r[4 * q + 1] = t.y;
+        r[4 * q + 2] = t.z;
+        r[4 * q + 3] = t.w;
+    }
+}
+
 template <int D, bool DFX, bool DFU, class OPS, int PRIV>
 __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
 {
+    static_assert(DFX == DFU, "records carry (hi, lo) for both or neither");
     constexpr int NV = OPS::n;
     constexpr int NXF = DFX ? 2 * D : D;
     constexpr int NUF = DFU ? 2 * D : D;
+    constexpr int NR = FlatRec<D, DFX>::NR;
     using Needs = ListNeeds<OPS>;
     using Hist = BlockHist<float, NV, PRIV>;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -216,11 +240,10 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n = a.n;
     LutEntry32* lut = reinterpret_cast<LutEntry32*>(smem);
-    float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);
-    float* su = sx + NXF * T;
+    float* srec = reinterpret_cast<float*>(smem + a.lut_bytes);  // T records of NR floats
     __shared__ unsigned long long s_recheck;
     Hist hist;
-    hist.init(smem + a.lut_bytes + (((size_t)(NXF + NUF) * T * 4 + 15) & ~(size_t)15), NW, a.nb + 2);
+    hist.init(smem + a.lut_bytes + (size_t)NR * T * 4, NW, a.nb + 2);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry32); k += T)
         lut[k] = static_cast<const LutEntry32*>(a.lut)[k];
     if (threadIdx.x == 0) s_recheck = 0ull;
@@ -242,20 +265,36 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
         const int j0 = tj * T;
         const int jn = min(T, n - j0);
         if ((int)threadIdx.x < jn) {
+            float* rec = srec + (size_t)threadIdx.x * NR;
+            const int jg = j0 + threadIdx.x;
 #pragma unroll
-            for (int c = 0; c < NXF; ++c) sx[c * T + threadIdx.x] = a.XF[(size_t)c * n + j0 + threadIdx.x];
+            for (int d = 0; d < D; ++d) {
+                rec[d] = a.XF[(size_t)d * n + jg];
+                rec[D + d] = a.UF[(size_t)d * n + jg];
+                if constexpr (DFX) {
+                    rec[2 * D + d] = a.XF[(size_t)(D + d) * n + jg];
+                    rec[3 * D + d] = a.UF[(size_t)(D + d) * n + jg];
+                }
+            }
 #pragma unroll
-            for (int c = 0; c < NUF; ++c) su[c * T + threadIdx.x] = a.UF[(size_t)c * n + j0 + threadIdx.x];
+            for (int c = FlatRec<D, DFX>::NRAW; c < NR; ++c) rec[c] = 0.f;
         }
         __syncthreads();
         const bool diag = ti == tj;
         for (int jj = 0; jj < jn; ++jj) {
             const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+            float rj[NR];
+            load_rec4<NR>(srec + (size_t)jj * NR, rj);
             float dx[D], du[D];
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                dx[d] = df_diff<DFX>(sx, d, D, T, jj, xi);
-                du[d] = df_diff<DFU>(su, d, D, T, jj, ui);
+                if constexpr (DFX) {
+                    dx[d] = __fadd_rn(__fsub_rn(rj[d], xi[d]), __fsub_rn(rj[2 * D + d], xi[D + d]));
+                    du[d] = __fadd_rn(__fsub_rn(rj[D + d], ui[d]), __fsub_rn(rj[3 * D + d], ui[D + d]));
+                } else {
+                    dx[d] = __fsub_rn(rj[d], xi[d]);
+                    du[d] = __fsub_rn(rj[D + d], ui[d]);
+                }
             }
             const float h2 = fmaf(dx[1], dx[1], dx[0] * dx[0]);
             float r2 = h2;

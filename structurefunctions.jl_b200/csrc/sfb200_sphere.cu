@@ -19,6 +19,7 @@ static KernelChoice sphere_entry(int priv)
     case 8: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 8>(); break;
     case 4: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 4>(); break;
     case 1: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 1>(); break;
+    case 2: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 2>(); break;
     }
     return sphere_kernel<D, MIXED, OPS, 0>();
 }
