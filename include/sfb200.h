@@ -188,9 +188,25 @@ SFB200_API int sfb200_plan_last_stats(const sfb200_plan* plan, sfb200_stats* out
 
 /* Autotuner override of the 1D kernels' launch: tile size (points per tile = threads per block; 0 =
  * automatic), histogram privatization depth (-1 = automatic; 0 = one warp-aggregated histogram per
- * warp; 1, 4, 8 = copies per warp updated with shared-memory atomics; 32 = one column per lane), and a
- * cap on resident blocks per SM (0 = occupancy limit). */
+ * warp; 2 = warp-aggregated with shared-memory atomics; 3 = per-lane runs added into a block table
+ * of lane columns (the default); 1, 4, 8 = copies per warp updated with shared-memory atomics; 32 =
+ * one column per lane of every warp), and a cap on resident blocks per SM (0 = occupancy limit).
+ * No counterpart in the reference (its GPU backend has no launch knobs). */
 SFB200_API int sfb200_plan_set_launch(sfb200_plan* plan, int tile, int privatization, int blocks_per_sm);
+
+/* Plan options for sfb200_plan_set_option. */
+typedef enum {
+    /* Point storage order on the device: -1 automatic (Morton order from 16384 points), 0 the
+     * caller's order, 1 Morton (Z-curve) order. Results are the same up to the rounding of the
+     * sums (counts are identical); the joint sphere path always keeps the caller's order. */
+    SFB200_OPT_POINT_ORDER = 1,
+    /* Columns of the run-length histogram table (privatization 3): 0 automatic, else 1, 2, 4, 8,
+     * 16 or 32. */
+    SFB200_OPT_HIST_COLUMNS = 2
+} sfb200_option;
+
+/* Set a plan option (autotuning; no counterpart in the reference). */
+SFB200_API int sfb200_plan_set_option(sfb200_plan* plan, int option, int64_t value);
 
 #ifdef __cplusplus
 }

@@ -23,22 +23,39 @@ namespace sfb {
 //   PRIV = 2  warp-aggregated as PRIV = 0, but the group leader adds into the warp's copy with a
 //             shared-memory atomic (no read-modify-write chain on the leader; FP32 cells, folded into
 //             the block FP64 histogram like the copies).
+//   PRIV = 3  run-length: every lane keeps its current bin, one running sum per operator and a count
+//             in registers, and only when its bin changes adds the finished run into column
+//             (lane % LC) of a block-wide [o][bin][column] table with shared-memory atomics (LC = 32:
+//             the lanes of one warp hit 32 distinct banks; the atomics only order different warps).
+//             Runs are closed at every tile-pair boundary (a run never holds more than one tile's
+//             terms) and the table is folded into the block FP64 histogram every `flush_every` tile
+//             pairs. With the points in space-filling-curve order, the j of consecutive steps are
+//             neighbours, the pair distance changes little from step to step and most steps extend
+//             the run: the per-pair cost is a compare and one add + select per operator.
 template <typename R, int NV, int PRIV>
 struct BlockHist {
     static constexpr bool AGG = PRIV == 0;
     static constexpr bool AGG_RED = PRIV == 2;
-    static constexpr int C = (PRIV == 0 || PRIV == 2) ? 1 : PRIV;
+    static constexpr bool RUN = PRIV == 3;
+    static constexpr int C = (PRIV == 0 || PRIV == 2 || PRIV == 3) ? 1 : PRIV;
     using CountT = typename std::conditional<AGG && sizeof(R) == 8, unsigned long long, unsigned>::type;
 
-    R* hv;          // values: AGG: [warp][o][bin] (+ lo plane for FP32); else [warp][o][bin][copy]
+    R* hv;          // values: AGG: [warp][o][bin] (+ lo plane for FP32); RUN: [o][bin][column];
+                    // else [warp][o][bin][copy]
     R* hlo;         // AGG FP32 only
-    CountT* hc;     // counts: AGG: [warp][bin]; else [warp][bin][copy]
+    CountT* hc;     // counts: AGG: [warp][bin]; RUN: [bin][column]; else [warp][bin][copy]
     double* sblk;   // !AGG: block FP64 values [o][bin]
     unsigned long long* scnt;  // !AGG: block counts [bin]
     int NBP, NW;
+    int LC;         // RUN: table columns (power of two <= 32)
+    // RUN: the lane's open run
+    int rkey;
+    unsigned rc;
+    R rs[NV];
 
-    // Bytes of shared memory this accumulator needs (mirrored on the host by hist_bytes()).
-    static __host__ __device__ size_t bytes(int NW_, int NBP_)
+    // Bytes of shared memory this accumulator needs (mirrored on the host by hist_bytes()); `lc` is
+    // the RUN table's column count.
+    static __host__ __device__ size_t bytes(int NW_, int NBP_, int lc = 32)
     {
         if (AGG) {
             size_t b = (size_t)NW_ * NV * NBP_ * sizeof(R) * (sizeof(R) == 4 ? 2 : 1);
@@ -46,17 +63,32 @@ struct BlockHist {
             return (b + 15) & ~(size_t)15;
         }
         size_t b = (size_t)NV * NBP_ * 8 + (size_t)NBP_ * 8;  // sblk, scnt (8-byte aligned first)
+        if (RUN) {
+            b += (size_t)NV * NBP_ * lc * sizeof(R) + (size_t)NBP_ * lc * sizeof(unsigned);
+            return (b + 15) & ~(size_t)15;
+        }
         b += (size_t)NW_ * NV * NBP_ * C * sizeof(R);
         b += (size_t)NW_ * NBP_ * C * sizeof(unsigned);
         return (b + 15) & ~(size_t)15;
     }
 
-    __device__ void init(unsigned char* base, int NW_, int NBP_)
+    __device__ void init(unsigned char* base, int NW_, int NBP_, int lc = 32)
     {
         NW = NW_;
         NBP = NBP_;
+        LC = lc;
         const int T = blockDim.x;
-        if constexpr (AGG) {
+        if constexpr (RUN) {
+            sblk = reinterpret_cast<double*>(base);
+            scnt = reinterpret_cast<unsigned long long*>(sblk + (size_t)NV * NBP);
+            hv = reinterpret_cast<R*>(scnt + NBP);
+            hc = reinterpret_cast<CountT*>(hv + (size_t)NV * NBP * LC);
+            for (int k = threadIdx.x; k < NV * NBP; k += T) sblk[k] = 0.0;
+            for (int k = threadIdx.x; k < NBP; k += T) scnt[k] = 0ull;
+            for (int k = threadIdx.x; k < NV * NBP * LC; k += T) hv[k] = R(0);
+            for (int k = threadIdx.x; k < NBP * LC; k += T) hc[k] = 0u;
+            open_empty();
+        } else if constexpr (AGG) {
             hv = reinterpret_cast<R*>(base);
             hlo = hv + (size_t)NW * NV * NBP;
             hc = reinterpret_cast<CountT*>(hv + (size_t)NW * NV * NBP * (sizeof(R) == 4 ? 2 : 1));
@@ -74,10 +106,45 @@ struct BlockHist {
         }
     }
 
+    // RUN: an empty run on the dropped overflow row, so that the first add may flush it unguarded.
+    __device__ __forceinline__ void open_empty()
+    {
+        rkey = NBP - 1;
+        rc = 0u;
+#pragma unroll
+        for (int o = 0; o < NV; ++o) rs[o] = R(0);
+    }
+
+    // RUN: add the lane's open run into its table column.
+    __device__ __forceinline__ void flush_run(int lane)
+    {
+        const int col = lane & (LC - 1);
+        R* t = hv + (size_t)rkey * LC + col;
+#pragma unroll
+        for (int o = 0; o < NV; ++o) atomicAdd(t + (size_t)o * NBP * LC, rs[o]);
+        atomicAdd(&hc[rkey * LC + col], rc);
+    }
+
+    // RUN: close every lane's run (tile-pair boundary; before a fold or the merge).
+    __device__ __forceinline__ void close_runs(int lane)
+    {
+        if constexpr (RUN) {
+            if (rc) flush_run(lane);
+            open_empty();
+        }
+    }
+
     // One pair step of the warp: every lane adds its values v under bin `key` (all lanes call).
     __device__ __forceinline__ void add(int key, R (&v)[NV], int lane, int warp)
     {
-        if constexpr (AGG) {
+        if constexpr (RUN) {
+            const bool brk = key != rkey;
+            if (brk) flush_run(lane);
+#pragma unroll
+            for (int o = 0; o < NV; ++o) rs[o] = brk ? v[o] : rs[o] + v[o];
+            rc = brk ? 1u : rc + 1u;
+            rkey = key;
+        } else if constexpr (AGG) {
             const unsigned peers = __match_any_sync(FULL, key);
             reduce_peers<NV>(peers, lane, v);
             if (lane == __ffs(peers) - 1) {
@@ -122,7 +189,31 @@ struct BlockHist {
     // Fold the copies into the block FP64 histogram (all threads of the block call; !AGG only).
     __device__ void fold()
     {
-        if constexpr (!AGG) {
+        if constexpr (RUN) {
+            // one warp per table row: lane c reads column c, a shuffle tree sums the row in FP64
+            __syncthreads();
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            for (int r = warp; r < NV * NBP; r += NW) {
+                double s = 0.0;
+                if (lane < LC) {
+                    s = (double)hv[(size_t)r * LC + lane];
+                    hv[(size_t)r * LC + lane] = R(0);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+                if (lane == 0) sblk[r] += s;
+            }
+            for (int b = warp; b < NBP; b += NW) {
+                unsigned c = 0u;
+                if (lane < LC) {
+                    c = hc[b * LC + lane];
+                    hc[b * LC + lane] = 0u;
+                }
+                c = __reduce_add_sync(FULL, c);
+                if (lane == 0) scnt[b] += c;
+            }
+            __syncthreads();
+        } else if constexpr (!AGG) {
             const int T = blockDim.x;
             __syncthreads();
             for (int k = threadIdx.x; k < NV * NBP; k += T) {
@@ -175,6 +266,7 @@ struct BlockHist {
                 if (c) atomicAdd(&g_counts[b - 1], c);
             }
         } else {
+            close_runs(threadIdx.x & 31);
             fold();
             for (int k = threadIdx.x; k < min(NV, nops) * nb; k += T) {
                 const int o = k / nb, b = k - o * nb + 1;

@@ -12,6 +12,8 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "../../include/sfb200.h"
 #include "sfb200_internal.h"
 #include "sfb200_kernels.cuh"
@@ -61,6 +63,12 @@ struct sfb200_plan {
     double* d_U64 = nullptr;
     float* d_XF = nullptr;
     float* d_UF = nullptr;
+    // spatial order: Morton keys and the permutation (double-buffered for the radix sort)
+    unsigned* d_keys = nullptr;   // 2 * cap
+    int* d_perm = nullptr;        // 2 * cap
+    unsigned* d_box = nullptr;    // 6
+    void* d_sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
     long long n_sums = 0, n_counts = 0;
     double* d_sums = nullptr;
     unsigned long long* d_counts = nullptr;
@@ -70,6 +78,9 @@ struct sfb200_plan {
     sfb200_stats stats{};
     bool stats_pending = false;
     int tile_ovr = 0, priv_ovr = -1, bps_ovr = 0;
+    double vq = 1.0, vq_inv = 1.0;  // joint mixed: fixed-point scale of the value offsets
+    int order_ovr = -1;   // -1 auto, 0 caller order, 1 Morton order
+    int cols_ovr = 0;     // run-length histogram columns (0 auto)
 };
 
 // ------------------------------------------------------------------------------- errors
@@ -327,8 +338,14 @@ static void free_workspace(sfb200_plan* p)
 {
     cudaFree(p->d_rawx); cudaFree(p->d_rawu);
     cudaFree(p->d_X64); cudaFree(p->d_U64); cudaFree(p->d_XF); cudaFree(p->d_UF);
+    cudaFree(p->d_keys); cudaFree(p->d_perm); cudaFree(p->d_box); cudaFree(p->d_sort_tmp);
     p->d_rawx = p->d_rawu = nullptr;
     p->d_X64 = p->d_U64 = nullptr;
+    p->d_keys = nullptr;
+    p->d_perm = nullptr;
+    p->d_box = nullptr;
+    p->d_sort_tmp = nullptr;
+    p->sort_tmp_bytes = 0;
     p->d_XF = p->d_UF = nullptr;
     p->cap = 0;
 }
@@ -488,6 +505,23 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         if (d.value.kind == SFB200_BINS_LINEAR) p->vlin = linear_of(d.value);
         else p->vedges.assign(d.value.edges, d.value.edges + d.value.n_edges);
     }
+    if (p->joint && p->mixed) {
+        // fixed-point scale of the value offsets from the bin centres: 2^k with (half width) 2^k < 2^30
+        double hw = 0.0;
+        if (d.value.kind == SFB200_BINS_LINEAR) {
+            hw = 0.5 * d.value.step;
+        } else {
+            for (size_t k = 0; k < p->vedges.size(); ++k)
+                if (!std::isfinite(p->vedges[k]))
+                    return set_err(ctx, SFB200_ERR_UNSUPPORTED,
+                                   "value_bins: infinite edges need precision=fp64 for a joint histogram");
+            for (size_t k = 0; k + 1 < p->vedges.size(); ++k) hw = std::max(hw, 0.5 * (p->vedges[k + 1] - p->vedges[k]));
+        }
+        int ex = 0;
+        if (hw > 0.0 && std::isfinite(hw)) std::frexp(hw, &ex);  // hw < 2^ex
+        p->vq = std::ldexp(1.0, 30 - ex);
+        p->vq_inv = std::ldexp(1.0, ex - 30);
+    }
 
     // device allocations
     cudaError_t e;
@@ -565,15 +599,33 @@ extern "C" int sfb200_plan_set_launch(sfb200_plan* p, int tile, int privatizatio
     sfb200_ctx* ctx = p->ctx;
     if (tile != 0 && tile != 32 && tile != 64 && tile != 128 && tile != 256 && tile != 512)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile must be 0, 32, 64, 128, 256 or 512");
-    if (privatization != -1 && privatization != 0 && privatization != 1 && privatization != 4 &&
-        privatization != 8 && privatization != 32 && privatization != 2)
-        return set_err(ctx, SFB200_ERR_INVALID_ARG, "privatization must be -1 (auto), 0, 1, 4, 8 or 32");
+    if (privatization != -1 && privatization != 0 && privatization != 1 && privatization != 2 &&
+        privatization != 3 && privatization != 4 && privatization != 8 && privatization != 32)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "privatization must be -1 (auto), 0, 1, 2, 3, 4, 8 or 32");
     if (blocks_per_sm < 0 || blocks_per_sm > 32)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "blocks_per_sm must be in 0..32");
     p->tile_ovr = tile;
     p->priv_ovr = privatization;
     p->bps_ovr = blocks_per_sm;
     return SFB200_OK;
+}
+
+extern "C" int sfb200_plan_set_option(sfb200_plan* p, int option, int64_t value)
+{
+    if (!p) return SFB200_ERR_INVALID_ARG;
+    sfb200_ctx* ctx = p->ctx;
+    switch (option) {
+    case SFB200_OPT_POINT_ORDER:
+        if (value < -1 || value > 1) return set_err(ctx, SFB200_ERR_INVALID_ARG, "point order must be -1, 0 or 1");
+        p->order_ovr = (int)value;
+        return SFB200_OK;
+    case SFB200_OPT_HIST_COLUMNS:
+        if (value < 0 || value > 32 || (value & (value - 1)))
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "histogram columns must be 0 (auto) or a power of two <= 32");
+        p->cols_ovr = (int)value;
+        return SFB200_OK;
+    }
+    return set_err(ctx, SFB200_ERR_INVALID_ARG, "unknown plan option %d", option);
 }
 
 // ------------------------------------------------------------------------------- run
@@ -595,30 +647,73 @@ static int ensure_workspace(sfb200_plan* p, long long n)
         CK(cudaMalloc(&p->d_XF, sizeof(float) * nxf * cap));
         if (!p->sphere) CK(cudaMalloc(&p->d_UF, sizeof(float) * (p->df ? 2 : 1) * p->D * cap));
     }
+    CK(cudaMalloc(&p->d_keys, sizeof(unsigned) * 2 * cap));
+    CK(cudaMalloc(&p->d_perm, sizeof(int) * 2 * cap));
+    CK(cudaMalloc(&p->d_box, sizeof(unsigned) * 6));
+    size_t tmp = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, p->d_keys, p->d_keys + cap, p->d_perm, p->d_perm + cap,
+                                       (int)cap, 0, 32, ctx->stream));
+    CK(cudaMalloc(&p->d_sort_tmp, std::max<size_t>(tmp, 16)));
+    p->sort_tmp_bytes = tmp;
     p->cap = cap;
     return SFB200_OK;
 }
 
 template <typename TX, typename TU>
-static void launch_pack(sfb200_plan* p, const void* x, const void* u, int n, cudaStream_t s)
+static void launch_pack(sfb200_plan* p, const void* x, const void* u, int n, const int* perm, cudaStream_t s)
 {
     const int tb = 256, nblk = (n + tb - 1) / tb;
     if (p->sphere)
-        k_pack_sphere<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->desc.angle_unit,
+        k_pack_sphere<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->desc.angle_unit, perm,
                                                   p->d_X64, p->d_U64, p->mixed ? p->d_XF : nullptr, p->d_aux + 1);
     else
-        k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->df, p->d_X64, p->d_U64,
-                                                p->mixed ? p->d_XF : nullptr, p->mixed ? p->d_UF : nullptr,
-                                                p->d_aux + 1);
+        k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->df, perm, p->d_X64,
+                                                p->d_U64, p->mixed ? p->d_XF : nullptr,
+                                                p->mixed ? p->d_UF : nullptr, p->d_aux + 1);
 }
 
-// Host mirror of BlockHist<R, NV, PRIV>::bytes (sfb200_acc.cuh).
-static size_t hist_bytes(bool fp32, int NV, int priv, int NW, int NBP)
+// Points below this count keep the caller's order: the sort costs more than the runs it lengthens.
+static const long long kOrderMinPoints = 16384;
+
+// Whether a run of n points stores them in Morton order. The joint sphere path keeps the caller's
+// order: its FP64 value binning uses the reference's pair frame, whose rounding is not symmetric in
+// the two points, so the pair orientation (i < j in caller order) must be kept.
+static bool use_spatial_order(const sfb200_plan* p, long long n)
+{
+    if (p->joint && p->sphere) return false;
+    if (p->order_ovr >= 0) return p->order_ovr == 1;
+    return n >= kOrderMinPoints;
+}
+
+// Morton keys of the caller's points, radix-sorted with their indices; returns the permutation
+// (slot -> caller index) in device memory.
+template <typename TX>
+static int launch_order(sfb200_plan* p, const void* x, int n, cudaStream_t s, const int** perm)
+{
+    sfb200_ctx* ctx = p->ctx;
+    const int tb = 256, nblk = (n + tb - 1) / tb;
+    CK(cudaMemsetAsync(p->d_box, 0xff, sizeof(unsigned) * 3, s));
+    CK(cudaMemsetAsync(p->d_box + 3, 0, sizeof(unsigned) * 3, s));
+    k_morton_box<TX><<<nblk, tb, 0, s>>>((const TX*)x, n, p->W, p->sphere, p->desc.angle_unit, p->d_box);
+    k_morton_keys<TX><<<nblk, tb, 0, s>>>((const TX*)x, n, p->W, p->sphere, p->desc.angle_unit, p->d_box,
+                                          p->d_keys, p->d_perm);
+    CK(cudaGetLastError());
+    size_t tmp = p->sort_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(p->d_sort_tmp, tmp, p->d_keys, p->d_keys + p->cap, p->d_perm,
+                                       p->d_perm + p->cap, n, 0, 32, s));
+    *perm = p->d_perm + p->cap;
+    return SFB200_OK;
+}
+
+// Host mirror of BlockHist<R, NV, PRIV>::bytes (sfb200_acc.cuh); `lc`: run-length table columns.
+static size_t hist_bytes(bool fp32, int NV, int priv, int NW, int NBP, int lc)
 {
     const size_t rs = fp32 ? 4 : 8;
     size_t b;
     if (priv == 0) {
         b = (size_t)NW * NV * NBP * rs * (fp32 ? 2 : 1) + (size_t)NW * NBP * (fp32 ? 4 : 8);
+    } else if (priv == 3) {
+        b = (size_t)NV * NBP * 8 + (size_t)NBP * 8 + (size_t)NV * NBP * lc * rs + (size_t)NBP * lc * 4;
     } else {
         const int C = priv == 2 ? 1 : priv;  // 2: warp-aggregated with leader atomics, one copy
         b = (size_t)NV * NBP * 8 + (size_t)NBP * 8 + (size_t)NW * NV * NBP * C * rs + (size_t)NW * NBP * C * 4;
@@ -626,7 +721,7 @@ static size_t hist_bytes(bool fp32, int NV, int priv, int NW, int NBP)
     return (b + 15) & ~(size_t)15;
 }
 
-static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_hist, int priv)
+static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_hist, int priv, int lc = 32)
 {
     const int NW = T / 32, NBP = p->nb + 2, NV = p->nops_pad;
     if (p->joint) {
@@ -636,22 +731,22 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
             return (size_t)(nx + p->D) * T * 8 + (smem_hist ? (size_t)ncell * 12 : 0);
         }
         const int nx = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 4 : 2) * p->D;
-        return (size_t)lut_bytes + (size_t)nx * T * 4 + (size_t)ncell * 8 + (size_t)(p->nb + 2) * 4;
+        return (size_t)lut_bytes + (size_t)nx * T * 4 + (size_t)ncell * 12 + (size_t)(p->nb + 2) * 4;
     }
     if (!p->mixed) {
         const int nx = p->sphere ? 8 : p->D;
-        return (size_t)lut_bytes + (size_t)(nx + p->D) * T * 8 + hist_bytes(false, NV, priv, NW, NBP);
+        return (size_t)lut_bytes + (size_t)(nx + p->D) * T * 8 + hist_bytes(false, NV, priv, NW, NBP, lc);
     }
     // sphere: NF floats per point; flat: one record of (hi[, lo]) x and u padded to 4 floats
     const int nx = p->sphere ? (p->D == 3 ? 20 : 18) : ((((p->df ? 4 : 2) * p->D) + 3) & ~3);
-    return (size_t)lut_bytes + (((size_t)nx * T * 4 + 15) & ~(size_t)15) + hist_bytes(true, NV, priv, NW, NBP);
+    return (size_t)lut_bytes + (((size_t)nx * T * 4 + 15) & ~(size_t)15) + hist_bytes(true, NV, priv, NW, NBP, lc);
 }
 
-// Autotuner default for the histogram privatization depth (overridable per plan).
+// Default histogram mode (overridable per plan): the run-length table.
 static int default_privatization(const sfb200_plan* p)
 {
     (void)p;
-    return 0;
+    return 3;
 }
 
 static long long tile_pairs(long long n, int T)
@@ -697,10 +792,16 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
             uin = p->d_rawu;
         }
         const bool x64 = xs == 8, u64 = us == 8;
-        if (x64 && u64) launch_pack<double, double>(p, xin, uin, (int)n, s);
-        else if (x64) launch_pack<double, float>(p, xin, uin, (int)n, s);
-        else if (u64) launch_pack<float, double>(p, xin, uin, (int)n, s);
-        else launch_pack<float, float>(p, xin, uin, (int)n, s);
+        const int* perm = nullptr;
+        if (use_spatial_order(p, n)) {
+            rc = x64 ? launch_order<double>(p, xin, (int)n, s, &perm) : launch_order<float>(p, xin, (int)n, s, &perm);
+            if (rc) return rc;
+            launches += 2;  // box + keys (the radix sort's own launches are not counted)
+        }
+        if (x64 && u64) launch_pack<double, double>(p, xin, uin, (int)n, perm, s);
+        else if (x64) launch_pack<double, float>(p, xin, uin, (int)n, perm, s);
+        else if (u64) launch_pack<float, double>(p, xin, uin, (int)n, perm, s);
+        else launch_pack<float, float>(p, xin, uin, (int)n, perm, s);
         ++launches;
         CK(cudaGetLastError());
         if (p->mixed) {
@@ -738,6 +839,7 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         int dev_smem_max = 0;
         CK(cudaDeviceGetAttribute(&dev_smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
         int flush_every = 0;
+        int hist_cols = 32;
         if (p->joint) {
             T = p->tile_ovr ? p->tile_ovr : (n >= 32768 ? 512 : (n >= 4096 ? 256 : 64));
             smem = smem_bytes(p, T, lut_bytes, true, 0);
@@ -750,6 +852,8 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
                 smem = smem_bytes(p, T, lut_bytes, false, 0);
             }
             kc = pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->df, p->opl);
+            // block cells hold at most 2^31 pairs between flushes (T^2 pairs per tile pair)
+            flush_every = (int)std::max<long long>(1, (1ll << 31) / ((long long)T * T));
         } else {
             const int want = p->priv_ovr >= 0 ? p->priv_ovr : default_privatization(p);
             kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, want)
@@ -763,16 +867,31 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
                 }
             }
             if (T > kc.max_threads) T = kc.max_threads;
-            smem = smem_bytes(p, T, lut_bytes, true, kc.priv);
+            if (kc.priv == 3) {
+                // run-length table: the most columns (<= 32) that leave room for 3 blocks per SM,
+                // at least one column
+                hist_cols = p->cols_ovr ? p->cols_ovr : 32;
+                if (!p->cols_ovr) {
+                    int smem_sm = 0;
+                    CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+                    while (hist_cols > 1 && smem_bytes(p, T, lut_bytes, true, 3, hist_cols) + 1024 > (size_t)smem_sm / 3)
+                        hist_cols /= 2;
+                }
+            }
+            smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols);
             while (smem > (size_t)dev_smem_max && T > 32) {
                 T /= 2;
-                smem = smem_bytes(p, T, lut_bytes, true, kc.priv);
+                smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols);
             }
             if (smem > (size_t)dev_smem_max)
                 return set_err(ctx, SFB200_ERR_UNSUPPORTED, "%d bins x %d operators do not fit shared memory",
                                p->nb, p->nops);
-            // FP32 copies are folded into FP64 before any lane-bin cell can hold more than ~512 terms
-            if (kc.priv > 0) {
+            if (kc.priv == 3) {
+                // FP32 table cells are folded into FP64 before any of them holds more than ~4096
+                // pair terms (NW warps x T steps per tile pair add into one column)
+                flush_every = p->mixed ? std::max(1, 4096 / ((T / 32) * T)) : 64;
+            } else if (kc.priv > 0) {
+                // FP32 copies are folded into FP64 before any lane-bin cell can hold more than ~512 terms
                 const int copies = kc.priv == 2 ? 1 : kc.priv;
                 flush_every = p->mixed ? std::max(1, 512 * copies / (32 * T)) : 64;
             }
@@ -785,6 +904,10 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         if (p->bps_ovr) occ = std::min(occ, p->bps_ovr);
         const long long ntp = tile_pairs(n, T);
         const long long grid = std::min<long long>(ntp, (long long)ctx->nsm * occ);
+        // the warp-aggregated FP32 histogram counts in 32 bits per warp and bin without folding
+        if (!p->joint && kc.priv == 0 && p->mixed && ((ntp + grid - 1) / grid) * 32ll * T >= (1ll << 32))
+            return set_err(ctx, SFB200_ERR_UNSUPPORTED,
+                           "privatization 0 would overflow its 32-bit counters at %lld points; use another", n);
 
         PairArgs a{};
         a.n = (int)n;
@@ -811,9 +934,12 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         a.n_vedges = p->joint ? p->desc.value.n_edges : 0;
         a.vwin = p->d_vwin;
         a.flush_every = flush_every;
+        a.hist_cols = hist_cols;
         // per-pair relative value error: compensated du_L carries ~(6 order + 6) u; otherwise only
         // the rounding of t itself (the rest is in the per-row absolute window)
         a.vrel = (float)((p->l_only ? (6.0 * p->vorder + 6.0) * 1.25 : 4.0) * 0x1p-24);
+        a.vq = p->vq;
+        a.vq_inv = p->vq_inv;
         a.gen = p->gen;
         a.g_sums = p->d_sums;
         a.g_counts = p->d_counts;

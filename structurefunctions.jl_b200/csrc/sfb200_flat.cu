@@ -12,12 +12,14 @@ static KernelChoice flat_kernel()
     else return {reinterpret_cast<const void*>(&k_flat1d_fp64<D, OPS, PRIV>), 256, PRIV};
 }
 
-// Specialized operator lists get every privatization depth; generic lists warp-aggregated or per lane.
+// Specialized operator lists get every privatization depth; generic lists warp-aggregated,
+// run-length or per lane.
 template <int D, int MODE, class OPS, bool ALL>
 static KernelChoice flat_entry(int priv)
 {
     switch (priv) {
     case 32: return flat_kernel<D, MODE, OPS, 32>();
+    case 3: return flat_kernel<D, MODE, OPS, 3>();
     case 8: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 8>(); break;
     case 4: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 4>(); break;
     case 1: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 1>(); break;

@@ -8,11 +8,15 @@
 // sparsely hit, so warp aggregation buys little); otherwise the kernel adds straight into the global
 // FP64 / uint64 accumulators.
 //
-// The FP32 kernel accumulates each cell as count and the FP32 sum of (v - c_vbin), the value's
-// offset from its value-bin centre: a cell's values are within half a bin width of c_vbin, so the
-// FP32 running sum carries the small residuals only, and the merge rebuilds
-// sum = count * c_vbin + residual in FP64. Pairs whose value (or distance) lies within the FP32
-// error bound of an edge are recomputed in FP64 with the reference arithmetic.
+// The FP32 kernel accumulates each cell as its count and the sum of (v - c_vbin), the value's
+// offset from its value-bin centre, in 64-bit fixed point: a cell's values lie within half a bin
+// width h of c_vbin, so with the power-of-two scale S = 2^k, h S < 2^30, every offset is one integer
+// of at most 2^30 and a block's cell sum stays exact (the quantum 1/S is below 2^-30 h). The merge
+// rebuilds sum = count * c_vbin + residual / S in FP64. Pairs whose value (or distance) lies within
+// the FP32 error bound of an edge are recomputed in FP64 with the reference arithmetic.
+//
+// Both kernels move their block histogram to the global one every `flush_every` tile pairs, so a
+// 32-bit cell count never exceeds 2^31 pairs.
 #pragma once
 
 #include "sfb200_kernels.cuh"
@@ -20,6 +24,20 @@
 namespace sfb {
 
 // ------------------------------------------------------------------------------------ FP64
+// Add the block's cells into the global histogram and clear them (all threads, after a barrier).
+__device__ __forceinline__ void joint_flush_fp64(const PairArgs& a, double* hs, unsigned* hc, int ncell)
+{
+    for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
+        if (hc[k]) {
+            atomicAdd(&a.g_sums[k], hs[k]);
+            atomicAdd(&a.g_counts[k], (unsigned long long)hc[k]);
+            hs[k] = 0.0;
+            hc[k] = 0u;
+        }
+    }
+    __syncthreads();
+}
+
 template <bool SPHERE, int D, bool SMEM>
 __global__ void __launch_bounds__(512) k_joint_fp64(const PairArgs a)
 {
@@ -39,7 +57,14 @@ __global__ void __launch_bounds__(512) k_joint_fp64(const PairArgs a)
     if constexpr (SMEM) {
         for (int k = threadIdx.x; k < ncell; k += T) { hs[k] = 0.0; hc[k] = 0u; }
     }
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+    int iter = 0;
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        if constexpr (SMEM) {
+            if (iter && iter % a.flush_every == 0) {
+                __syncthreads();
+                joint_flush_fp64(a, hs, hc, ncell);
+            }
+        }
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
         const int i = ti * T + threadIdx.x;
@@ -108,21 +133,17 @@ __global__ void __launch_bounds__(512) k_joint_fp64(const PairArgs a)
     }
     if constexpr (SMEM) {
         __syncthreads();
-        for (int k = threadIdx.x; k < ncell; k += T) {
-            if (hc[k]) {
-                atomicAdd(&a.g_sums[k], hs[k]);
-                atomicAdd(&a.g_counts[k], (unsigned long long)hc[k]);
-            }
-        }
+        joint_flush_fp64(a, hs, hc, ncell);
     }
 }
 
 // ------------------------------------------------------------------------------------ mixed
-// Value-bin centre (FP32) of value bin vb in [1, nv].
-__device__ __forceinline__ float value_center(const PairArgs& a, int vb)
+// Value-bin centre of value bin vb in [1, nv] (FP64: the offsets from it stay within half a bin
+// width even where the bin is narrow next to its centre).
+__device__ __forceinline__ double value_center(const PairArgs& a, int vb)
 {
-    if (a.val_linear) return (float)(a.vlin.first + ((double)vb - 0.5) * a.vlin.step);
-    return (float)(0.5 * (a.vedges[vb - 1] + a.vedges[vb]));
+    if (a.val_linear) return a.vlin.first + ((double)vb - 0.5) * a.vlin.step;
+    return 0.5 * a.vedges[vb - 1] + 0.5 * a.vedges[vb];
 }
 
 // Compensated dot product (Ogita-Rump-Oishi Dot2): the exact product errors come from fma and the
@@ -147,6 +168,24 @@ __device__ __forceinline__ float dot2(const float* x, const float* y)
     return __fadd_rn(p, e);
 }
 
+// Add the block's cells (count, fixed-point offset sum) into the global FP64 histogram and clear
+// them (all threads, after a barrier).
+__device__ __forceinline__ void joint_flush_mixed(const PairArgs& a, unsigned long long* hres, unsigned* hc,
+                                                  int ncell)
+{
+    for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
+        if (hc[k]) {
+            const int vb = k / a.nb + 1;
+            const double s = (double)hc[k] * value_center(a, vb) + (double)(long long)hres[k] * a.vq_inv;
+            atomicAdd(&a.g_sums[k], s);
+            atomicAdd(&a.g_counts[k], (unsigned long long)hc[k]);
+            hres[k] = 0ull;
+            hc[k] = 0u;
+        }
+    }
+    __syncthreads();
+}
+
 template <bool SPHERE, int D, bool DFX, bool DFU, class OPS>
 __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
 {
@@ -162,14 +201,14 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
     LutEntry32* lut = reinterpret_cast<LutEntry32*>(smem);
     float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);  // NXF * T
     float* su = sx + NXF * T;                                   // NUF * T (flat)
-    float* hres = su + NUF * T;                                 // ncell
-    unsigned* hc = reinterpret_cast<unsigned*>(hres + ncell);   // ncell
-    float* swin = reinterpret_cast<float*>(hc + ncell);         // nd + 2
+    unsigned long long* hres = reinterpret_cast<unsigned long long*>(su + NUF * T);  // ncell
+    unsigned* hc = reinterpret_cast<unsigned*>(hres + ncell);                        // ncell
+    float* swin = reinterpret_cast<float*>(hc + ncell);                              // nd + 2
     __shared__ unsigned long long s_recheck;
 
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry32); k += T)
         lut[k] = static_cast<const LutEntry32*>(a.lut)[k];
-    for (int k = threadIdx.x; k < ncell; k += T) { hres[k] = 0.f; hc[k] = 0u; }
+    for (int k = threadIdx.x; k < ncell; k += T) { hres[k] = 0ull; hc[k] = 0u; }
     for (int k = threadIdx.x; k < nd + 2; k += T) swin[k] = a.vwin[k];
     if (threadIdx.x == 0) s_recheck = 0ull;
     unsigned long long my_recheck = 0;
@@ -177,7 +216,12 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
     const float vnegf = (float)a.vlin.neg_f_inv;
     const float tmax = (float)(a.vlin.n - 1);
 
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x) {
+    int iter = 0;
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        if (iter && iter % a.flush_every == 0) {
+            __syncthreads();
+            joint_flush_mixed(a, hres, hc, ncell);
+        }
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
         const int i = ti * T + threadIdx.x;
@@ -268,11 +312,11 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
             }
             slow = slow && valid;
             bool ok = true;
+            double v64 = 0.0;
             if (__any_sync(FULL, slow)) {
                 if (slow) {
                     const int j = j0 + jj;
                     double du64[D];
-                    double v64;
                     if constexpr (!SPHERE) {
                         double dx64[D];
 #pragma unroll
@@ -299,28 +343,22 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
                         v64 = x_sphere_value<D>(a.gen.op[0], du64);
                     }
                     vb = value_exact_bin(a, v64);
-                    val = (float)v64;
                 }
                 const unsigned sb = __ballot_sync(FULL, slow);
                 if (lane == 0) my_recheck += __popc(sb);
             }
             if (valid && ok && db >= 1 && db <= nd && vb >= 1 && vb <= nv) {
                 const int cell = (db - 1) + nd * (vb - 1);
-                atomicAdd(&hres[cell], val - value_center(a, vb));
+                const double c = value_center(a, vb);
+                const double off = (slow ? v64 : (double)val) - c;
+                atomicAdd(&hres[cell], (unsigned long long)__double2ll_rn(off * a.vq));
                 atomicAdd(&hc[cell], 1u);
             }
         }
     }
     if (lane == 0 && my_recheck) atomicAdd(&s_recheck, my_recheck);
     __syncthreads();
-    for (int k = threadIdx.x; k < ncell; k += T) {
-        if (hc[k]) {
-            const int vb = k / nd + 1;
-            const double s = (double)hc[k] * (double)value_center(a, vb) + (double)hres[k];
-            atomicAdd(&a.g_sums[k], s);
-            atomicAdd(&a.g_counts[k], (unsigned long long)hc[k]);
-        }
-    }
+    joint_flush_mixed(a, hres, hc, ncell);
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 

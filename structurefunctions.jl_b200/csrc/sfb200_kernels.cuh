@@ -54,7 +54,10 @@ struct PairArgs {
     const float* vwin; // per distance row: absolute half-width of the value ambiguity window in
                        // value-bin index units (mixed)
     float vrel;        // relative half-width: window += (|t| + |first/step|) * vrel
+    double vq;         // fixed-point scale of the value offsets (power of two), and its inverse
+    double vq_inv;
     int flush_every;   // privatized histograms: fold copies into FP64 every this many tile pairs
+    int hist_cols;     // run-length histogram: table columns (power of two <= 32)
     GenOps gen;
     double* g_sums;
     unsigned long long* g_counts;
@@ -117,12 +120,13 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
     double* sx = reinterpret_cast<double*>(smem + a.lut_bytes);
     double* su = sx + D * T;
     Hist hist;
-    hist.init(reinterpret_cast<unsigned char*>(su + D * T), NW, a.nb + 2);
+    hist.init(reinterpret_cast<unsigned char*>(su + D * T), NW, a.nb + 2, a.hist_cols);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
 
     int iter = 0;
     for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
@@ -243,7 +247,7 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
     float* srec = reinterpret_cast<float*>(smem + a.lut_bytes);  // T records of NR floats
     __shared__ unsigned long long s_recheck;
     Hist hist;
-    hist.init(smem + a.lut_bytes + (size_t)NR * T * 4, NW, a.nb + 2);
+    hist.init(smem + a.lut_bytes + (size_t)NR * T * 4, NW, a.nb + 2, a.hist_cols);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry32); k += T)
         lut[k] = static_cast<const LutEntry32*>(a.lut)[k];
     if (threadIdx.x == 0) s_recheck = 0ull;
@@ -251,6 +255,7 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
 
     int iter = 0;
     for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
@@ -396,12 +401,13 @@ __global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
     double* sx = reinterpret_cast<double*>(smem + a.lut_bytes);  // NX * T
     double* su = sx + NX * T;                                     // D * T
     Hist hist;
-    hist.init(reinterpret_cast<unsigned char*>(su + D * T), NW, a.nb + 2);
+    hist.init(reinterpret_cast<unsigned char*>(su + D * T), NW, a.nb + 2, a.hist_cols);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
 
     int iter = 0;
     for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
@@ -480,7 +486,7 @@ __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
     float* sx = reinterpret_cast<float*>(smem + a.lut_bytes);  // NF * T
     __shared__ unsigned long long s_recheck;
     Hist hist;
-    hist.init(smem + a.lut_bytes + (((size_t)NF * T * 4 + 15) & ~(size_t)15), NW, a.nb + 2);
+    hist.init(smem + a.lut_bytes + (((size_t)NF * T * 4 + 15) & ~(size_t)15), NW, a.nb + 2, a.hist_cols);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry32); k += T)
         lut[k] = static_cast<const LutEntry32*>(a.lut)[k];
     if (threadIdx.x == 0) s_recheck = 0ull;
@@ -488,6 +494,7 @@ __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
 
     int iter = 0;
     for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);

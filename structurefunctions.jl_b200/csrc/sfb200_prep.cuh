@@ -33,6 +33,121 @@ __device__ __forceinline__ void block_max2_to(double vx, double vu, unsigned lon
     }
 }
 
+// ---------------------------------------------------------------- spatial order of the points
+//
+// The pair kernels visit the j of a tile in storage order. Storing the points along a Morton
+// (Z-order) curve makes consecutive j spatial neighbours, so the distance from a fixed i changes
+// slowly along the loop and the run-length histogram mostly extends runs. The order never changes
+// which pairs are formed (each unordered pair is still visited once) and every pair quantity used
+// for binning is symmetric in the two points, so counts are unchanged; only the summation order of
+// the sums differs.
+
+// Unsigned image of a float that orders like the float (for integer atomicMin / atomicMax).
+__device__ __forceinline__ unsigned float_order_key(float f)
+{
+    const unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float float_from_order_key(unsigned k)
+{
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// Per-dimension bounding box of the Morton coordinates, as order keys: box[0..2] minima (start at
+// 0xffffffff), box[3..5] maxima (start at 0). Flat: the D coordinates; sphere: the unit vector.
+template <typename TX>
+__device__ __forceinline__ int morton_coords(const TX* __restrict__ x, int i, int W, bool sphere, int unit, float* c)
+{
+    if (!sphere) {
+        for (int d = 0; d < W; ++d) c[d] = (float)x[(size_t)W * i + d];
+        return W;
+    }
+    float lon = (float)x[(size_t)2 * i], lat = (float)x[(size_t)2 * i + 1];
+    if (unit == SFB200_ANGLE_DEG) {
+        lon *= 0.017453292519943295f;
+        lat *= 0.017453292519943295f;
+    }
+    float sl, cl, sp, cp;
+    sincosf(lon, &sl, &cl);
+    sincosf(lat, &sp, &cp);
+    c[0] = cp * cl;
+    c[1] = cp * sl;
+    c[2] = sp;
+    return 3;
+}
+
+template <typename TX>
+__global__ void k_morton_box(const TX* __restrict__ x, int n, int W, int sphere, int unit, unsigned* box)
+{
+    __shared__ unsigned smin[3], smax[3];
+    if (threadIdx.x < 3) { smin[threadIdx.x] = 0xffffffffu; smax[threadIdx.x] = 0u; }
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        float c[3];
+        const int nd = morton_coords(x, i, W, sphere != 0, unit, c);
+        for (int d = 0; d < nd; ++d) {
+            if (c[d] != c[d]) continue;  // NaN coordinates do not widen the box
+            const unsigned k = float_order_key(c[d]);
+            atomicMin(&smin[d], k);
+            atomicMax(&smax[d], k);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        atomicMin(&box[threadIdx.x], smin[threadIdx.x]);
+        atomicMax(&box[3 + threadIdx.x], smax[threadIdx.x]);
+    }
+}
+
+// Spread the low 16 bits of v to the even bit positions / the low 10 bits to every third position.
+__device__ __forceinline__ unsigned spread2(unsigned v)
+{
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+__device__ __forceinline__ unsigned spread3(unsigned v)
+{
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// Morton key and identity index of every point (points with a NaN coordinate sort last).
+template <typename TX>
+__global__ void k_morton_keys(const TX* __restrict__ x, int n, int W, int sphere, int unit, const unsigned* box,
+                              unsigned* keys, int* idx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float c[3];
+    const int nd = morton_coords(x, i, W, sphere != 0, unit, c);
+    const int bits = nd == 2 ? 16 : 10;
+    const float top = (float)((1 << bits) - 1);
+    unsigned q[3] = {0u, 0u, 0u};
+    bool nan = false;
+    for (int d = 0; d < nd; ++d) {
+        const float lo = float_from_order_key(box[d]), hi = float_from_order_key(box[3 + d]);
+        const float ext = hi - lo;
+        if (c[d] != c[d]) { nan = true; continue; }
+        const float t = ext > 0.f ? (c[d] - lo) / ext * top : 0.f;
+        q[d] = (unsigned)fminf(fmaxf(t, 0.f), top);
+    }
+    unsigned key;
+    if (nan) key = 0xffffffffu;
+    else if (nd == 2) key = spread2(q[0]) | (spread2(q[1]) << 1);
+    else key = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+    keys[i] = key;
+    idx[i] = i;
+}
+
 // FP32 image of an FP64 value as (hi, lo): hi = fl32(v), lo = fl32(v - hi); hi + lo equals v to
 // about 2^-48 relative.
 __device__ __forceinline__ void split_df(double v, float& hi, float& lo)
@@ -43,15 +158,18 @@ __device__ __forceinline__ void split_df(double v, float& hi, float& lo)
 
 template <typename TX, typename TU>
 __global__ void k_pack_flat(const TX* __restrict__ x, const TU* __restrict__ u, int n, int D, int df,
-                            double* X64, double* U64, float* XF, float* UF, unsigned long long* bound)
+                            const int* __restrict__ perm, double* X64, double* U64, float* XF, float* UF,
+                            unsigned long long* bound)
 {
-    // with df, every FP32 value is stored as (hi, lo) (lo = 0 for FP32 inputs)
+    // with df, every FP32 value is stored as (hi, lo) (lo = 0 for FP32 inputs); slot i holds caller
+    // point perm[i] (the identity without a permutation)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double mx = 0.0, mu = 0.0;
     if (i < n) {
+        const size_t src = perm ? (size_t)perm[i] : (size_t)i;
         for (int d = 0; d < D; ++d) {
-            const double xv = (double)x[(size_t)D * i + d];
-            const double uv = (double)u[(size_t)D * i + d];
+            const double xv = (double)x[(size_t)D * src + d];
+            const double uv = (double)u[(size_t)D * src + d];
             X64[(size_t)d * n + i] = xv;
             U64[(size_t)d * n + i] = uv;
             if (XF) {
@@ -74,16 +192,18 @@ __global__ void k_pack_flat(const TX* __restrict__ x, const TU* __restrict__ u, 
 // check), velocities as given; FP32 images p, U = u_e E + u_n N, W = u_n E - u_e N, [up].
 template <typename TX, typename TU>
 __global__ void k_pack_sphere(const TX* __restrict__ x, const TU* __restrict__ u, int n, int D,
-                              int unit, double* X64, double* U64, float* XF, unsigned long long* bound)
+                              int unit, const int* __restrict__ perm, double* X64, double* U64, float* XF,
+                              unsigned long long* bound)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t src = (i < n && perm) ? (size_t)perm[i] : (size_t)i;
     double mu = 0.0;
     if (i < n) {
-        for (int d = 0; d < D; ++d) mu = fmax(mu, fabs((double)u[(size_t)D * i + d]));
+        for (int d = 0; d < D; ++d) mu = fmax(mu, fabs((double)u[(size_t)D * src + d]));
     }
     block_max2_to(1.0, mu, bound);
     if (i >= n) return;
-    const double lon = (double)x[(size_t)2 * i], lat = (double)x[(size_t)2 * i + 1];
+    const double lon = (double)x[(size_t)2 * src], lat = (double)x[(size_t)2 * src + 1];
     double sl, cl, sp, cp;
     if (unit == SFB200_ANGLE_DEG) {
         sfb_sincosd(lon, &sl, &cl);
@@ -99,7 +219,7 @@ __global__ void k_pack_sphere(const TX* __restrict__ x, const TU* __restrict__ u
     for (int k = 0; k < 8; ++k) X64[(size_t)k * n + i] = c[k];
     double uv[3] = {0.0, 0.0, 0.0};
     for (int d = 0; d < D; ++d) {
-        uv[d] = (double)u[(size_t)D * i + d];
+        uv[d] = (double)u[(size_t)D * src + d];
         U64[(size_t)d * n + i] = uv[d];
     }
     if (XF) {

@@ -16,6 +16,7 @@ static KernelChoice sphere_entry(int priv)
 {
     switch (priv) {
     case 32: return sphere_kernel<D, MIXED, OPS, 32>();
+    case 3: return sphere_kernel<D, MIXED, OPS, 3>();
     case 8: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 8>(); break;
     case 4: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 4>(); break;
     case 1: if constexpr (ALL) return sphere_kernel<D, MIXED, OPS, 1>(); break;

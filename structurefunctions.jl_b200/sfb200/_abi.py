@@ -104,4 +104,9 @@ EXPORTED_SYMBOLS = (
     "sfb200_run",
     "sfb200_plan_last_stats",
     "sfb200_plan_set_launch",
+    "sfb200_plan_set_option",
 )
+
+# sfb200_option
+OPT_POINT_ORDER = 1
+OPT_HIST_COLUMNS = 2

@@ -49,6 +49,8 @@ def load():
         lib.sfb200_plan_last_stats.restype = C.c_int
         lib.sfb200_plan_set_launch.argtypes = [P, C.c_int, C.c_int, C.c_int]
         lib.sfb200_plan_set_launch.restype = C.c_int
+        lib.sfb200_plan_set_option.argtypes = [P, C.c_int, C.c_int64]
+        lib.sfb200_plan_set_option.restype = C.c_int
         if lib.sfb200_abi_version() != _abi.ABI_VERSION:
             raise OSError(f"libsfb200.so ABI {lib.sfb200_abi_version()} != {_abi.ABI_VERSION}")
         _lib = lib
@@ -125,6 +127,10 @@ class Plan:
 
     def set_launch(self, tile=0, privatization=-1, blocks_per_sm=0):
         check(load().sfb200_plan_set_launch(self.ptr, tile, privatization, blocks_per_sm), self.ctx.ptr)
+
+    def set_option(self, option, value):
+        """sfb200_plan_set_option: `option` is _abi.OPT_POINT_ORDER or _abi.OPT_HIST_COLUMNS."""
+        check(load().sfb200_plan_set_option(self.ptr, int(option), int(value)), self.ctx.ptr)
 
     def close(self):
         if self.ptr:

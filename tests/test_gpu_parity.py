@@ -11,7 +11,7 @@ import pytest
 import oracle_py
 from helpers import TOL_FP64, TOL_MIXED, compare
 import sfb200 as SF
-from sfb200 import _lib, synthetic
+from sfb200 import _abi, _lib, synthetic
 from sfb200.api import plan_description
 
 pytestmark = pytest.mark.gpu
@@ -19,12 +19,14 @@ pytestmark = pytest.mark.gpu
 PRECISIONS = [("fp64", TOL_FP64), ("mixed", TOL_MIXED)]
 
 
-def run_gpu(ops, x, u, bins, metric=None, value_bins=None, precision="mixed", tile=0, priv=None):
+def run_gpu(ops, x, u, bins, metric=None, value_bins=None, precision="mixed", tile=0, priv=None, options=None):
     be = SF.B200Backend(precision=precision, tile=tile)
     desc, keep = plan_description(ops, u.shape[0], bins, value_bins, metric, precision, x.dtype, u.dtype)
     plan = _lib.Plan(be.context, desc, keep)
     if tile or priv is not None:
         plan.set_launch(tile, -1 if priv is None else priv, 0)
+    for opt, val in (options or {}).items():
+        plan.set_option(opt, val)
     sums = np.zeros(plan.n_sums)
     counts = np.zeros(plan.n_counts, dtype=np.uint64)
     xa = np.asfortranarray(x)
@@ -153,7 +155,7 @@ def test_joint_sphere(precision, tol):
 
 
 @pytest.mark.parametrize("precision,tol", PRECISIONS)
-@pytest.mark.parametrize("priv", [0, 1, 4, 8, 32])
+@pytest.mark.parametrize("priv", [0, 1, 2, 3, 4, 8, 32])
 @pytest.mark.parametrize("tile", [32, 64, 256])
 def test_privatization_modes(precision, tol, priv, tile):
     """Every histogram privatization depth and tile size gives the oracle's histogram."""
@@ -169,6 +171,37 @@ def test_privatization_modes(precision, tol, priv, tile):
                          tile=tile, priv=priv)
     rs, rc, ra = run_oracle(ws.ops, ws.x, ws.u, ws.distance_bins.edges, metric=ws.metric)
     compare(gs, gc, rs, rc, ra, tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("cols", [1, 8, 32])
+def test_point_order_and_table_columns(precision, tol, order, cols):
+    """Morton-ordered storage and every run-length table width give the oracle's histogram."""
+    opts = {_abi.OPT_POINT_ORDER: order, _abi.OPT_HIST_COLUMNS: cols}
+    w = synthetic.config("c1", n=2000)
+    gs, gc, st = run_gpu(w.ops, w.x, w.u, w.distance_bins.edges, precision=precision, priv=3, options=opts)
+    rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges)
+    nb = len(w.distance_bins) - 1
+    for k in range(len(w.ops)):
+        compare(gs[k * nb:(k + 1) * nb], gc, rs[k * nb:(k + 1) * nb], rc, ra[k * nb:(k + 1) * nb], tol)
+    for name in ("c0", "c2"):
+        w = synthetic.config(name, n=2500)
+        gs, gc, st = run_gpu(w.ops, w.x, w.u, w.distance_bins.edges, metric=w.metric, precision=precision,
+                             priv=3, options=opts)
+        rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges, metric=w.metric)
+        compare(gs, gc, rs, rc, ra, tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_joint_point_order(precision, tol):
+    """The joint flat histogram is the same in caller and Morton order."""
+    w = synthetic.config("c3", n=2500)
+    for order in (0, 1):
+        gs, gc, st = run_gpu(w.ops, w.x, w.u, w.distance_bins.edges, value_bins=w.value_bins,
+                             precision=precision, options={_abi.OPT_POINT_ORDER: order})
+        rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges, value_bins=w.value_bins)
+        compare(gs, gc, rs, rc, ra, tol)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
