@@ -211,14 +211,26 @@ def run_ours(args):
     clocks = ClockSampler(local)
     mixed, msums, mcounts = make("mixed")
     fp64, fsums, fcounts = make("fp64")
+    fp32, hsums, hcounts = make("fp32")
 
     clocks.start()
     t_mixed, kms_mixed, launches_mixed, st_mixed = device_steps(mixed, msums, mcounts, args.steps, args.warmup)
     t_fp64, kms_fp64, launches_fp64, st_fp64 = device_steps(fp64, fsums, fcounts, args.steps, args.warmup)
+    t_fp32, kms_fp32, launches_fp32, st_fp32 = device_steps(fp32, hsums, hcounts, args.steps, args.warmup)
     clk = clocks.stop()
 
-    # counts of the two kernels must agree (bit-exact binning in both)
-    same_counts = bool(torch.equal(mcounts, fcounts))
+    # counts of the kernels must agree (bit-exact binning in all); sums: per-bin deviation of the
+    # mixed and FP32-bulk kernels from the FP64 kernel at the full size (relative to |FP64 sum|)
+    same_counts = bool(torch.equal(mcounts, fcounts)) and bool(torch.equal(hcounts, fcounts))
+
+    def max_rel_dev(a, b):
+        a = a.cpu().numpy()
+        b = b.cpu().numpy()
+        ok = np.isfinite(b) & (np.abs(b) > 0)
+        return float(np.max(np.abs(a[ok] - b[ok]) / np.abs(b[ok]))) if ok.any() else 0.0
+
+    dev_mixed = max_rel_dev(msums, fsums)
+    dev_fp32 = max_rel_dev(hsums, fsums)
 
     # e2e through the C ABI with host buffers (pinned)
     xp = torch.from_numpy(np.ascontiguousarray(x_host.T)).pin_memory()
@@ -250,14 +262,18 @@ def run_ours(args):
     t_fp64 = max_over_ranks(t_fp64)
     e2e_total = max_over_ranks(e2e_total * 1e3)
 
+    t_fp32 = max_over_ranks(t_fp32)
     ms_mixed = t_mixed / args.steps
     ms_fp64 = t_fp64 / args.steps
+    ms_fp32 = t_fp32 / args.steps
     value = world * pairs / (ms_mixed * 1e-3)
     fp64_value = world * pairs / (ms_fp64 * 1e-3)
+    fp32_value = world * pairs / (ms_fp32 * 1e-3)
     e2e_value = world * pairs / (e2e_total / args.steps * 1e-3)
 
     kmed_mixed = sorted(kms_mixed)[len(kms_mixed) // 2]
     kmed_fp64 = sorted(kms_fp64)[len(kms_fp64) // 2]
+    kmed_fp32 = sorted(kms_fp32)[len(kms_fp32) // 2]
     peak32 = measure_peak(local, False)
     peak64 = measure_peak(local, True)
     flops = w.flops_per_pair
@@ -287,9 +303,9 @@ def run_ours(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32",
-            "precision": "mixed: FP32 pair arithmetic with two-sum accumulation, FP64 recheck of near-edge/short "
-                         "pairs, FP64 merge",
+            "dtype": "f64+f32",
+            "precision": "mixed: FP64 point differences, squared distance (exact bin) and projection numerators; "
+                         "FP32 normalisation, operator powers and per-lane run accumulation; FP64 merge",
             "data": "synthetic (seeded; no dataset)",
             "config": {
                 "workload": w.name,
@@ -304,8 +320,13 @@ def run_ours(args):
             },
             "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms_fp64, "kernel_ms": kmed_fp64,
                      "roofline_frac_fp64": (achieved64 / peak64) if peak64 else None},
+            "fp32": {"value": fp32_value, "unit": UNIT, "ms_per_step": ms_fp32, "kernel_ms": kmed_fp32,
+                     "rechecked_pairs_per_step": st_fp32["rechecked"],
+                     "max_rel_dev_vs_fp64": dev_fp32,
+                     "note": "FP32-bulk kernel: FP32 differences, FP64 recheck of bin membership only"},
             "mixed_over_fp64": value / fp64_value,
-            "counts_equal_mixed_fp64": same_counts,
+            "counts_equal_all_precisions": same_counts,
+            "mixed_max_rel_dev_vs_fp64": dev_mixed,
             "rechecked_pairs_per_step": st_mixed["rechecked"],
             "roofline": {
                 "bound": "fp32",
@@ -330,6 +351,7 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     mixed.close()
     fp64.close()
+    fp32.close()
     ctx.close()
     if dist:
         dist.destroy_process_group()

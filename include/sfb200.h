@@ -111,8 +111,13 @@ typedef struct {
 
 typedef enum {
     SFB200_PREC_FP64 = 0,  /* plain form: every pair in FP64 */
-    SFB200_PREC_MIXED = 1  /* FP32 bulk, FP64 recheck of near-edge / short / near-antipodal pairs,
-                              FP64 merge */
+    SFB200_PREC_MIXED = 1, /* FP64 point differences, squared distance (exact bin) and projection
+                              numerators; FP32 normalisation, operator powers and run accumulation;
+                              FP64 merge. Sums within 1e-6 of the FP64 oracle per bin. */
+    SFB200_PREC_FP32 = 2   /* FP32 bulk: FP32 differences ((hi, lo) records for FP64 inputs) and
+                              binning with an FP64 recheck of near-edge / short / near-antipodal
+                              pairs; counts exact, sums within FP32 accuracy of each pair (a pair
+                              whose projection cancels carries ~1e-7 |du| absolute error) */
 } sfb200_precision;
 
 typedef enum { SFB200_F64 = 0, SFB200_F32 = 1 } sfb200_dtype;

@@ -118,11 +118,11 @@ struct BlockHist {
     // RUN: add the lane's open run into its table column.
     __device__ __forceinline__ void flush_run(int lane)
     {
-        const int col = lane & (LC - 1);
-        R* t = hv + (size_t)rkey * LC + col;
+        const int at = rkey * LC + (lane & (LC - 1));
+        const int plane = NBP * LC;
 #pragma unroll
-        for (int o = 0; o < NV; ++o) atomicAdd(t + (size_t)o * NBP * LC, rs[o]);
-        atomicAdd(&hc[rkey * LC + col], rc);
+        for (int o = 0; o < NV; ++o) atomicAdd(hv + (at + o * plane), rs[o]);
+        atomicAdd(hc + at, rc);
     }
 
     // RUN: close every lane's run (tile-pair boundary; before a fold or the merge).
@@ -245,7 +245,9 @@ struct BlockHist {
     }
 
     // Merge into the global FP64 sums / uint64 counts (all threads call, after the pair loop).
-    __device__ void merge(double* g_sums, unsigned long long* g_counts, int nops, int nb)
+    // `oscale` (optional, NV entries): exact power-of-two factor applied to operator o's sums.
+    __device__ void merge(double* g_sums, unsigned long long* g_counts, int nops, int nb,
+                          const double* oscale = nullptr)
     {
         const int T = blockDim.x;
         if constexpr (AGG) {
@@ -258,6 +260,7 @@ struct BlockHist {
                     s += (double)hv[idx];
                     if constexpr (sizeof(R) == 4) s += (double)hlo[idx];
                 }
+                if (oscale) s *= oscale[o];
                 if (s != 0.0) atomicAdd(&g_sums[(size_t)o * nb + b - 1], s);
             }
             for (int b = threadIdx.x + 1; b <= nb; b += T) {
@@ -270,7 +273,8 @@ struct BlockHist {
             fold();
             for (int k = threadIdx.x; k < min(NV, nops) * nb; k += T) {
                 const int o = k / nb, b = k - o * nb + 1;
-                const double s = sblk[o * NBP + b];
+                double s = sblk[o * NBP + b];
+                if (oscale) s *= oscale[o];
                 if (s != 0.0) atomicAdd(&g_sums[(size_t)o * nb + b - 1], s);
             }
             for (int b = threadIdx.x + 1; b <= nb; b += T) {

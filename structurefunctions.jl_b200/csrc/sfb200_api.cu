@@ -32,7 +32,9 @@ struct sfb200_ctx {
 struct sfb200_plan {
     sfb200_ctx* ctx = nullptr;
     sfb200_plan_desc desc{};
-    bool sphere = false, mixed = false, joint = false;
+    bool sphere = false, joint = false;
+    bool mixed = false;  // precision FP32: FP32-bulk kernels with the FP64 recheck
+    bool mx = false;     // precision MIXED: FP64 differences / numerators, FP32 normalisation + accumulation
     bool df = false;  // FP32 records carry (hi, lo) pairs (an input is FP64, or the sphere basis)
     bool l_only = false;  // the joint value depends on du_L only (compensated in FP32)
     int D = 0, W = 0, nb = 0, nv = 0, nops = 0, nops_pad = 0, opl = 0, vorder = 1;
@@ -63,6 +65,7 @@ struct sfb200_plan {
     double* d_U64 = nullptr;
     float* d_XF = nullptr;
     float* d_UF = nullptr;
+    double* d_XM = nullptr;       // mixed sphere: FP64 p(3), U(3), W(3)[, up] per point (SoA)
     // spatial order: Morton keys and the permutation (double-buffered for the radix sort)
     unsigned* d_keys = nullptr;   // 2 * cap
     int* d_perm = nullptr;        // 2 * cap
@@ -195,8 +198,14 @@ static double bits_to_double(unsigned long long b)
     return d;
 }
 
-// Cell geometry over FP64 keys for the exact table.
-static void build_lut64(const std::vector<double>& tab, LutGeom& g, std::vector<LutEntry64>& out)
+// Relative half-width of the mixed sphere kernel's ambiguity band around an edge's chord key:
+// far above the FP64 error of the chord and of the edge images (~1e-15), far below a cell.
+static const double kChordWrel = 0x1p-40;
+
+// Cell geometry over FP64 keys for the exact table. With wrel > 0, a cell is also marked SLOW when
+// the band [e (1 - wrel), e (1 + wrel)] of one of its edges reaches into a neighbouring cell, so the
+// kernel's in-cell band test (|key - e| <= wrel e) sees every key of the band.
+static void build_lut64(const std::vector<double>& tab, LutGeom& g, std::vector<LutEntry64>& out, double wrel = 0.0)
 {
     double mn = INFINITY, mx = 0.0;
     for (double v : tab) {
@@ -249,6 +258,21 @@ static void build_lut64(const std::vector<double>& tab, LutGeom& g, std::vector<
         e.e = cnt ? val : NAN;
         if (distinct > 1) e.mult = LUT_FLAG_SLOW;
         out[c] = e;
+    }
+    if (wrel > 0.0) {
+        auto cell_of = [&](double key) -> long long {
+            unsigned long long b;
+            std::memcpy(&b, &key, 8);
+            b &= 0x7fffffffffffffffull;
+            long long c = (long long)(b >> g.shift) - g.base;
+            return std::min(std::max(c, 0ll), (long long)g.ncell - 1);
+        };
+        for (double v : tab) {
+            if (!(v > 0.0) || !std::isfinite(v)) continue;
+            const long long c0 = cell_of(v * (1.0 - 2.0 * wrel)), c1 = cell_of(v * (1.0 + 2.0 * wrel));
+            if (c0 != c1)
+                for (long long c = c0; c <= c1; ++c) out[c].mult = LUT_FLAG_SLOW;
+        }
     }
 }
 
@@ -337,7 +361,9 @@ static LinearParams linear_of(const sfb200_bins& b)
 static void free_workspace(sfb200_plan* p)
 {
     cudaFree(p->d_rawx); cudaFree(p->d_rawu);
-    cudaFree(p->d_X64); cudaFree(p->d_U64); cudaFree(p->d_XF); cudaFree(p->d_UF);
+    cudaFree(p->d_X64); cudaFree(p->d_U64); cudaFree(p->d_XF); cudaFree(p->d_UF); cudaFree(p->d_XM);
+    p->d_XF = p->d_UF = nullptr;
+    p->d_XM = nullptr;
     cudaFree(p->d_keys); cudaFree(p->d_perm); cudaFree(p->d_box); cudaFree(p->d_sort_tmp);
     p->d_rawx = p->d_rawu = nullptr;
     p->d_X64 = p->d_U64 = nullptr;
@@ -393,11 +419,12 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         if (!(std::isfinite(d.radius) && d.radius > 0.0))
             return set_err(ctx, SFB200_ERR_INVALID_ARG, "sphere radius must be finite and positive");
     }
-    if (d.precision != SFB200_PREC_FP64 && d.precision != SFB200_PREC_MIXED)
+    if (d.precision != SFB200_PREC_FP64 && d.precision != SFB200_PREC_MIXED && d.precision != SFB200_PREC_FP32)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "unknown precision %d", d.precision);
     if ((d.x_dtype != SFB200_F64 && d.x_dtype != SFB200_F32) || (d.u_dtype != SFB200_F64 && d.u_dtype != SFB200_F32))
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "x_dtype/u_dtype must be F64 or F32");
-    p->mixed = d.precision == SFB200_PREC_MIXED;
+    p->mixed = d.precision == SFB200_PREC_FP32;
+    p->mx = d.precision == SFB200_PREC_MIXED;
     p->joint = d.joint != 0;
     p->df = p->mixed && (p->sphere || d.x_dtype == SFB200_F64 || d.u_dtype == SFB200_F64);
     if (d.n_ops < 1 || d.n_ops > SFB200_MAX_OPS)
@@ -462,8 +489,8 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
                 return set_err(ctx, SFB200_ERR_INVALID_ARG,
                                "distance_bins: Euclidean edges must be non-negative (their squares must stay sorted)");
     }
-    // edge keys of the FP32 path
-    if (p->mixed) {
+    // edge keys of the FP32 path (and the chord keys of the mixed sphere path)
+    if (p->mixed || (p->mx && p->sphere)) {
         p->ck.resize(db.n_edges);
         for (int k = 0; k < db.n_edges; ++k) {
             double r = dlinear ? std::fma((double)k, db.step, db.first) : db.edges[k];
@@ -475,9 +502,9 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
                 p->ck[k] = p->exact_tab[k];
             }
         }
-        if (!geom_lut32(p->ck, p->lg32))
+        if (p->mixed && !geom_lut32(p->ck, p->lg32))
             return set_err(ctx, SFB200_ERR_UNSUPPORTED,
-                           "distance edges outside the FP32 range of the mixed-precision kernel; use precision=fp64");
+                           "distance edges outside the FP32 range of the fp32 kernel; use precision=mixed or fp64");
         const double u32 = 0x1p-24, u64 = 0x1p-53;
         if (p->sphere) {
             // (hi, lo) records: the chord carries ~2u per component plus the FMA chain; the FP64
@@ -505,7 +532,7 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         if (d.value.kind == SFB200_BINS_LINEAR) p->vlin = linear_of(d.value);
         else p->vedges.assign(d.value.edges, d.value.edges + d.value.n_edges);
     }
-    if (p->joint && p->mixed) {
+    if (p->joint && (p->mixed || p->mx)) {
         // fixed-point scale of the value offsets from the bin centres: 2^k with (half width) 2^k < 2^30
         double hw = 0.0;
         if (d.value.kind == SFB200_BINS_LINEAR) {
@@ -527,7 +554,12 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
     cudaError_t e;
     if (!p->exact_tab.empty() && (e = upload(&p->d_exact, p->exact_tab.data(), p->exact_tab.size())) != cudaSuccess)
         return cuda_fail(ctx, e, "upload distance table");
-    if (!dlinear && !p->mixed) {
+    if (p->mx && p->sphere) {
+        std::vector<LutEntry64> lut;
+        build_lut64(p->ck, p->lg64, lut, kChordWrel);
+        p->lut64_bytes = (int)(lut.size() * sizeof(LutEntry64));
+        if ((e = upload(&p->d_lut64, lut.data(), lut.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload table");
+    } else if (!dlinear && !p->mixed) {
         std::vector<LutEntry64> lut;
         build_lut64(p->exact_tab, p->lg64, lut);
         p->lut64_bytes = (int)(lut.size() * sizeof(LutEntry64));
@@ -556,9 +588,14 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
     p->h_counts.resize(p->n_counts);
 
     // the kernel exists for this combination
-    KernelChoice kc = p->joint ? pick_joint(p->sphere, p->D, p->mixed, true, p->df, p->opl)
-                               : (p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, 0)
-                                            : pick_flat1d(p->D, p->mixed, p->df, p->opl, 0));
+    KernelChoice kc;
+    if (p->mx)
+        kc = p->joint ? pick_joint_mx(p->sphere, p->D, p->opl)
+                      : (p->sphere ? pick_sphere1d_mx(p->D, p->opl, 0) : pick_flat1d_mx(p->D, p->opl, 0));
+    else
+        kc = p->joint ? pick_joint(p->sphere, p->D, p->mixed, true, p->df, p->opl)
+                      : (p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, 0)
+                                   : pick_flat1d(p->D, p->mixed, p->df, p->opl, 0));
     if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this operator on the joint mixed path");
     return SFB200_OK;
 }
@@ -647,6 +684,7 @@ static int ensure_workspace(sfb200_plan* p, long long n)
         CK(cudaMalloc(&p->d_XF, sizeof(float) * nxf * cap));
         if (!p->sphere) CK(cudaMalloc(&p->d_UF, sizeof(float) * (p->df ? 2 : 1) * p->D * cap));
     }
+    if (p->mx && p->sphere) CK(cudaMalloc(&p->d_XM, sizeof(double) * 10 * cap));
     CK(cudaMalloc(&p->d_keys, sizeof(unsigned) * 2 * cap));
     CK(cudaMalloc(&p->d_perm, sizeof(int) * 2 * cap));
     CK(cudaMalloc(&p->d_box, sizeof(unsigned) * 6));
@@ -665,7 +703,8 @@ static void launch_pack(sfb200_plan* p, const void* x, const void* u, int n, con
     const int tb = 256, nblk = (n + tb - 1) / tb;
     if (p->sphere)
         k_pack_sphere<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->desc.angle_unit, perm,
-                                                  p->d_X64, p->d_U64, p->mixed ? p->d_XF : nullptr, p->d_aux + 1);
+                                                  p->d_X64, p->d_U64, p->mixed ? p->d_XF : nullptr,
+                                                  p->mx ? p->d_XM : nullptr, p->d_aux + 1);
     else
         k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->df, perm, p->d_X64,
                                                 p->d_U64, p->mixed ? p->d_XF : nullptr,
@@ -724,6 +763,11 @@ static size_t hist_bytes(bool fp32, int NV, int priv, int NW, int NBP, int lc)
 static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_hist, int priv, int lc = 32)
 {
     const int NW = T / 32, NBP = p->nb + 2, NV = p->nops_pad;
+    if (p->mx) {
+        const int rec = p->sphere ? 10 : 2 * p->D;  // doubles per j record
+        if (p->joint) return (size_t)lut_bytes + (size_t)rec * T * 8 + (size_t)p->nb * p->nv * 12;
+        return (size_t)lut_bytes + (size_t)rec * T * 8 + hist_bytes(true, NV, priv, NW, NBP, lc);
+    }
     if (p->joint) {
         const long long ncell = (long long)p->nb * p->nv;
         if (!p->mixed) {
@@ -831,6 +875,7 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         const bool dlinear = p->desc.distance.kind == SFB200_BINS_LINEAR;
         int lut_bytes = 0;
         if (p->mixed) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
+        else if (p->mx) lut_bytes = p->lut64_bytes;  // exact table (flat) or chord table (sphere); 0 if linear
         else if (!dlinear && !p->joint) lut_bytes = p->lut64_bytes;
         int T;
         bool smem_hist = true;
@@ -843,21 +888,29 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         if (p->joint) {
             T = p->tile_ovr ? p->tile_ovr : (n >= 32768 ? 512 : (n >= 4096 ? 256 : 64));
             smem = smem_bytes(p, T, lut_bytes, true, 0);
+            while (p->mx && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr) {
+                T /= 2;
+                smem = smem_bytes(p, T, lut_bytes, true, 0);
+            }
             if (smem > (size_t)dev_smem_max) {
-                if (p->mixed)
+                if (p->mixed || p->mx)
                     return set_err(ctx, SFB200_ERR_UNSUPPORTED,
                                    "joint histogram of %d x %d cells does not fit shared memory on the mixed path; use fp64",
                                    p->nb, p->nv);
                 smem_hist = false;
                 smem = smem_bytes(p, T, lut_bytes, false, 0);
             }
-            kc = pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->df, p->opl);
+            kc = p->mx ? pick_joint_mx(p->sphere, p->D, p->opl)
+                       : pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->df, p->opl);
             // block cells hold at most 2^31 pairs between flushes (T^2 pairs per tile pair)
             flush_every = (int)std::max<long long>(1, (1ll << 31) / ((long long)T * T));
         } else {
             const int want = p->priv_ovr >= 0 ? p->priv_ovr : default_privatization(p);
-            kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, want)
-                           : pick_flat1d(p->D, p->mixed, p->df, p->opl, want);
+            if (p->mx)
+                kc = p->sphere ? pick_sphere1d_mx(p->D, p->opl, want) : pick_flat1d_mx(p->D, p->opl, want);
+            else
+                kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, want)
+                               : pick_flat1d(p->D, p->mixed, p->df, p->opl, want);
             if (p->tile_ovr) {
                 T = p->tile_ovr;
             } else {
@@ -889,11 +942,11 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
             if (kc.priv == 3) {
                 // FP32 table cells are folded into FP64 before any of them holds more than ~4096
                 // pair terms (NW warps x T steps per tile pair add into one column)
-                flush_every = p->mixed ? std::max(1, 4096 / ((T / 32) * T)) : 64;
+                flush_every = (p->mixed || p->mx) ? std::max(1, 4096 / ((T / 32) * T)) : 64;
             } else if (kc.priv > 0) {
                 // FP32 copies are folded into FP64 before any lane-bin cell can hold more than ~512 terms
                 const int copies = kc.priv == 2 ? 1 : kc.priv;
-                flush_every = p->mixed ? std::max(1, 512 * copies / (32 * T)) : 64;
+                flush_every = (p->mixed || p->mx) ? std::max(1, 512 * copies / (32 * T)) : 64;
             }
         }
         if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this plan");
@@ -905,7 +958,7 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         const long long ntp = tile_pairs(n, T);
         const long long grid = std::min<long long>(ntp, (long long)ctx->nsm * occ);
         // the warp-aggregated FP32 histogram counts in 32 bits per warp and bin without folding
-        if (!p->joint && kc.priv == 0 && p->mixed && ((ntp + grid - 1) / grid) * 32ll * T >= (1ll << 32))
+        if (!p->joint && kc.priv == 0 && (p->mixed || p->mx) && ((ntp + grid - 1) / grid) * 32ll * T >= (1ll << 32))
             return set_err(ctx, SFB200_ERR_UNSUPPORTED,
                            "privatization 0 would overflow its 32-bit counters at %lld points; use another", n);
 
@@ -917,8 +970,12 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         a.U64 = p->d_U64;
         a.XF = p->d_XF;
         a.UF = p->d_UF;
+        a.XM = p->d_XM;
         a.lut = p->mixed ? (const void*)p->d_lut32 : (const void*)p->d_lut64;
         a.lg = p->mixed ? p->lg32 : p->lg64;
+        a.chord_wrel = kChordWrel;
+        a.chord_short = 0x1p-40;         // (near-)coincident: the reference frame is degenerate
+        a.chord_anti = 4.0 - 0x1p-40;    // (near-)antipodal: likewise
         a.lut_bytes = lut_bytes;
         a.edges = p->d_exact;
         a.n_edges = p->desc.distance.n_edges;
@@ -938,6 +995,8 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         // per-pair relative value error: compensated du_L carries ~(6 order + 6) u; otherwise only
         // the rounding of t itself (the rest is in the per-row absolute window)
         a.vrel = (float)((p->l_only ? (6.0 * p->vorder + 6.0) * 1.25 : 4.0) * 0x1p-24);
+        // mixed: the FP32 value carries ~5 ulps per order of L / T (conversion, rsqrtf, scaling)
+        if (p->mx) a.vrel = (float)((5.0 * p->vorder + 3.0) * 1.25 * 0x1p-24);
         a.vq = p->vq;
         a.vq_inv = p->vq_inv;
         a.gen = p->gen;

@@ -56,13 +56,15 @@ struct LutGeom {
     int64_t base;     // bits >> shift of the first cell's lower end
 };
 
+// FP64 key -> cell. shift = 52 - m >= 42, so the cell index lives in the high word of the key:
+// (bits >> shift) == (hi >> (shift - 32)), and base < 2^22 fits 32-bit arithmetic.
 __device__ __forceinline__ int lut_cell64(double key, const LutGeom& g)
 {
-    const uint64_t bits = (uint64_t)__double_as_longlong(key) & 0x7fffffffffffffffull;
-    long long c = (long long)(bits >> g.shift) - g.base;
-    c = c < 0 ? 0 : c;
-    c = c > g.ncell - 1 ? g.ncell - 1 : c;
-    return (int)c;
+    const int hi = __double2hiint(key) & 0x7fffffff;
+    int c = (hi >> (g.shift - 32)) - (int)g.base;
+    c = max(c, 0);
+    c = min(c, g.ncell - 1);
+    return c;
 }
 
 __device__ __forceinline__ int lut_cell32(float key, const LutGeom& g)

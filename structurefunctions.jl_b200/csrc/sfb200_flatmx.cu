@@ -1,0 +1,51 @@
+// sfb200_flatmx.cu -- instantiations of the mixed-precision Euclidean 1D kernels.
+#include "sfb200_internal.h"
+#include "sfb200_mixed.cuh"
+
+namespace sfb {
+
+template <int D, class OPS, int PRIV>
+static KernelChoice flatmx_kernel()
+{
+    return {reinterpret_cast<const void*>(&k_flat1d_mx<D, OPS, PRIV>), 256, PRIV};
+}
+
+template <int D, class OPS, bool ALL>
+static KernelChoice flatmx_entry(int priv)
+{
+    switch (priv) {
+    case 3: return flatmx_kernel<D, OPS, 3>();
+    case 32: return flatmx_kernel<D, OPS, 32>();
+    case 2: if constexpr (ALL) return flatmx_kernel<D, OPS, 2>(); break;
+    case 8: if constexpr (ALL) return flatmx_kernel<D, OPS, 8>(); break;
+    case 4: if constexpr (ALL) return flatmx_kernel<D, OPS, 4>(); break;
+    case 1: if constexpr (ALL) return flatmx_kernel<D, OPS, 1>(); break;
+    }
+    return flatmx_kernel<D, OPS, 0>();
+}
+
+template <int D>
+static KernelChoice flatmx_by_list(int opl, int priv)
+{
+    switch (opl) {
+    case OPL_L2: return flatmx_entry<D, OpList<OC_L2>, true>(priv);
+    case OPL_L3: return flatmx_entry<D, OpList<OC_L3>, true>(priv);
+    case OPL_L1: return flatmx_entry<D, OpList<OC_L1>, true>(priv);
+    case OPL_QUAD: return flatmx_entry<D, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, true>(priv);
+    case OPL_GEN1: return flatmx_entry<D, OpList<OC_GEN>, false>(priv);
+    case OPL_GEN2: return flatmx_entry<D, OpList<OC_GEN, OC_GEN>, false>(priv);
+    case OPL_GEN4: return flatmx_entry<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv);
+    case OPL_GEN8:
+        return flatmx_entry<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv);
+    }
+    return {nullptr, 0, 0};
+}
+
+KernelChoice pick_flat1d_mx(int D, int opl, int priv)
+{
+    if (D == 2) return flatmx_by_list<2>(opl, priv);
+    if (D == 3) return flatmx_by_list<3>(opl, priv);
+    return {nullptr, 0, 0};
+}
+
+}  // namespace sfb

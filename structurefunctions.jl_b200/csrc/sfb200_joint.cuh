@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
             int db = e.base + (key > e.hi ? (e.mult & 0xffff) : 0);
             bool slow = (e.mult & LUT_FLAG_SLOW) || (key >= e.lo && key <= e.hi);
             float v[NV];
-            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
+            eval_ops(OPS{}, L, Tt, Q - L * L, Q, D, a.gen, v);
             float val = v[0];
             int vb;
             {

@@ -35,6 +35,7 @@ struct PairArgs {
     const double* U64; // FP64 SoA velocities
     const float* XF;   // FP32 SoA (mixed)
     const float* UF;
+    const double* XM;  // FP64 sphere records for the mixed kernels: p(3), U(3), W(3)[, up] (SoA)
     const void* lut;   // LutEntry64 (FP64 kernels) or LutEntry32 (mixed)
     LutGeom lg;
     int lut_bytes;     // bytes of the table copied to shared memory (0: no table)
@@ -43,6 +44,9 @@ struct PairArgs {
     int dist_linear;   // 1: LinearBinEdges search on r (flat: sqrt(r^2))
     LinearParams dlin;
     double radius;     // sphere
+    double chord_wrel; // mixed sphere: relative half-width of the chord ambiguity band at an edge
+    double chord_short;// mixed sphere: chord^2 below this is recomputed (near-coincident)
+    double chord_anti; // mixed sphere: chord^2 above this is recomputed (near-antipodal)
     int nb;            // distance bins
     int nops;          // operators (1D)
     // joint
@@ -117,10 +121,9 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n = a.n;
     LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
-    double* sx = reinterpret_cast<double*>(smem + a.lut_bytes);
-    double* su = sx + D * T;
+    double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);  // T records x(D) u(D)
     Hist hist;
-    hist.init(reinterpret_cast<unsigned char*>(su + D * T), NW, a.nb + 2, a.hist_cols);
+    hist.init(reinterpret_cast<unsigned char*>(srec + (size_t)2 * D * T), NW, a.nb + 2, a.hist_cols);
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
 
@@ -142,30 +145,30 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
         const int j0 = tj * T;
         const int jn = min(T, n - j0);
         if ((int)threadIdx.x < jn) {
+            double* rec = srec + threadIdx.x * 2 * D;
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                sx[d * T + threadIdx.x] = a.X64[(size_t)d * n + j0 + threadIdx.x];
-                su[d * T + threadIdx.x] = a.U64[(size_t)d * n + j0 + threadIdx.x];
+                rec[d] = a.X64[(size_t)d * n + j0 + threadIdx.x];
+                rec[D + d] = a.U64[(size_t)d * n + j0 + threadIdx.x];
             }
         }
         __syncthreads();
         const bool diag = ti == tj;
-        for (int jj = 0; jj < jn; ++jj) {
-            const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+        auto pair = [&](int jj, int& key, double (&v)[NV]) {
             double dx[D], du[D];
 #pragma unroll
-            for (int d = 0; d < D; ++d) {
-                dx[d] = SFB_SUB(sx[d * T + jj], xi[d]);
-                du[d] = su[d * T + jj] - ui[d];
+            for (int q = 0; q < D; ++q) {  // D double2 per record
+                const double2 t = reinterpret_cast<const double2*>(srec + jj * 2 * D)[q];
+                const int c0 = 2 * q, c1 = 2 * q + 1;
+                if (c0 < D) dx[c0] = SFB_SUB(t.x, xi[c0]); else du[c0 - D] = t.x - ui[c0 - D];
+                if (c1 < D) dx[c1] = SFB_SUB(t.y, xi[c1]); else du[c1 - D] = t.y - ui[c1 - D];
             }
             // r^2 exactly as the reference: left-to-right, no contraction (decides the bin)
             const double h2 = SFB_ADD(SFB_MUL(dx[0], dx[0]), SFB_MUL(dx[1], dx[1]));
             double r2 = h2;
             if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
-            int bin;
-            if (a.dist_linear) bin = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
-            else bin = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
-            const int key = valid ? bin : a.nb + 1;
+            if (a.dist_linear) key = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
+            else key = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
 
             double L = 0.0, Tt = 0.0, Q = 0.0;
             const double rs = rsqrt(r2);
@@ -184,9 +187,26 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
 #pragma unroll
                 for (int d = 1; d < D; ++d) Q = fma(du[d], du[d], Q);
             }
-            double v[NV];
-            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
-            hist.add(key, v, lane, warp);
+            eval_ops(OPS{}, L, Tt, Q - L * L, Q, D, a.gen, v);
+        };
+        if constexpr (Hist::RUN) {
+            if (iv) {
+#pragma unroll 2
+                for (int jj = diag ? (int)threadIdx.x + 1 : 0; jj < jn; ++jj) {
+                    int key;
+                    double v[NV];
+                    pair(jj, key, v);
+                    hist.add(key, v, lane, warp);
+                }
+            }
+        } else {
+            for (int jj = 0; jj < jn; ++jj) {
+                const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+                int key;
+                double v[NV];
+                pair(jj, key, v);
+                hist.add(valid ? key : a.nb + 1, v, lane, warp);
+            }
         }
     }
     hist.merge(a.g_sums, a.g_counts, a.nops, a.nb);
@@ -326,7 +346,7 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
                 for (int d = 1; d < D; ++d) Q = fmaf(du[d], du[d], Q);
             }
             float v[NV];
-            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
+            eval_ops(OPS{}, L, Tt, Q - L * L, Q, D, a.gen, v);
 
             slow = slow && valid;
             if (__any_sync(FULL, slow)) {
@@ -361,7 +381,7 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
                         for (int d = 1; d < D; ++d) Q64 = fma(du64[d], du64[d], Q64);
                     }
                     double v64[NV];
-                    eval_ops(OPS{}, L64, T64, Q64, D, a.gen, v64);
+                    eval_ops(OPS{}, L64, T64, Q64 - L64 * L64, Q64, D, a.gen, v64);
 #pragma unroll
                     for (int o = 0; o < NV; ++o) v[o] = (float)v64[o];
                 }
@@ -430,7 +450,7 @@ __global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
         }
         __syncthreads();
         const bool diag = ti == tj;
-        for (int jj = 0; jj < jn; ++jj) {
+        auto pair = [&](int jj, int& key, double (&v)[NV]) {
             SphPoint B;
             B.p[0] = sx[0 * T + jj]; B.p[1] = sx[1 * T + jj]; B.p[2] = sx[2 * T + jj];
             B.E[0] = sx[3 * T + jj]; B.E[1] = sx[4 * T + jj];
@@ -440,8 +460,7 @@ __global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
             int bin;
             if (a.dist_linear) bin = linear_bin(a.dlin, r);
             else bin = (r != r) ? a.n_edges : lut64_bin(lut, a, r);
-            const bool valid = iv && ok && (!diag || jj > (int)threadIdx.x);
-            const int key = valid ? bin : a.nb + 1;
+            key = ok ? bin : a.nb + 1;
             double uB[D], du[D];
 #pragma unroll
             for (int d = 0; d < D; ++d) uB[d] = su[d * T + jj];
@@ -449,9 +468,25 @@ __global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
             const double L = du[0], Tt = du[1];
             double Q = du[0] * du[0] + du[1] * du[1];
             if constexpr (D == 3) Q = fma(du[2], du[2], Q);
-            double v[NV];
-            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
-            hist.add(key, v, lane, warp);
+            eval_ops(OPS{}, L, Tt, Q - L * L, Q, D, a.gen, v);
+        };
+        if constexpr (Hist::RUN) {
+            if (iv) {
+                for (int jj = diag ? (int)threadIdx.x + 1 : 0; jj < jn; ++jj) {
+                    int key;
+                    double v[NV];
+                    pair(jj, key, v);
+                    hist.add(key, v, lane, warp);
+                }
+            }
+        } else {
+            for (int jj = 0; jj < jn; ++jj) {
+                const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+                int key;
+                double v[NV];
+                pair(jj, key, v);
+                hist.add(valid ? key : a.nb + 1, v, lane, warp);
+            }
         }
     }
     hist.merge(a.g_sums, a.g_counts, a.nops, a.nb);
@@ -545,7 +580,7 @@ __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
                 }
             }
             float v[NV];
-            eval_ops(OPS{}, L, Tt, Q, D, a.gen, v);
+            eval_ops(OPS{}, L, Tt, Q - L * L, Q, D, a.gen, v);
 
             slow = slow && valid;
             bool ok = true;
@@ -567,7 +602,7 @@ __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
                     double Q64 = du[0] * du[0] + du[1] * du[1];
                     if constexpr (D == 3) Q64 = fma(du[2], du[2], Q64);
                     double v64[NV];
-                    eval_ops(OPS{}, du[0], du[1], Q64, D, a.gen, v64);
+                    eval_ops(OPS{}, du[0], du[1], Q64 - du[0] * du[0], Q64, D, a.gen, v64);
 #pragma unroll
                     for (int o = 0; o < NV; ++o) v[o] = (float)v64[o];
                 }

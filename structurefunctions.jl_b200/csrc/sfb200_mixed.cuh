@@ -1,0 +1,609 @@
+// sfb200_mixed.cuh -- the mixed-precision pair kernels (precision SFB200_PREC_MIXED).
+//
+// Split of the arithmetic:
+//   FP64  every difference of two points (dx, du; the sphere's chord d = q - p, s = p + q and the
+//         tangent-velocity differences), the squared distance that decides the bin, and the dot /
+//         cross-product numerators of the projections (p = dx . du, the cross product dx x du).
+//         The differences are then exact to a rounding, so the numerators keep full relative
+//         accuracy even when the projection cancels (du nearly perpendicular to r): a pair's value
+//         is accurate to a few FP32 ulps relative to itself, which keeps every bin within the
+//         1e-6 per-bin tolerance down to bins holding a single pair.
+//   FP32  the normalisation by 1/r (rsqrtf), every operator power, and the accumulation (per-lane
+//         run sums folded into the block FP64 histogram, see sfb200_acc.cuh).
+// The flat squared distance is computed exactly as the reference (left to right, no contraction),
+// so the bin comes from the exact FP64 table and no pair is rechecked. The sphere bins on the FP64
+// chord |q - p|^2 against the chord images of the edges and recomputes with the reference frame
+// in FP64 the pairs within 2^-40 (relative) of an edge image, near-coincident and near-antipodal
+// pairs. Transverse quantities avoid Q - L^2: T2 is |dx x du|^2 / r^2 (3D) or T^2 (2D), and Q is
+// L^2 + T2.
+#pragma once
+
+#include "sfb200_joint.cuh"
+
+namespace sfb {
+
+// FP32 image of an FP64 value (round to nearest).
+__device__ __forceinline__ float f32(double v) { return __double2float_rn(v); }
+
+// Loads `NP` double2 from shared memory into r[2 * NP].
+template <int NP>
+__device__ __forceinline__ void load_rec2(const double* base, double (&r)[2 * NP])
+{
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+        const double2 t = reinterpret_cast<const double2*>(base)[q];
+        r[2 * q] = t.x;
+        r[2 * q + 1] = t.y;
+    }
+}
+
+// Velocity scale: velocities are multiplied by us = 2^-ku (exact) when they are loaded, with
+// |u| us <= 1 from the pack kernel's bound, so every FP32 value is of order one: an operator of order
+// k then carries us^k, removed exactly at the merge. Coordinates are not scaled (the squared distance
+// decides the bin and stays the reference's); pairs whose squared distance leaves [2^-100, 2^100]
+// (and, for the 3D transverse direction, whose horizontal part does) are evaluated in FP64.
+__device__ __forceinline__ int pow2_exponent_above(unsigned long long bound_bits)
+{
+    // smallest k with bound <= 2^k (0 for a zero or non-finite bound)
+    const double b = __longlong_as_double((long long)bound_bits);
+    if (!(b > 0.0) || !(b < 1e300)) return 0;
+    int e;
+    const double m = frexp(b, &e);  // b = m 2^e, m in [0.5, 1)
+    return m == 0.5 ? e - 1 : e;
+}
+
+// Order of operator K (its sums scale as us^order).
+template <int K>
+__device__ __forceinline__ int op_order_of(const sfb200_operator& g)
+{
+    if constexpr (K == OC_L1) return 1;
+    else if constexpr (K == OC_L2 || K == OC_T2 || K == OC_S2 || K == OC_T2C) return 2;
+    else if constexpr (K == OC_L3 || K == OC_T3 || K == OC_S3 || K == OC_L1T2 || K == OC_L2T1 || K == OC_L1T2C) return 3;
+    else {
+        switch (g.kind) {
+        case SFB200_OP_PROJECTED: return g.nl + g.nt;
+        case SFB200_OP_S2: case SFB200_OP_T2C: return 2;
+        case SFB200_OP_S3: case SFB200_OP_L1T2C: return 3;
+        case SFB200_OP_FULLVEC: return g.nf;
+        }
+        return 0;
+    }
+}
+
+template <int... K>
+__device__ __forceinline__ void op_unscale(OpList<K...>, const GenOps& g, int ku, double (&sc)[sizeof...(K)])
+{
+    int k = 0;
+    ((sc[k] = ldexp(1.0, ku * op_order_of<K>(g.op[k])), ++k), ...);
+}
+
+__device__ __forceinline__ bool f32_range_ok(float v) { return v >= 0x1p-100f && v <= 0x1p100f; }
+
+// Approximate reciprocal square root (rsqrt.approx) for arguments known to be normal: no
+// denormal handling is needed around it.
+__device__ __forceinline__ float rsqrt_normal(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Per-pair FP32 primitives of a flat pair from FP64 differences (du already scaled by us).
+// Returns false when the pair must be evaluated in FP64 (squared distances outside FP32's range).
+template <int D, class OPS>
+__device__ __forceinline__ bool flat_primitives_mx(const double (&dx)[D], const double (&du)[D], double r2, double h2,
+                                                   float& L, float& Tt, float& T2, float& Q)
+{
+    using N = ListNeeds2<OPS>;
+    const float r2f = f32(r2);
+    bool fine = f32_range_ok(r2f);
+    const float rs = rsqrt_normal(r2f);
+    L = 0.f;
+    Tt = 0.f;
+    T2 = 0.f;
+    Q = 0.f;
+    double p = 0.0;
+    if constexpr (N::L || N::T2 || N::Q) {
+        p = dx[0] * du[0];
+#pragma unroll
+        for (int d = 1; d < D; ++d) p = fma(dx[d], du[d], p);
+        L = f32(p) * rs;
+    }
+    // cz = (dx x du)_z: the signed transverse numerator in 2D and 3D (n_hat = z_hat x r_hat)
+    double cz = 0.0;
+    if constexpr (N::T || (D == 2 && (N::T2 || N::Q))) cz = fma(dx[0], du[1], -(dx[1] * du[0]));
+    if constexpr (D == 2) {
+        if constexpr (N::T || N::T2 || N::Q) {
+            Tt = f32(cz) * rs;
+            T2 = Tt * Tt;
+        }
+    } else {
+        if constexpr (N::T) {
+            const float h2f = f32(h2);
+            fine = fine && f32_range_ok(h2f);
+            Tt = f32(cz) * rsqrt_normal(h2f);
+        }
+        if constexpr (N::T2 || N::Q) {
+            // |dx x du|^2 = |dx|^2 |du|^2 - (dx . du)^2 (Lagrange), in FP64
+            double q = du[0] * du[0];
+#pragma unroll
+            for (int d = 1; d < D; ++d) q = fma(du[d], du[d], q);
+            const double c2 = fma(q, r2, -(p * p));
+            T2 = f32(c2) * (rs * rs);
+        }
+    }
+    if constexpr (N::Q) Q = fmaf(L, L, T2);
+    return fine;
+}
+
+// FP64 values of a flat pair (the FP64 kernel's formulas) rounded to FP32; du already scaled.
+template <int D, class OPS>
+__device__ __forceinline__ void flat_values_fp64(const double (&dx)[D], const double (&du)[D], double r2, double h2,
+                                                 const GenOps& g, float (&v)[OPS::n])
+{
+    constexpr int NV = OPS::n;
+    const double rs = rsqrt(r2);
+    double pp = dx[0] * du[0];
+#pragma unroll
+    for (int d = 1; d < D; ++d) pp = fma(dx[d], du[d], pp);
+    const double L = pp * rs;
+    const double t = fma(du[1], dx[0], -du[0] * dx[1]);
+    const double Tt = (D == 2) ? t * rs : t * rsqrt(h2);
+    double Q = du[0] * du[0];
+#pragma unroll
+    for (int d = 1; d < D; ++d) Q = fma(du[d], du[d], Q);
+    double v64[NV];
+    eval_ops(OPS{}, L, Tt, Q - L * L, Q, D, g, v64);
+#pragma unroll
+    for (int o = 0; o < NV; ++o) v[o] = f32(v64[o]);
+}
+
+// ================================================================================================
+// Flat (Euclidean) 1D
+//
+// The run-length histogram (PRIV 3) needs no warp-synchronous step, so each lane walks its own
+// range of j (j > i on a diagonal tile) and no pair is masked; the other histogram modes step the
+// warp in lockstep with out-of-range pairs sent to the dropped row.
+// ================================================================================================
+template <int D, class OPS, int PRIV>
+__global__ void __launch_bounds__(256) k_flat1d_mx(const PairArgs a)
+{
+    constexpr int NV = OPS::n;
+    constexpr int NP = D;  // double2 per j record: x(D) u(D)
+    using Hist = BlockHist<float, NV, PRIV>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x, NW = T >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n = a.n;
+    LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
+    double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);  // T records of 2D doubles
+    Hist hist;
+    hist.init(reinterpret_cast<unsigned char*>(srec + (size_t)2 * NP * T), NW, a.nb + 2, a.hist_cols);
+    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
+        lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
+    const int ku = pow2_exponent_above(a.g_stats[2]);
+    const double us = ldexp(1.0, -ku);
+    double unscale[NV];
+    op_unscale(OPS{}, a.gen, ku, unscale);
+
+    int iter = 0;
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        hist.close_runs(lane);
+        if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + threadIdx.x;
+        const bool iv = i < n;
+        double xi[D], ui[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            xi[d] = iv ? a.X64[(size_t)d * n + i] : 0.0;
+            ui[d] = iv ? a.U64[(size_t)d * n + i] * us : 0.0;
+        }
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+            double* rec = srec + threadIdx.x * 2 * NP;
+            const int jg = j0 + threadIdx.x;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                rec[d] = a.X64[(size_t)d * n + jg];
+                rec[D + d] = a.U64[(size_t)d * n + jg] * us;
+            }
+        }
+        __syncthreads();
+        const bool diag = ti == tj;
+        // one pair: key (bin) and values
+        auto pair = [&](int jj, int& key, float (&v)[NV]) {
+            double rj[2 * NP];
+            load_rec2<NP>(srec + jj * 2 * NP, rj);
+            double dx[D], du[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                dx[d] = SFB_SUB(rj[d], xi[d]);
+                du[d] = rj[D + d] - ui[d];
+            }
+            // r^2 exactly as the reference: left-to-right, no contraction (decides the bin)
+            const double h2 = SFB_ADD(SFB_MUL(dx[0], dx[0]), SFB_MUL(dx[1], dx[1]));
+            double r2 = h2;
+            if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
+            if (a.dist_linear) key = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
+            else key = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+            float L, Tt, T2, Q;
+            const bool fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q);
+            eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
+            if (!fine) flat_values_fp64<D, OPS>(dx, du, r2, h2, a.gen, v);
+        };
+        if constexpr (Hist::RUN) {
+            if (iv) {
+#pragma unroll 2
+                for (int jj = diag ? (int)threadIdx.x + 1 : 0; jj < jn; ++jj) {
+                    int key;
+                    float v[NV];
+                    pair(jj, key, v);
+                    hist.add(key, v, lane, warp);
+                }
+            }
+        } else {
+            for (int jj = 0; jj < jn; ++jj) {
+                const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+                int key;
+                float v[NV];
+                pair(jj, key, v);
+                hist.add(valid ? key : a.nb + 1, v, lane, warp);
+            }
+        }
+    }
+    hist.merge(a.g_sums, a.g_counts, a.nops, a.nb, unscale);
+}
+
+// ================================================================================================
+// Sphere 1D
+//
+// Per point (FP64, built by the pack kernel): p (unit position), U = u_e E + u_n N (ambient tangent
+// velocity), W = u_n E - u_e N (U turned by a quarter), [u_up]. With d = q - p and s = p + q the
+// reference's transported increments are du_L = d . (U_B - U_A) / sin(sigma) and
+// du_T = d . (W_B - W_A) / sin(sigma), with sin^2(sigma) = |d|^2 |s|^2 / 4.
+// ================================================================================================
+// Chord-key bin from the FP64 table with its ambiguity test.
+__device__ __forceinline__ int sphere_chord_bin(const LutEntry64* lut, const PairArgs& a, double ch2, bool& slow)
+{
+    const LutEntry64 e = lut[lut_cell64(ch2, a.lg)];
+    slow = (e.mult & LUT_FLAG_SLOW) || fabs(ch2 - e.e) <= a.chord_wrel * e.e || ch2 < a.chord_short ||
+           ch2 > a.chord_anti || ch2 != ch2;
+    return e.base + (ch2 > e.e ? e.mult : 0);
+}
+
+// FP64 reference recomputation of a sphere pair: bin (nb + 1 when the frame is degenerate) and the
+// values scaled by us^order in FP32. Kept out of line (it is rare and large); inputs and the result
+// travel by value so that the caller's arrays stay in registers.
+template <int NV>
+struct ExactPair {
+    float v[NV];
+    int bin;
+};
+
+template <int D, class OPS>
+__device__ __forceinline__ ExactPair<OPS::n> sphere_pair_exact(const PairArgs& a, int i, int j, int ku)
+{
+    constexpr int NV = OPS::n;
+    ExactPair<NV> res;
+    double unscale[NV];
+    op_unscale(OPS{}, a.gen, ku, unscale);
+    SphPoint A, B;
+    load_sph64(a.X64, a.n, i, A);
+    load_sph64(a.X64, a.n, j, B);
+    double r, tA[2], tB[2], uA[D], uB[D], du[D];
+    const bool ok = x_sphere_frame(A, B, a.radius, r, tA, tB);
+    res.bin = ok ? sphere_exact_bin(a, r) : a.nb + 1;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        uA[d] = a.U64[(size_t)d * a.n + i];
+        uB[d] = a.U64[(size_t)d * a.n + j];
+    }
+    x_sphere_delta<D>(tA, tB, uA, uB, du);
+    double Q64 = du[0] * du[0] + du[1] * du[1];
+    if constexpr (D == 3) Q64 = fma(du[2], du[2], Q64);
+    double v64[NV];
+    eval_ops(OPS{}, du[0], du[1], Q64 - du[0] * du[0], Q64, D, a.gen, v64);
+#pragma unroll
+    for (int o = 0; o < NV; ++o) res.v[o] = f32(v64[o] / unscale[o]);
+    return res;
+}
+
+// Per-pair FP32 primitives of a sphere pair from the FP64 records (fields: p 0-2, U 3-5, W 6-8,
+// up 9; velocities already scaled by us). Returns the chord^2.
+template <int D, class OPS>
+__device__ __forceinline__ double sphere_primitives_mx(const double* ra, const double* rb, float& L, float& Tt,
+                                                       float& T2, float& Q)
+{
+    using N = ListNeeds2<OPS>;
+    double d[3], sv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        d[c] = rb[c] - ra[c];
+        sv[c] = rb[c] + ra[c];
+    }
+    const double ch2 = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
+    const double ss = fma(sv[2], sv[2], fma(sv[1], sv[1], sv[0] * sv[0]));
+    // chord^2 and |s|^2 lie in [0, 4]; out-of-range products only occur for the near-coincident or
+    // near-antipodal pairs that are recomputed anyway
+    const float inv_s = rsqrt_normal(0.25f * f32(ch2) * f32(ss));
+    L = 0.f;
+    Tt = 0.f;
+    T2 = 0.f;
+    Q = 0.f;
+    if constexpr (N::L || N::Q) {
+        double pl = d[0] * (rb[3] - ra[3]);
+        pl = fma(d[1], rb[4] - ra[4], pl);
+        pl = fma(d[2], rb[5] - ra[5], pl);
+        L = f32(pl) * inv_s;
+    }
+    if constexpr (N::T || N::T2 || N::Q) {
+        double pt = d[0] * (rb[6] - ra[6]);
+        pt = fma(d[1], rb[7] - ra[7], pt);
+        pt = fma(d[2], rb[8] - ra[8], pt);
+        Tt = f32(pt) * inv_s;
+        T2 = Tt * Tt;
+        if constexpr (D == 3) {
+            const float dw = f32(rb[9] - ra[9]);
+            T2 = fmaf(dw, dw, T2);
+        }
+    }
+    if constexpr (N::Q) Q = fmaf(L, L, T2);
+    return ch2;
+}
+
+template <int D, class OPS, int PRIV>
+__global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
+{
+    constexpr int NV = OPS::n;
+    constexpr int NP = 5;  // double2 per record: p(3) U(3) W(3) up/pad(1)
+    using Hist = BlockHist<float, NV, PRIV>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x, NW = T >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n = a.n;
+    LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
+    double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);
+    __shared__ unsigned long long s_recheck;
+    Hist hist;
+    hist.init(reinterpret_cast<unsigned char*>(srec + (size_t)2 * NP * T), NW, a.nb + 2, a.hist_cols);
+    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
+        lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
+    if (threadIdx.x == 0) s_recheck = 0ull;
+    unsigned my_recheck = 0;
+    const int ku = pow2_exponent_above(a.g_stats[2]);
+    const double us = ldexp(1.0, -ku);
+    double unscale[NV];
+    op_unscale(OPS{}, a.gen, ku, unscale);
+    constexpr int NF = 9 + (D == 3);  // stored fields
+
+    int iter = 0;
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        hist.close_runs(lane);
+        if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + threadIdx.x;
+        const bool iv = i < n;
+        double ra[2 * NP];
+#pragma unroll
+        for (int c = 0; c < 2 * NP; ++c)
+            ra[c] = (iv && c < NF) ? a.XM[(size_t)c * n + i] * (c < 3 ? 1.0 : us) : 0.0;
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+            double* rec = srec + threadIdx.x * 2 * NP;
+            const int jg = j0 + threadIdx.x;
+#pragma unroll
+            for (int c = 0; c < 2 * NP; ++c) rec[c] = (c < NF) ? a.XM[(size_t)c * n + jg] * (c < 3 ? 1.0 : us) : 0.0;
+        }
+        __syncthreads();
+        const bool diag = ti == tj;
+        auto pair = [&](int jj, int& key, float (&v)[NV]) {
+            double rb[2 * NP];
+            load_rec2<NP>(srec + jj * 2 * NP, rb);
+            float L, Tt, T2, Q;
+            const double ch2 = sphere_primitives_mx<D, OPS>(ra, rb, L, Tt, T2, Q);
+            bool slow;
+            key = sphere_chord_bin(lut, a, ch2, slow);
+            eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
+            if (slow) {
+                const ExactPair<NV> ex = sphere_pair_exact<D, OPS>(a, i, j0 + jj, ku);
+                key = ex.bin;
+#pragma unroll
+                for (int o = 0; o < NV; ++o) v[o] = ex.v[o];
+                ++my_recheck;
+            }
+        };
+        if constexpr (Hist::RUN) {
+            if (iv) {
+#pragma unroll 2
+                for (int jj = diag ? (int)threadIdx.x + 1 : 0; jj < jn; ++jj) {
+                    int key;
+                    float v[NV];
+                    pair(jj, key, v);
+                    hist.add(key, v, lane, warp);
+                }
+            }
+        } else {
+            for (int jj = 0; jj < jn; ++jj) {
+                const bool valid = iv && (!diag || jj > (int)threadIdx.x);
+                int key;
+                float v[NV];
+                if (valid) pair(jj, key, v);
+                else {
+                    key = a.nb + 1;
+#pragma unroll
+                    for (int o = 0; o < NV; ++o) v[o] = 0.f;
+                }
+                hist.add(key, v, lane, warp);
+            }
+        }
+    }
+    if (my_recheck) atomicAdd(&s_recheck, (unsigned long long)my_recheck);
+    hist.merge(a.g_sums, a.g_counts, a.nops, a.nb, unscale);
+    if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
+}
+
+// ================================================================================================
+// Joint (distance x value) histogram
+//
+// The value comes from the FP64 numerators, so its FP32 error is relative to itself (a few ulps):
+// the value-bin index t = (v - first) / step is trusted when it lies more than
+// (|t| + |first / step|) * vrel from an integer; closer pairs, sphere pairs in the chord ambiguity
+// band and every pair of a vector value axis are recomputed in FP64 with the reference formula.
+// Cells accumulate counts and fixed-point offsets from the value-bin centres (sfb200_joint.cuh).
+// ================================================================================================
+template <bool SPHERE, int D, class OPS>
+__global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
+{
+    constexpr int NP = SPHERE ? 5 : D;
+    constexpr int NF = SPHERE ? 9 + (D == 3) : 2 * D;  // stored fields per record
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x;
+    const int n = a.n;
+    const int nd = a.nb, nv = a.nv;
+    const int ncell = nd * nv;
+    LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
+    double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);                                // T * 2NP
+    unsigned long long* hres = reinterpret_cast<unsigned long long*>(srec + (size_t)2 * NP * T);  // ncell
+    unsigned* hc = reinterpret_cast<unsigned*>(hres + ncell);                                     // ncell
+    __shared__ unsigned long long s_recheck;
+
+    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
+        lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
+    for (int k = threadIdx.x; k < ncell; k += T) { hres[k] = 0ull; hc[k] = 0u; }
+    if (threadIdx.x == 0) s_recheck = 0ull;
+    unsigned my_recheck = 0;
+    const int ku = pow2_exponent_above(a.g_stats[2]);
+    const double us = ldexp(1.0, -ku);
+    double unscale[1];
+    op_unscale(OPS{}, a.gen, ku, unscale);
+    // the FP32 value is v us^k: fold us^-k into the index scale (every pair exact if that overflows)
+    const float vinv = (float)(a.vlin.inv_step * unscale[0]);
+    const bool vfast = a.val_linear && isfinite(vinv) && vinv != 0.f;
+    const float vnegf = (float)a.vlin.neg_f_inv;
+    const float tmax = (float)(a.vlin.n - 1);
+
+    // field c of point k as staged: sphere XM (velocity fields scaled), flat x then u (u scaled)
+    auto field = [&](int c, int k) -> double {
+        if constexpr (SPHERE) return a.XM[(size_t)c * n + k] * (c < 3 ? 1.0 : us);
+        else return c < D ? a.X64[(size_t)c * n + k] : a.U64[(size_t)(c - D) * n + k] * us;
+    };
+
+    int iter = 0;
+    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+        if (iter && iter % a.flush_every == 0) {
+            __syncthreads();
+            joint_flush_mixed(a, hres, hc, ncell);
+        }
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + threadIdx.x;
+        const bool iv = i < n;
+        double ra[2 * NP];
+#pragma unroll
+        for (int c = 0; c < 2 * NP; ++c) ra[c] = (iv && c < NF) ? field(c, i) : 0.0;
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+            double* rec = srec + threadIdx.x * 2 * NP;
+#pragma unroll
+            for (int c = 0; c < 2 * NP; ++c) rec[c] = c < NF ? field(c, j0 + threadIdx.x) : 0.0;
+        }
+        __syncthreads();
+        if (!iv) continue;
+        const bool diag = ti == tj;
+        for (int jj = diag ? (int)threadIdx.x + 1 : 0; jj < jn; ++jj) {
+            double rb[2 * NP];
+            load_rec2<NP>(srec + jj * 2 * NP, rb);
+            float L, Tt, T2, Q;
+            int db;
+            bool slow = false, fine = true;
+            if constexpr (SPHERE) {
+                const double ch2 = sphere_primitives_mx<D, OPS>(ra, rb, L, Tt, T2, Q);
+                db = sphere_chord_bin(lut, a, ch2, slow);
+            } else {
+                double dx[D], du[D];
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    dx[d] = SFB_SUB(rb[d], ra[d]);
+                    du[d] = rb[D + d] - ra[D + d];
+                }
+                const double h2 = SFB_ADD(SFB_MUL(dx[0], dx[0]), SFB_MUL(dx[1], dx[1]));
+                double r2 = h2;
+                if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
+                if (a.dist_linear) db = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
+                else db = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+                // flat bins are exact: a pair outside the distance range needs no value
+                if (db < 1 || db > nd) continue;
+                fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q);
+            }
+            float v[1];
+            eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
+            const float val = v[0];
+            int vb = 0;
+            if (vfast) {
+                const float t = fmaf(val, vinv, vnegf);
+                const float fl = floorf(t);
+                const float fr = t - fl;
+                const float wt = (fabsf(t) + fabsf(vnegf)) * a.vrel;
+                vb = (t <= 0.f) ? 0 : ((t > tmax) ? a.vlin.n : (int)fl + 1);
+                slow = slow || !fine || fr < wt || fr > 1.f - wt || fabsf(t) < wt || fabsf(t - tmax) < wt ||
+                       !(t == t);
+            } else {
+                slow = true;  // vector value edges (or an unrepresentable index scale): exact FP64 search
+            }
+            double v64 = 0.0;
+            bool ok = true;
+            if (slow) {
+                const int j = j0 + jj;
+                double du64[D];
+                if constexpr (!SPHERE) {
+                    double dx64[D];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        dx64[d] = SFB_SUB(a.X64[(size_t)d * n + j], a.X64[(size_t)d * n + i]);
+                        du64[d] = SFB_SUB(a.U64[(size_t)d * n + j], a.U64[(size_t)d * n + i]);
+                    }
+                    const double r264 = x_dot<D>(dx64, dx64);
+                    db = flat_exact_bin(a, r264);
+                    v64 = x_sf_raw<D>(a.gen.op[0], du64, dx64, r264);
+                } else {
+                    SphPoint A, B;
+                    load_sph64(a.X64, n, i, A);
+                    load_sph64(a.X64, n, j, B);
+                    double r, tA[2], tB[2], uA[D], uB[D];
+                    ok = x_sphere_frame(A, B, a.radius, r, tA, tB);
+                    db = sphere_exact_bin(a, r);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        uA[d] = a.U64[(size_t)d * n + i];
+                        uB[d] = a.U64[(size_t)d * n + j];
+                    }
+                    x_sphere_delta<D>(tA, tB, uA, uB, du64);
+                    v64 = x_sphere_value<D>(a.gen.op[0], du64);
+                }
+                vb = value_exact_bin(a, v64);
+                ++my_recheck;
+            }
+            if (ok && db >= 1 && db <= nd && vb >= 1 && vb <= nv) {
+                const int cell = (db - 1) + nd * (vb - 1);
+                const double off = (slow ? v64 : (double)val * unscale[0]) - value_center(a, vb);
+                atomicAdd(&hres[cell], (unsigned long long)__double2ll_rn(off * a.vq));
+                atomicAdd(&hc[cell], 1u);
+            }
+        }
+    }
+    if (my_recheck) atomicAdd(&s_recheck, (unsigned long long)my_recheck);
+    __syncthreads();
+    joint_flush_mixed(a, hres, hc, ncell);
+    if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
+}
+
+}  // namespace sfb

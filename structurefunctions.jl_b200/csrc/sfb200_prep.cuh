@@ -193,7 +193,7 @@ __global__ void k_pack_flat(const TX* __restrict__ x, const TU* __restrict__ u, 
 template <typename TX, typename TU>
 __global__ void k_pack_sphere(const TX* __restrict__ x, const TU* __restrict__ u, int n, int D,
                               int unit, const int* __restrict__ perm, double* X64, double* U64, float* XF,
-                              unsigned long long* bound)
+                              double* XM, unsigned long long* bound)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t src = (i < n && perm) ? (size_t)perm[i] : (size_t)i;
@@ -221,6 +221,13 @@ __global__ void k_pack_sphere(const TX* __restrict__ x, const TU* __restrict__ u
     for (int d = 0; d < D; ++d) {
         uv[d] = (double)u[(size_t)D * src + d];
         U64[(size_t)d * n + i] = uv[d];
+    }
+    if (XM) {
+        // FP64 records: p at 0..2, U at 3..5, W at 6..8, up at 9
+        const double ue = uv[0], un = uv[1];
+        const double m[10] = {p0, p1, p2, ue * E0 + un * N0, ue * E1 + un * N1, un * N2,
+                              un * E0 - ue * N0, un * E1 - ue * N1, -ue * N2, uv[2]};
+        for (int k = 0; k < 9 + (D == 3); ++k) XM[(size_t)k * n + i] = m[k];
     }
     if (XF) {
         // records of (hi, lo) pairs: p at 0..5, U at 6..11, W at 12..17, up at 18..19

@@ -36,6 +36,8 @@ BINS_LINEAR = 2
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_FP32 = 2
+PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED, "fp32": PREC_FP32}
 
 F64 = 0
 F32 = 1

@@ -47,13 +47,15 @@ def _context(device):
 class B200Backend:
     """Execution backend that runs the pair loop on a B200 through libsfb200.so.
 
-    precision: "mixed" (FP32 bulk, FP64 recheck near bin edges, FP64 merge) or "fp64" (every
-    pair in FP64). Plans are cached per (operator set, bins, metric, dtypes).
+    precision: "mixed" (FP64 differences, squared distance and projection numerators; FP32
+    normalisation, powers and accumulation; FP64 merge), "fp64" (every pair in FP64) or "fp32"
+    (FP32 bulk with an FP64 recheck of bin membership). Plans are cached per (operator set, bins,
+    metric, dtypes).
     """
 
     def __init__(self, device=0, precision="mixed", tile=0):
-        if precision not in ("mixed", "fp64"):
-            raise ArgumentError("precision must be 'mixed' or 'fp64'")
+        if precision not in _abi.PRECISIONS:
+            raise ArgumentError("precision must be 'mixed', 'fp64' or 'fp32'")
         self.device = int(device)
         self.precision = precision
         self.tile = int(tile)
@@ -235,7 +237,7 @@ def plan_description(ops, D, distance_bins, value_bins=None, distance_metric=Non
     desc.joint = 1 if value_bins is not None else 0
     if value_bins is not None:
         desc.value = as_bin_edges(value_bins).value_abi(keep)
-    desc.precision = _abi.PREC_MIXED if precision == "mixed" else _abi.PREC_FP64
+    desc.precision = _abi.PRECISIONS[precision]
     desc.x_dtype = _dtype_code(np.dtype(x_dtype))
     desc.u_dtype = _dtype_code(np.dtype(u_dtype))
     return desc, keep

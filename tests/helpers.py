@@ -5,6 +5,9 @@ import numpy as np
 # sum of absolute values), which is the meaningful scale for signed and near-cancelling bins.
 TOL_FP64 = 1e-12
 TOL_MIXED = 1e-6
+# FP32-bulk kernels: each pair value carries FP32 rounding of its differences, ~1e-7 |du|^k absolute,
+# which in bins of a few near-cancelling pairs reaches a few 1e-6 of sum|v|.
+TOL_FP32 = 2e-5
 
 
 def compare(gpu_sums, gpu_counts, ref_sums, ref_counts, scale, tol):

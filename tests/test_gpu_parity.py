@@ -9,14 +9,14 @@ import numpy as np
 import pytest
 
 import oracle_py
-from helpers import TOL_FP64, TOL_MIXED, compare
+from helpers import TOL_FP32, TOL_FP64, TOL_MIXED, compare
 import sfb200 as SF
 from sfb200 import _abi, _lib, synthetic
 from sfb200.api import plan_description
 
 pytestmark = pytest.mark.gpu
 
-PRECISIONS = [("fp64", TOL_FP64), ("mixed", TOL_MIXED)]
+PRECISIONS = [("fp64", TOL_FP64), ("mixed", TOL_MIXED), ("fp32", TOL_FP32)]
 
 
 def run_gpu(ops, x, u, bins, metric=None, value_bins=None, precision="mixed", tile=0, priv=None, options=None):
@@ -204,7 +204,7 @@ def test_joint_point_order(precision, tol):
         compare(gs, gc, rs, rc, ra, tol)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
 def test_tiny_and_empty(precision):
     be = SF.B200Backend(precision=precision)
     for n in (0, 1, 2, 3):
@@ -215,7 +215,7 @@ def test_tiny_and_empty(precision):
         assert int(r.counts.sum()) == n * (n - 1) // 2
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
 def test_points_on_edges_exact(precision):
     """Pairs placed exactly on bin edges (right-inclusive) and at edge +- 1 ulp."""
     edges = np.array([0.1, 0.2, 0.3, 0.5])
@@ -226,3 +226,21 @@ def test_points_on_edges_exact(precision):
     x[0] = xs
     u = np.random.default_rng(3).standard_normal((2, len(xs)))
     check((SF.L2SF,), x, u, edges, precision=precision, tol=TOL_MIXED)
+
+
+@pytest.mark.parametrize("xscale,uscale", [(1e-15, 1e30), (1e12, 1e-25), (3.0, 7.0)])
+def test_mixed_extreme_scales(xscale, uscale):
+    """The mixed kernels scale into FP32 range exactly: coordinates and velocities far outside
+    FP32's comfortable range (third-order values ~1e90 or ~1e-75) keep the 1e-6 tolerance."""
+    w = synthetic.config("c1", n=1200)
+    x = w.x * xscale
+    u = w.u * uscale
+    edges = w.distance_bins.edges * xscale
+    check(w.ops, x, u, edges, precision="mixed", tol=TOL_MIXED)
+    ws = synthetic.config("c2", n=800)
+    check(ws.ops, ws.x, ws.u.astype(np.float64) * uscale, ws.distance_bins.edges, metric=ws.metric,
+          precision="mixed", tol=TOL_MIXED)
+    wj = synthetic.config("c3", n=1500)
+    vb = SF.LinearBinEdges(wj.value_bins.first_edge * uscale, wj.value_bins.last_edge * uscale, len(wj.value_bins))
+    check(wj.ops, wj.x.astype(np.float64) * xscale, wj.u.astype(np.float64) * uscale,
+          wj.distance_bins.edges * xscale, value_bins=vb, precision="mixed", tol=TOL_MIXED)
