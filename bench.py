@@ -224,10 +224,15 @@ def run_ours(args):
     same_counts = bool(torch.equal(mcounts, fcounts)) and bool(torch.equal(hcounts, fcounts))
 
     def max_rel_dev(a, b):
-        a = a.cpu().numpy()
-        b = b.cpu().numpy()
-        ok = np.isfinite(b) & (np.abs(b) > 0)
-        return float(np.max(np.abs(a[ok] - b[ok]) / np.abs(b[ok]))) if ok.any() else 0.0
+        # per operator: max over bins of |a - b| / |b| (sign-definite operators: the tolerance figure;
+        # signed ones: near-cancelling bins make it large, see the CPU-oracle parity tests)
+        a = a.cpu().numpy().reshape(-1, mixed.n_counts if w.value_bins is None else mixed.n_sums)
+        b = b.cpu().numpy().reshape(a.shape)
+        out = []
+        for k in range(a.shape[0]):
+            ok = np.isfinite(b[k]) & (np.abs(b[k]) > 0)
+            out.append(float(np.max(np.abs(a[k][ok] - b[k][ok]) / np.abs(b[k][ok]))) if ok.any() else 0.0)
+        return out
 
     dev_mixed = max_rel_dev(msums, fsums)
     dev_fp32 = max_rel_dev(hsums, fsums)
@@ -322,11 +327,11 @@ def run_ours(args):
                      "roofline_frac_fp64": (achieved64 / peak64) if peak64 else None},
             "fp32": {"value": fp32_value, "unit": UNIT, "ms_per_step": ms_fp32, "kernel_ms": kmed_fp32,
                      "rechecked_pairs_per_step": st_fp32["rechecked"],
-                     "max_rel_dev_vs_fp64": dev_fp32,
+                     "max_rel_dev_vs_fp64_per_operator": dev_fp32,
                      "note": "FP32-bulk kernel: FP32 differences, FP64 recheck of bin membership only"},
             "mixed_over_fp64": value / fp64_value,
             "counts_equal_all_precisions": same_counts,
-            "mixed_max_rel_dev_vs_fp64": dev_mixed,
+            "mixed_max_rel_dev_vs_fp64_per_operator": dev_mixed,
             "rechecked_pairs_per_step": st_mixed["rechecked"],
             "roofline": {
                 "bound": "fp32",
@@ -336,6 +341,8 @@ def run_ours(args):
                 "frac": (achieved / peak32) if peak32 else None,
                 "traffic": traffic,
                 "flops_per_pair": flops,
+                "flops_per_pair_source": "reference FP64 formula (frozen in synthetic.FLOPS); the mixed kernel's own "
+                                         f"formulation performs {synthetic.KERNEL_FLOPS[args.config]} per pair",
                 "kernel_ms": kmed_mixed,
                 "peak_source": "measured FP32 FMA probe on this GPU (MEASURED_PEAKS.json has no FP32 vector "
                                "figure); nominal 148 SM x 128 lanes x 2 x clock",

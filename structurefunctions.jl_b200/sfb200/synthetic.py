@@ -151,11 +151,22 @@ def config(name, n=None):
     raise KeyError(name)
 
 
-# Algorithmic FP32/FP64 operations per pair of the FP32 kernel's formulation (+, -, *, sqrt/rsqrt,
-# rcp = 1 each, FMA = 2; binning compares and rechecks not counted; one add per accumulated sum).
-#   c0 (2D L2):  dx 2, r^2 3 (mul + fma), du 2, p 3, rsqrt 1, L 1, L^2 1, acc 1            = 14
-#   c1 (3D L2,T2,L3,T3): dx 3, h^2 3, r^2 2, du 3, p 5, |du|^2 5, rsqrt 1, L 1, L2 1, T2 1,
-#        L3 2, t 3, rsqrt(h^2) 1, T 1, T3 2, acc 4                                       = 38
-#   c2 (sphere L2): d 3, |d|^2 5, s^2 3, rsqrt 1, dU 3, d.dU 5, scale 1, L^2 1, acc 1       = 23
-#   c3 (2D joint du_L): dx 2, r^2 3, du 2, p 3, rsqrt 1, L 1, t 2, centre 1, acc 1         = 16
-FLOPS = {"c0": 14, "c1": 38, "c2": 23, "c3": 16}
+# Algorithmic flops per pair: the reference's FP64 formula as restated by the oracle, counting +, -,
+# x, / and sqrt as 1, FMA as 2, one add per accumulated sum; binning compares and recheck work are
+# not counted. These are the roofline numerators.
+#   c0 (2D L2):  dx 2, r^2 3, du 2, p 3, p^2/r^2 2, acc 1                                   = 13
+#   c1 (3D L2,T2,L3,T3): dx 3, r^2 5, du 3, p 5, |du|^2 5, L2 2, T2 1, sqrt 1, r_hat 3,
+#        du.r_hat 5, L3 2, n_hat 6, du.n_hat 5, T3 2, acc 4                                 = 52
+#   c2 (sphere L2, per-point basis precomputed): geodesic frame, tangents and increments 107,
+#        plus 1 atan2 and 2 square roots counted as 1 each                                  = 110
+#   c3 (2D joint du_L): dx 2, r^2 3, sqrt 1, r_hat 2, du 2, dot 3, L 1, acc 1                = 15
+FLOPS = {"c0": 13, "c1": 52, "c2": 110, "c3": 15}
+
+# Operations per pair of the mixed kernel's own formulation (FP64 + FP32, same counting), for
+# reference next to FLOPS:
+#   c0: dx 2, r^2 3, du 2, p 3, rsqrt 1, L 1, L^2 1, acc 1                                  = 14
+#   c1: dx 3, r^2 5, du 3, p 5, cz 3, |du|^2 5, c2 3, rsqrt 2, L 1, T 1, T2 2, L2 1, L3 1,
+#       T3 2, acc 4                                                                        = 41
+#   c2: d 3, s 3, |d|^2 5, |s|^2 5, dU 3, d.dU 5, scale 3, rsqrt 1, L 1, L^2 1, acc 1        = 31
+#   c3: dx 2, r^2 3, du 2, p 3, rsqrt 1, L 1, t 2, centre 1, acc 1                           = 16
+KERNEL_FLOPS = {"c0": 14, "c1": 41, "c2": 31, "c3": 16}
