@@ -201,9 +201,10 @@ SFB200_API int sfb200_plan_set_launch(sfb200_plan* plan, int tile, int privatiza
 
 /* Plan options for sfb200_plan_set_option. */
 typedef enum {
-    /* Point storage order on the device: -1 automatic (Morton order from 16384 points), 0 the
-     * caller's order, 1 Morton (Z-curve) order. Results are the same up to the rounding of the
-     * sums (counts are identical); the joint sphere path always keeps the caller's order. */
+    /* Point storage order on the device: -1 automatic (from 16384 points: Morton order for 1D
+     * histograms, scattered for the flat joint histogram), 0 the caller's order, 1 Morton (Z-curve)
+     * order, 2 scattered (slot i holds point (i m) mod N). Results are the same up to the rounding
+     * of the sums (counts are identical); the joint sphere path always keeps the caller's order. */
     SFB200_OPT_POINT_ORDER = 1,
     /* Columns of the run-length histogram table (privatization 3): 0 automatic, else 1, 2, 4, 8,
      * 16 or 32. */

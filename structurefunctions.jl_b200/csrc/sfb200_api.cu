@@ -82,6 +82,8 @@ struct sfb200_plan {
     bool stats_pending = false;
     int tile_ovr = 0, priv_ovr = -1, bps_ovr = 0;
     double vq = 1.0, vq_inv = 1.0;  // joint mixed: fixed-point scale of the value offsets
+    double vqc = 1.0, vqc_inv = 1.0;  // mixed joint: coarse scale of the packed cells
+    int vfine_lo = 1, nfine = 0;      // mixed joint: value bins with exact offsets
     int order_ovr = -1;   // -1 auto, 0 caller order, 1 Morton order
     int cols_ovr = 0;     // run-length histogram columns (0 auto)
 };
@@ -548,6 +550,31 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         if (hw > 0.0 && std::isfinite(hw)) std::frexp(hw, &ex);  // hw < 2^ex
         p->vq = std::ldexp(1.0, 30 - ex);
         p->vq_inv = std::ldexp(1.0, ex - 30);
+        p->vqc = std::ldexp(1.0, 22 - ex);
+        p->vqc_inv = std::ldexp(1.0, ex - 22);
+        // value bins whose values come closer to zero than the half width keep exact offsets
+        p->vfine_lo = 1;
+        p->nfine = 0;
+        int lo = 0, hi = -1;
+        for (int k = 1; k <= p->nv; ++k) {
+            double a0, a1;
+            if (d.value.kind == SFB200_BINS_LINEAR) {
+                a0 = std::fma((double)(k - 1), d.value.step, d.value.first);
+                a1 = std::fma((double)k, d.value.step, d.value.first);
+            } else {
+                a0 = p->vedges[k - 1];
+                a1 = p->vedges[k];
+            }
+            const double mn = (a0 < 0.0 && a1 > 0.0) ? 0.0 : std::min(std::fabs(a0), std::fabs(a1));
+            if (mn < 2.0 * hw) {
+                if (hi < 0) lo = k;
+                hi = k;
+            }
+        }
+        if (hi >= lo && hi > 0) {
+            p->vfine_lo = lo;
+            p->nfine = hi - lo + 1;
+        }
     }
 
     // device allocations
@@ -653,7 +680,7 @@ extern "C" int sfb200_plan_set_option(sfb200_plan* p, int option, int64_t value)
     sfb200_ctx* ctx = p->ctx;
     switch (option) {
     case SFB200_OPT_POINT_ORDER:
-        if (value < -1 || value > 1) return set_err(ctx, SFB200_ERR_INVALID_ARG, "point order must be -1, 0 or 1");
+        if (value < -1 || value > 2) return set_err(ctx, SFB200_ERR_INVALID_ARG, "point order must be -1, 0, 1 or 2");
         p->order_ovr = (int)value;
         return SFB200_OK;
     case SFB200_OPT_HIST_COLUMNS:
@@ -714,14 +741,40 @@ static void launch_pack(sfb200_plan* p, const void* x, const void* u, int n, con
 // Points below this count keep the caller's order: the sort costs more than the runs it lengthens.
 static const long long kOrderMinPoints = 16384;
 
-// Whether a run of n points stores them in Morton order. The joint sphere path keeps the caller's
-// order: its FP64 value binning uses the reference's pair frame, whose rounding is not symmetric in
-// the two points, so the pair orientation (i < j in caller order) must be kept.
-static bool use_spatial_order(const sfb200_plan* p, long long n)
+// Storage order of a run of n points: 0 the caller's, 1 Morton, 2 scattered. The joint sphere path
+// keeps the caller's order: its FP64 value binning uses the reference's pair frame, whose rounding
+// is not symmetric in the two points, so the pair orientation (i < j in caller order) must be kept.
+// The flat joint path scatters by default (its cells are hit by value, and neighbouring lanes with
+// neighbouring points would collide on cells); 1D paths use Morton order from kOrderMinPoints.
+static int point_order(const sfb200_plan* p, long long n)
 {
-    if (p->joint && p->sphere) return false;
-    if (p->order_ovr >= 0) return p->order_ovr == 1;
-    return n >= kOrderMinPoints;
+    if (p->joint && p->sphere) return 0;
+    if (p->order_ovr >= 0) return p->order_ovr;
+    if (p->joint) return n >= kOrderMinPoints ? 2 : 0;
+    return n >= kOrderMinPoints ? 1 : 0;
+}
+
+static unsigned long long gcd_u64(unsigned long long a, unsigned long long b)
+{
+    while (b) {
+        const unsigned long long t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+// Scattered permutation: slot i -> (i * mult) mod n with mult coprime to n.
+static int launch_scatter(sfb200_plan* p, int n, cudaStream_t s, const int** perm)
+{
+    sfb200_ctx* ctx = p->ctx;
+    unsigned long long mult = 2654435761ull % (unsigned long long)n;
+    if (mult < 2) mult = 2;
+    while (gcd_u64(mult, (unsigned long long)n) != 1ull) ++mult;
+    k_scatter_perm<<<(n + 255) / 256, 256, 0, s>>>(n, mult, p->d_perm + p->cap);
+    CK(cudaGetLastError());
+    *perm = p->d_perm + p->cap;
+    return SFB200_OK;
 }
 
 // Morton keys of the caller's points, radix-sorted with their indices; returns the permutation
@@ -765,7 +818,8 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
     const int NW = T / 32, NBP = p->nb + 2, NV = p->nops_pad;
     if (p->mx) {
         const int rec = p->sphere ? 10 : 2 * p->D;  // doubles per j record
-        if (p->joint) return (size_t)lut_bytes + (size_t)rec * T * 8 + (size_t)p->nb * p->nv * 12;
+        if (p->joint)
+            return (size_t)lut_bytes + (size_t)rec * T * 8 + ((size_t)p->nb * p->nv + (size_t)p->nb * p->nfine) * 8;
         return (size_t)lut_bytes + (size_t)rec * T * 8 + hist_bytes(true, NV, priv, NW, NBP, lc);
     }
     if (p->joint) {
@@ -837,10 +891,15 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         }
         const bool x64 = xs == 8, u64 = us == 8;
         const int* perm = nullptr;
-        if (use_spatial_order(p, n)) {
+        const int order = point_order(p, n);
+        if (order == 1) {
             rc = x64 ? launch_order<double>(p, xin, (int)n, s, &perm) : launch_order<float>(p, xin, (int)n, s, &perm);
             if (rc) return rc;
             launches += 2;  // box + keys (the radix sort's own launches are not counted)
+        } else if (order == 2) {
+            rc = launch_scatter(p, (int)n, s, &perm);
+            if (rc) return rc;
+            launches += 1;
         }
         if (x64 && u64) launch_pack<double, double>(p, xin, uin, (int)n, perm, s);
         else if (x64) launch_pack<double, float>(p, xin, uin, (int)n, perm, s);
@@ -902,8 +961,9 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
             }
             kc = p->mx ? pick_joint_mx(p->sphere, p->D, p->opl)
                        : pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->df, p->opl);
-            // block cells hold at most 2^31 pairs between flushes (T^2 pairs per tile pair)
-            flush_every = (int)std::max<long long>(1, (1ll << 31) / ((long long)T * T));
+            // block cells hold at most 2^31 pairs between flushes (T^2 pairs per tile pair); the mixed
+            // kernel's packed cells fewer than 2^20
+            flush_every = (int)std::max<long long>(1, (p->mx ? (1ll << 20) - 1 : (1ll << 31)) / ((long long)T * T));
         } else {
             const int want = p->priv_ovr >= 0 ? p->priv_ovr : default_privatization(p);
             if (p->mx)
@@ -999,6 +1059,10 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         if (p->mx) a.vrel = (float)((5.0 * p->vorder + 3.0) * 1.25 * 0x1p-24);
         a.vq = p->vq;
         a.vq_inv = p->vq_inv;
+        a.vqc = p->vqc;
+        a.vqc_inv = p->vqc_inv;
+        a.vfine_lo = p->vfine_lo;
+        a.nfine = p->nfine;
         a.gen = p->gen;
         a.g_sums = p->d_sums;
         a.g_counts = p->d_counts;

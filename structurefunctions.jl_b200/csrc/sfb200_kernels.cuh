@@ -60,6 +60,10 @@ struct PairArgs {
     float vrel;        // relative half-width: window += (|t| + |first/step|) * vrel
     double vq;         // fixed-point scale of the value offsets (power of two), and its inverse
     double vq_inv;
+    double vqc;        // mixed joint: coarse scale of the packed cells (power of two), and its inverse
+    double vqc_inv;
+    int vfine_lo;      // mixed joint: value bins [vfine_lo, vfine_lo + nfine) keep exact offsets
+    int nfine;
     int flush_every;   // privatized histograms: fold copies into FP64 every this many tile pairs
     int hist_cols;     // run-length histogram: table columns (power of two <= 32)
     GenOps gen;

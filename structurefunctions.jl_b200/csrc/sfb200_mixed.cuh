@@ -456,8 +456,39 @@ __global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
 // the value-bin index t = (v - first) / step is trusted when it lies more than
 // (|t| + |first / step|) * vrel from an integer; closer pairs, sphere pairs in the chord ambiguity
 // band and every pair of a vector value axis are recomputed in FP64 with the reference formula.
-// Cells accumulate counts and fixed-point offsets from the value-bin centres (sfb200_joint.cuh).
+//
+// Cells are one 64-bit word each, updated with a single shared atomic per pair: the count in the
+// top 20 bits and, below, the sum of the pair offsets from the value-bin centre in fixed point
+// (quantum 2^-21 of the largest half bin width or finer; the packed word decodes exactly while the
+// cell holds fewer than 2^20 pairs and the offset sum stays below 2^43 in magnitude, so blocks flush
+// at least every 2^20 - 1 pairs). That quantum is far below the 1e-6 tolerance for every value bin
+// whose values stay at least a half width away from zero; the bins closer to zero (where a value
+// can be tiny next to the quantum) keep their offsets in a separate 64-bit word at 2^-30.
 // ================================================================================================
+__device__ __forceinline__ void joint_flush_packed(const PairArgs& a, unsigned long long* hcell,
+                                                   unsigned long long* hfine, int ncell)
+{
+    const int nd = a.nb;
+    for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
+        const unsigned long long w = hcell[k];
+        if (!w) continue;
+        const unsigned long long cnt = (w + (1ull << 43)) >> 44;
+        const long long off = (long long)(w - (cnt << 44));
+        const int vb = k / nd + 1;
+        double s = (double)cnt * value_center(a, vb) + (double)off * a.vqc_inv;
+        const int f = vb - a.vfine_lo;
+        if ((unsigned)f < (unsigned)a.nfine) {
+            unsigned long long* fw = hfine + (k - (vb - 1) * nd) + nd * f;
+            s += (double)(long long)*fw * a.vq_inv;
+            *fw = 0ull;
+        }
+        atomicAdd(&a.g_sums[k], s);
+        atomicAdd(&a.g_counts[k], cnt);
+        hcell[k] = 0ull;
+    }
+    __syncthreads();
+}
+
 template <bool SPHERE, int D, class OPS>
 __global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
 {
@@ -469,14 +500,14 @@ __global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
     const int nd = a.nb, nv = a.nv;
     const int ncell = nd * nv;
     LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
-    double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);                                // T * 2NP
-    unsigned long long* hres = reinterpret_cast<unsigned long long*>(srec + (size_t)2 * NP * T);  // ncell
-    unsigned* hc = reinterpret_cast<unsigned*>(hres + ncell);                                     // ncell
+    double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);                                 // T * 2NP
+    unsigned long long* hcell = reinterpret_cast<unsigned long long*>(srec + (size_t)2 * NP * T);  // ncell
+    unsigned long long* hfine = hcell + ncell;                                                     // nd * nfine
     __shared__ unsigned long long s_recheck;
 
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
-    for (int k = threadIdx.x; k < ncell; k += T) { hres[k] = 0ull; hc[k] = 0u; }
+    for (int k = threadIdx.x; k < ncell + nd * a.nfine; k += T) hcell[k] = 0ull;
     if (threadIdx.x == 0) s_recheck = 0ull;
     unsigned my_recheck = 0;
     const int ku = pow2_exponent_above(a.g_stats[2]);
@@ -499,7 +530,7 @@ __global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
     for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
         if (iter && iter % a.flush_every == 0) {
             __syncthreads();
-            joint_flush_mixed(a, hres, hc, ncell);
+            joint_flush_packed(a, hcell, hfine, ncell);
         }
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
@@ -595,14 +626,19 @@ __global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
             if (ok && db >= 1 && db <= nd && vb >= 1 && vb <= nv) {
                 const int cell = (db - 1) + nd * (vb - 1);
                 const double off = (slow ? v64 : (double)val * unscale[0]) - value_center(a, vb);
-                atomicAdd(&hres[cell], (unsigned long long)__double2ll_rn(off * a.vq));
-                atomicAdd(&hc[cell], 1u);
+                const int f = vb - a.vfine_lo;
+                if ((unsigned)f < (unsigned)a.nfine) {
+                    atomicAdd(&hcell[cell], 1ull << 44);
+                    atomicAdd(&hfine[(db - 1) + nd * f], (unsigned long long)__double2ll_rn(off * a.vq));
+                } else {
+                    atomicAdd(&hcell[cell], (1ull << 44) + (unsigned long long)__double2ll_rn(off * a.vqc));
+                }
             }
         }
     }
     if (my_recheck) atomicAdd(&s_recheck, (unsigned long long)my_recheck);
     __syncthreads();
-    joint_flush_mixed(a, hres, hc, ncell);
+    joint_flush_packed(a, hcell, hfine, ncell);
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 

@@ -148,6 +148,16 @@ __global__ void k_morton_keys(const TX* __restrict__ x, int n, int W, int sphere
     idx[i] = i;
 }
 
+// Scattered order: slot i holds point (i * mult) mod n, mult coprime to n (a bijection). Used by the
+// joint histograms, whose threads should hit unrelated cells: with neighbouring points in
+// neighbouring lanes (gridded input, or the Morton order) a warp's lanes often update the same cell
+// at once, and shared-memory atomics to one address serialise.
+__global__ void k_scatter_perm(int n, unsigned long long mult, int* perm)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) perm[i] = (int)(((unsigned long long)i * mult) % (unsigned long long)n);
+}
+
 // FP32 image of an FP64 value as (hi, lo): hi = fl32(v), lo = fl32(v - hi); hi + lo equals v to
 // about 2^-48 relative.
 __device__ __forceinline__ void split_df(double v, float& hi, float& lo)

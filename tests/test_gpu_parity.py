@@ -174,7 +174,7 @@ def test_privatization_modes(precision, tol, priv, tile):
 
 
 @pytest.mark.parametrize("precision,tol", PRECISIONS)
-@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("order", [0, 1, 2])
 @pytest.mark.parametrize("cols", [1, 8, 32])
 def test_point_order_and_table_columns(precision, tol, order, cols):
     """Morton-ordered storage and every run-length table width give the oracle's histogram."""
@@ -197,7 +197,7 @@ def test_point_order_and_table_columns(precision, tol, order, cols):
 def test_joint_point_order(precision, tol):
     """The joint flat histogram is the same in caller and Morton order."""
     w = synthetic.config("c3", n=2500)
-    for order in (0, 1):
+    for order in (0, 1, 2):
         gs, gc, st = run_gpu(w.ops, w.x, w.u, w.distance_bins.edges, value_bins=w.value_bins,
                              precision=precision, options={_abi.OPT_POINT_ORDER: order})
         rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges, value_bins=w.value_bins)
