@@ -42,7 +42,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3"])
+    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4"])
+    ap.add_argument("--requests", type=int, default=2000, help="c4: number of requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="c4: Poisson arrival rate per second")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample length")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
@@ -436,6 +438,185 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------------------------------ serving
+
+def _percentiles(v, qs=(50, 99)):
+    v = np.asarray(v, dtype=np.float64)
+    return {f"p{q}": float(np.percentile(v, q)) for q in qs} if v.size else {f"p{q}": None for q in qs}
+
+
+def run_serving(args):
+    """c4: a stream of requests with Poisson arrivals, served by the continuous-batching loop, then
+    by one launch per request (FIFO, same arrival times); latencies from arrival to result."""
+    import threading
+
+    import torch
+
+    import sfb200 as SF  # noqa: F401
+    from sfb200 import _lib, synthetic
+    from sfb200.api import plan_description
+    from sfb200.serving import GpuExecutor, Request, Server
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and rank != 0:
+        return  # the serving run is a single-GPU measurement (requests are not sharded here)
+    torch.cuda.set_device(local)
+    workers = max(1, min(16, (os.cpu_count() or 2) - 1))
+    t_gen = time.perf_counter()
+    reqs = synthetic.serving_requests(count=args.requests, rate=args.rate, workers=workers)
+    warm = synthetic.serving_requests(count=max(3, args.warmup) * 6, rate=1e9, seed=99, n_max=5000)
+    t_gen = time.perf_counter() - t_gen
+
+    def subrequests(q):
+        out = [Request(q["ops"], q["x"], q["u"], q["edges"], None, q["metric"])]
+        if q["value_bins"] is not None:
+            out.append(Request((SF.ProjectedStructureFunctionType(1, 0),), q["x"], q["u"], q["edges"],
+                               q["value_bins"], q["metric"]))
+        return out
+
+    def pairs_of(q):
+        return q["n"] * (q["n"] - 1) // 2 * (2 if q["value_bins"] is not None else 1)
+
+    total_pairs = sum(pairs_of(q) for q in reqs)
+
+    # ---- batched
+    ex = GpuExecutor(local)
+    clocks = ClockSampler(local)
+    srv = Server(ex, max_slots=48, round_pairs=1.5e9).start()
+    for q in warm:
+        for r in subrequests(q):
+            srv.submit(r).wait(120)
+    rounds0 = srv.rounds
+    ex.launches = 0
+    tickets = [None] * len(reqs)
+    clocks.start()
+    t0 = time.perf_counter() + 0.05
+
+    def feeder():
+        for k, q in enumerate(reqs):
+            d = t0 + q["t"] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[k] = (time.perf_counter(), [srv.submit(r) for r in subrequests(q)])
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    th.join()
+    lat_b, done_b = [], []
+    for k, (ta, ts) in enumerate(tickets):
+        for t in ts:
+            t.wait(600)
+        done = max(t.t_done for t in ts)
+        lat_b.append(done - ta)
+        done_b.append(done)
+    clk = clocks.stop()
+    srv.stop()
+    rounds = srv.rounds - rounds0
+    launches = ex.launches
+    span_b = max(done_b) - t0
+    ex.close()
+
+    # ---- one launch per request (FIFO on the same arrivals), each request's service time alone
+    ctx = _lib.Context(local)
+    plans = {}
+
+    def plan_for(r):
+        key = (tuple(repr(o) for o in r.ops), r.u.shape[0], repr(r.metric), r.x.dtype.str, r.u.dtype.str,
+               np.asarray(r.distance_bins).tobytes(), repr(r.value_bins))
+        if key not in plans:
+            desc, keep = plan_description(r.ops, r.u.shape[0], r.distance_bins, r.value_bins, r.metric, "mixed",
+                                          r.x.dtype, r.u.dtype)
+            plans[key] = (_lib.Plan(ctx, desc, keep), keep)
+        return plans[key][0]
+
+    def run_alone(r):
+        p = plan_for(r)
+        s = np.zeros(p.n_sums)
+        c = np.zeros(p.n_counts, dtype=np.uint64)
+        xa, ua = np.asfortranarray(r.x), np.asfortranarray(r.u)
+        p.run(xa.ctypes.data, ua.ctypes.data, r.n, 0, s.ctypes.data, c.ctypes.data)
+
+    for q in warm:
+        for r in subrequests(q):
+            run_alone(r)
+    subs = [subrequests(q) for q in reqs]
+    t0 = time.perf_counter() + 0.05
+    lat_1, svc_1, done_1 = [], [], []
+    for q, rs in zip(reqs, subs):
+        ta = t0 + q["t"]
+        d = ta - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        ts = time.perf_counter()
+        for r in rs:
+            run_alone(r)
+        te = time.perf_counter()
+        lat_1.append(te - ta)
+        svc_1.append(te - ts)
+        done_1.append(te)
+    span_1 = max(done_1) - t0
+    for p, _ in plans.values():
+        p.close()
+    ctx.close()
+
+    lat_b = np.array(lat_b)
+    lat_1 = np.array(lat_1)
+    svc = np.array(svc_1)
+    slow_b = lat_b / svc
+    slow_1 = lat_1 / svc
+    sizes = np.array([pairs_of(q) for q in reqs], dtype=np.float64)
+    deciles = []
+    edges = np.quantile(sizes, np.linspace(0, 1, 11))
+    for k in range(10):
+        m = (sizes >= edges[k]) & ((sizes <= edges[k + 1]) if k == 9 else (sizes < edges[k + 1]))
+        deciles.append({"pairs": [float(edges[k]), float(edges[k + 1])], "n": int(m.sum()),
+                        "latency_ms": {kk: v * 1e3 for kk, v in _percentiles(lat_b[m]).items()},
+                        "slowdown": _percentiles(slow_b[m])})
+    value = total_pairs / span_b
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": 1,
+        "steps": len(reqs),
+        "warmup": len(warm),
+        "ms_per_step": float(np.mean(lat_b) * 1e3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64+f32",
+        "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": f"c4 serving: {len(reqs)} requests, Poisson {args.rate}/s, N log-uniform "
+                               "[1e3, 1e5], 2D/3D planar or spherical, 32-64 log bins, order 2 or 3, half with "
+                               "the 256-value-bin joint histogram",
+                   "total_pairs": int(total_pairs), "step": "one request (1D and, if asked, joint histogram)",
+                   "l2": "inputs of a request are copied from host memory at admission (no flush needed)",
+                   "max_slots": 48, "round_pairs": 1.5e9, "generation_s": t_gen},
+        "latency": {"raw_ms": {k: v * 1e3 for k, v in _percentiles(lat_b).items()},
+                    "slowdown": _percentiles(slow_b),
+                    "slowdown_p99_over_p50": float(np.percentile(slow_b, 99) / np.percentile(slow_b, 50)),
+                    "raw_p99_over_p50": float(np.percentile(lat_b, 99) / np.percentile(lat_b, 50)),
+                    "by_size_decile": deciles,
+                    "slowdown_definition": "latency / the request's service time when run alone (one launch "
+                                           "per histogram, measured in the baseline run)"},
+        "rounds": rounds,
+        "one_launch_per_request": {"value": total_pairs / span_1, "unit": UNIT,
+                                   "latency_raw_ms": {k: v * 1e3 for k, v in _percentiles(lat_1).items()},
+                                   "slowdown": _percentiles(slow_1)},
+        "batched_over_one_launch": (total_pairs / span_b) / (total_pairs / span_1),
+        "e2e": {"value": value, "unit": UNIT,
+                "h2d_bytes_per_step": int(np.mean([q["x"].nbytes + q["u"].nbytes for q in reqs])),
+                "d2h_bytes_per_step": int(np.mean([8 * 2 * (len(q["edges"]) - 1) *
+                                                   (1 + (256 if q["value_bins"] is not None else 0))
+                                                   for q in reqs]))},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.warmup < 3:
@@ -444,6 +625,8 @@ def main():
         run_profile_case(args)
     elif args.impl == "reference":
         run_reference(args)
+    elif args.config == "c4":
+        run_serving(args)
     else:
         run_ours(args)
 

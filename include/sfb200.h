@@ -214,6 +214,49 @@ typedef enum {
 /* Set a plan option (autotuning; no counterpart in the reference). */
 SFB200_API int sfb200_plan_set_option(sfb200_plan* plan, int option, int64_t value);
 
+/* ------------------------------------------------------------------------------------ serving
+ * Batched execution for many independent point sets (time slices, fields, requests) of uneven size.
+ * No counterpart in the reference, which runs one call at a time; it serves the request loop of the
+ * host glue (admission by free device memory, continuous batching).
+ *
+ * A slice is one point set made resident on the device with its own histogram: created from a plan
+ * (precision SFB200_PREC_MIXED) and the inputs, it holds the packed points and a zeroed histogram.
+ * Its work is `tile_pairs` independent units. sfb200_batch_run queues one round: for every listed
+ * slice, the tile pairs [begin, end) are added into its histogram. Slices of different plans (2D/3D,
+ * planar/spherical, 1D or joint) may share a round: the library groups them by kernel and runs each
+ * group as one persistent launch whose blocks pull (slice, tile-pair range) items from a device
+ * counter; the round is captured as a CUDA graph and replayed with updated parameters. Every tile
+ * pair of a slice must be covered exactly once over the rounds; the result then equals sfb200_run's
+ * (counts identical, sums up to summation order). Rounds on one context must not overlap: a round's
+ * item list lives in a host buffer that the next call rewrites, so wait for the stream (or an event
+ * recorded after the round) before the next sfb200_batch_run. */
+typedef struct sfb200_slice sfb200_slice;
+
+typedef struct {
+    int64_t n_points;
+    int64_t pairs;          /* n (n - 1) / 2 */
+    int64_t tile_pairs;     /* work units of the batched kernels */
+    int64_t device_bytes;   /* device memory held by the slice */
+} sfb200_slice_info;
+
+/* Make one point set resident (copy if host input, order, pack, zero the histogram), queued on
+ * `stream` (NULL: the context stream). The plan must outlive the slice. */
+SFB200_API int sfb200_slice_create(sfb200_plan* plan, const void* x, const void* u, int64_t n, uint32_t flags,
+                                   void* stream, sfb200_slice** out);
+SFB200_API int sfb200_slice_get_info(const sfb200_slice* slice, sfb200_slice_info* out);
+/* One round: tile pairs [tp_begin[k], tp_end[k]) of slices[k], k < n (each slice at most once). */
+SFB200_API int sfb200_batch_run(sfb200_ctx* ctx, int32_t n, sfb200_slice* const* slices, const int64_t* tp_begin,
+                                const int64_t* tp_end, void* stream);
+/* Copy a slice's histogram out (host buffers: synchronous; SFB200_RUN_DEVICE_OUTPUT: queued on the
+ * stream; SFB200_RUN_ACCUMULATE adds into the caller's buffers). */
+SFB200_API int sfb200_slice_read(sfb200_slice* slice, double* sums, uint64_t* counts, uint32_t flags, void* stream);
+SFB200_API int sfb200_slice_destroy(sfb200_slice* slice);
+/* Wait for the last round of the context (blocking) / ask whether it has finished (*done = 0 or 1). */
+SFB200_API int sfb200_batch_wait(sfb200_ctx* ctx);
+SFB200_API int sfb200_batch_query(sfb200_ctx* ctx, int32_t* done);
+/* Free and total device memory of the context's device (cudaMemGetInfo), for admission control. */
+SFB200_API int sfb200_device_memory(sfb200_ctx* ctx, int64_t* free_bytes, int64_t* total_bytes);
+
 #ifdef __cplusplus
 }
 #endif

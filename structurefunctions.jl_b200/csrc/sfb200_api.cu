@@ -27,6 +27,45 @@ struct sfb200_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
+    // batched rounds: work items (pinned host staging + device copy), launch counters, the graph
+    void* h_items = nullptr;
+    void* d_items = nullptr;
+    size_t items_cap = 0;       // WorkItem capacity of both buffers
+    unsigned* d_counters = nullptr;
+    int counters_cap = 0;
+    cudaGraphExec_t batch_exec = nullptr;
+    bool batch_graph = true;    // capture rounds as a graph (cleared if capture is refused)
+    cudaEvent_t round_done = nullptr;  // recorded after each round (the item buffer is free again)
+    bool round_pending = false;
+    // the kernels of one round run concurrently on these streams (fork / join through events)
+    static constexpr int kLanes = 8;
+    cudaStream_t lane[kLanes] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kLanes] = {};
+    cudaStream_t prep_stream = nullptr;  // slice preparation, overlapping the running round
+};
+
+// Device buffers of one run over n <= cap points: raw inputs, the packed SoA layout, the point
+// order, and the accumulated histogram. A plan owns one (for sfb200_run); every slice its own.
+struct Workspace {
+    long long cap = 0;
+    void* d_rawx = nullptr;
+    void* d_rawu = nullptr;
+    double* d_X64 = nullptr;
+    double* d_U64 = nullptr;
+    float* d_XF = nullptr;
+    float* d_UF = nullptr;
+    double* d_XM = nullptr;       // mixed sphere: FP64 p(3), U(3), W(3)[, up] per point (SoA)
+    // spatial order: Morton keys and the permutation (double-buffered for the radix sort)
+    unsigned* d_keys = nullptr;   // 2 * cap
+    int* d_perm = nullptr;        // 2 * cap
+    unsigned* d_box = nullptr;    // 6
+    void* d_sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    double* d_sums = nullptr;
+    unsigned long long* d_counts = nullptr;
+    unsigned long long* d_aux = nullptr;  // [0] rechecked pairs, [1] |x| bound, [2] |u| bound
+    size_t bytes = 0;                     // device bytes held
 };
 
 struct sfb200_plan {
@@ -57,25 +96,8 @@ struct sfb200_plan {
     WindowParams wp{};
     double* d_rowlo = nullptr;
     float* d_vwin = nullptr;
-    // workspace
-    long long cap = 0;
-    void* d_rawx = nullptr;
-    void* d_rawu = nullptr;
-    double* d_X64 = nullptr;
-    double* d_U64 = nullptr;
-    float* d_XF = nullptr;
-    float* d_UF = nullptr;
-    double* d_XM = nullptr;       // mixed sphere: FP64 p(3), U(3), W(3)[, up] per point (SoA)
-    // spatial order: Morton keys and the permutation (double-buffered for the radix sort)
-    unsigned* d_keys = nullptr;   // 2 * cap
-    int* d_perm = nullptr;        // 2 * cap
-    unsigned* d_box = nullptr;    // 6
-    void* d_sort_tmp = nullptr;
-    size_t sort_tmp_bytes = 0;
+    Workspace ws;  // the workspace of sfb200_run
     long long n_sums = 0, n_counts = 0;
-    double* d_sums = nullptr;
-    unsigned long long* d_counts = nullptr;
-    unsigned long long* d_aux = nullptr;  // [0] rechecked pairs, [1] |x| bound, [2] |u| bound
     std::vector<double> h_sums;
     std::vector<unsigned long long> h_counts;
     sfb200_stats stats{};
@@ -152,6 +174,18 @@ extern "C" int sfb200_ctx_destroy(sfb200_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->prep_stream) cudaStreamSynchronize(ctx->prep_stream);
+    if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
+    if (ctx->round_done) cudaEventDestroy(ctx->round_done);
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
+    for (int k = 0; k < sfb200_ctx::kLanes; ++k) {
+        if (ctx->join[k]) cudaEventDestroy(ctx->join[k]);
+        if (ctx->lane[k]) cudaStreamDestroy(ctx->lane[k]);
+    }
+    if (ctx->prep_stream) cudaStreamDestroy(ctx->prep_stream);
+    if (ctx->h_items) cudaFreeHost(ctx->h_items);
+    cudaFree(ctx->d_items);
+    cudaFree(ctx->d_counters);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SFB200_OK;
@@ -360,30 +394,35 @@ static LinearParams linear_of(const sfb200_bins& b)
     return p;
 }
 
-static void free_workspace(sfb200_plan* p)
+// Frees the input / layout buffers of a workspace (its histogram buffers with `outputs`).
+static void free_workspace(Workspace& w, bool outputs)
 {
-    cudaFree(p->d_rawx); cudaFree(p->d_rawu);
-    cudaFree(p->d_X64); cudaFree(p->d_U64); cudaFree(p->d_XF); cudaFree(p->d_UF); cudaFree(p->d_XM);
-    p->d_XF = p->d_UF = nullptr;
-    p->d_XM = nullptr;
-    cudaFree(p->d_keys); cudaFree(p->d_perm); cudaFree(p->d_box); cudaFree(p->d_sort_tmp);
-    p->d_rawx = p->d_rawu = nullptr;
-    p->d_X64 = p->d_U64 = nullptr;
-    p->d_keys = nullptr;
-    p->d_perm = nullptr;
-    p->d_box = nullptr;
-    p->d_sort_tmp = nullptr;
-    p->sort_tmp_bytes = 0;
-    p->d_XF = p->d_UF = nullptr;
-    p->cap = 0;
+    cudaFree(w.d_rawx); cudaFree(w.d_rawu);
+    cudaFree(w.d_X64); cudaFree(w.d_U64); cudaFree(w.d_XF); cudaFree(w.d_UF); cudaFree(w.d_XM);
+    cudaFree(w.d_keys); cudaFree(w.d_perm); cudaFree(w.d_box); cudaFree(w.d_sort_tmp);
+    w.d_rawx = w.d_rawu = nullptr;
+    w.d_X64 = w.d_U64 = nullptr;
+    w.d_XF = w.d_UF = nullptr;
+    w.d_XM = nullptr;
+    w.d_keys = nullptr;
+    w.d_perm = nullptr;
+    w.d_box = nullptr;
+    w.d_sort_tmp = nullptr;
+    w.sort_tmp_bytes = 0;
+    w.cap = 0;
+    if (outputs) {
+        cudaFree(w.d_sums); cudaFree(w.d_counts); cudaFree(w.d_aux);
+        w.d_sums = nullptr;
+        w.d_counts = nullptr;
+        w.d_aux = nullptr;
+    }
 }
 
 static void free_plan_device(sfb200_plan* p)
 {
-    free_workspace(p);
+    free_workspace(p->ws, true);
     cudaFree(p->d_exact); cudaFree(p->d_vedges); cudaFree(p->d_lut64); cudaFree(p->d_ck);
     cudaFree(p->d_lut32); cudaFree(p->d_rowlo); cudaFree(p->d_vwin);
-    cudaFree(p->d_sums); cudaFree(p->d_counts); cudaFree(p->d_aux);
 }
 
 extern "C" int sfb200_plan_destroy(sfb200_plan* p)
@@ -607,10 +646,10 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
     }
     p->n_sums = p->joint ? (long long)p->nb * p->nv : (long long)p->nb * p->nops;
     p->n_counts = p->joint ? (long long)p->nb * p->nv : (long long)p->nb;
-    if ((e = cudaMalloc(&p->d_sums, sizeof(double) * p->n_sums)) != cudaSuccess) return cuda_fail(ctx, e, "alloc sums");
-    if ((e = cudaMalloc(&p->d_counts, sizeof(unsigned long long) * p->n_counts)) != cudaSuccess)
+    if ((e = cudaMalloc(&p->ws.d_sums, sizeof(double) * p->n_sums)) != cudaSuccess) return cuda_fail(ctx, e, "alloc sums");
+    if ((e = cudaMalloc(&p->ws.d_counts, sizeof(unsigned long long) * p->n_counts)) != cudaSuccess)
         return cuda_fail(ctx, e, "alloc counts");
-    if ((e = cudaMalloc(&p->d_aux, sizeof(unsigned long long) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc aux");
+    if ((e = cudaMalloc(&p->ws.d_aux, sizeof(unsigned long long) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc aux");
     p->h_sums.resize(p->n_sums);
     p->h_counts.resize(p->n_counts);
 
@@ -694,48 +733,66 @@ extern "C" int sfb200_plan_set_option(sfb200_plan* p, int option, int64_t value)
 
 // ------------------------------------------------------------------------------- run
 
-static int ensure_workspace(sfb200_plan* p, long long n)
+// Grows the input / layout buffers of `w` to n points (its histogram buffers are sized by the plan).
+static int ensure_workspace(sfb200_plan* p, Workspace& w, long long n)
 {
     sfb200_ctx* ctx = p->ctx;
-    if (n <= p->cap) return SFB200_OK;
-    CK(cudaStreamSynchronize(ctx->stream));
-    free_workspace(p);
+    if (n <= w.cap) return SFB200_OK;
+    if (w.cap) CK(cudaStreamSynchronize(ctx->stream));  // old buffers may still be in use
+    free_workspace(w, false);
     const long long cap = std::max<long long>(n, 1024);
     const int nx64 = p->sphere ? 8 : p->D;
     const int nxf = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 2 * p->D : p->D);
-    CK(cudaMalloc(&p->d_rawx, sizeof(double) * p->W * cap));
-    CK(cudaMalloc(&p->d_rawu, sizeof(double) * p->D * cap));
-    CK(cudaMalloc(&p->d_X64, sizeof(double) * nx64 * cap));
-    CK(cudaMalloc(&p->d_U64, sizeof(double) * p->D * cap));
+    size_t bytes = 0;
+    auto alloc = [&](void** ptr, size_t b) {
+        bytes += b;
+        return cudaMalloc(ptr, b);
+    };
+    CK(alloc(&w.d_rawx, sizeof(double) * p->W * cap));
+    CK(alloc(&w.d_rawu, sizeof(double) * p->D * cap));
+    CK(alloc((void**)&w.d_X64, sizeof(double) * nx64 * cap));
+    CK(alloc((void**)&w.d_U64, sizeof(double) * p->D * cap));
     if (p->mixed) {
-        CK(cudaMalloc(&p->d_XF, sizeof(float) * nxf * cap));
-        if (!p->sphere) CK(cudaMalloc(&p->d_UF, sizeof(float) * (p->df ? 2 : 1) * p->D * cap));
+        CK(alloc((void**)&w.d_XF, sizeof(float) * nxf * cap));
+        if (!p->sphere) CK(alloc((void**)&w.d_UF, sizeof(float) * (p->df ? 2 : 1) * p->D * cap));
     }
-    if (p->mx && p->sphere) CK(cudaMalloc(&p->d_XM, sizeof(double) * 10 * cap));
-    CK(cudaMalloc(&p->d_keys, sizeof(unsigned) * 2 * cap));
-    CK(cudaMalloc(&p->d_perm, sizeof(int) * 2 * cap));
-    CK(cudaMalloc(&p->d_box, sizeof(unsigned) * 6));
+    if (p->mx && p->sphere) CK(alloc((void**)&w.d_XM, sizeof(double) * 10 * cap));
+    CK(alloc((void**)&w.d_keys, sizeof(unsigned) * 2 * cap));
+    CK(alloc((void**)&w.d_perm, sizeof(int) * 2 * cap));
+    CK(alloc((void**)&w.d_box, sizeof(unsigned) * 6));
     size_t tmp = 0;
-    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, p->d_keys, p->d_keys + cap, p->d_perm, p->d_perm + cap,
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, w.d_keys, w.d_keys + cap, w.d_perm, w.d_perm + cap,
                                        (int)cap, 0, 32, ctx->stream));
-    CK(cudaMalloc(&p->d_sort_tmp, std::max<size_t>(tmp, 16)));
-    p->sort_tmp_bytes = tmp;
-    p->cap = cap;
+    CK(alloc(&w.d_sort_tmp, std::max<size_t>(tmp, 16)));
+    w.sort_tmp_bytes = tmp;
+    w.cap = cap;
+    w.bytes = bytes + (size_t)(p->n_sums + p->n_counts + 4) * 8;
+    return SFB200_OK;
+}
+
+// Allocates the histogram buffers of `w` for plan p.
+static int alloc_outputs(sfb200_plan* p, Workspace& w)
+{
+    sfb200_ctx* ctx = p->ctx;
+    CK(cudaMalloc(&w.d_sums, sizeof(double) * std::max<long long>(p->n_sums, 1)));
+    CK(cudaMalloc(&w.d_counts, sizeof(unsigned long long) * std::max<long long>(p->n_counts, 1)));
+    CK(cudaMalloc(&w.d_aux, sizeof(unsigned long long) * 4));
     return SFB200_OK;
 }
 
 template <typename TX, typename TU>
-static void launch_pack(sfb200_plan* p, const void* x, const void* u, int n, const int* perm, cudaStream_t s)
+static void launch_pack(sfb200_plan* p, Workspace& w, const void* x, const void* u, int n, const int* perm,
+                        cudaStream_t s)
 {
     const int tb = 256, nblk = (n + tb - 1) / tb;
     if (p->sphere)
         k_pack_sphere<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->desc.angle_unit, perm,
-                                                  p->d_X64, p->d_U64, p->mixed ? p->d_XF : nullptr,
-                                                  p->mx ? p->d_XM : nullptr, p->d_aux + 1);
+                                                  w.d_X64, w.d_U64, p->mixed ? w.d_XF : nullptr,
+                                                  p->mx ? w.d_XM : nullptr, w.d_aux + 1);
     else
-        k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->df, perm, p->d_X64,
-                                                p->d_U64, p->mixed ? p->d_XF : nullptr,
-                                                p->mixed ? p->d_UF : nullptr, p->d_aux + 1);
+        k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->df, perm, w.d_X64,
+                                                w.d_U64, p->mixed ? w.d_XF : nullptr,
+                                                p->mixed ? w.d_UF : nullptr, w.d_aux + 1);
 }
 
 // Points below this count keep the caller's order: the sort costs more than the runs it lengthens.
@@ -765,35 +822,35 @@ static unsigned long long gcd_u64(unsigned long long a, unsigned long long b)
 }
 
 // Scattered permutation: slot i -> (i * mult) mod n with mult coprime to n.
-static int launch_scatter(sfb200_plan* p, int n, cudaStream_t s, const int** perm)
+static int launch_scatter(sfb200_plan* p, Workspace& w, int n, cudaStream_t s, const int** perm)
 {
     sfb200_ctx* ctx = p->ctx;
     unsigned long long mult = 2654435761ull % (unsigned long long)n;
     if (mult < 2) mult = 2;
     while (gcd_u64(mult, (unsigned long long)n) != 1ull) ++mult;
-    k_scatter_perm<<<(n + 255) / 256, 256, 0, s>>>(n, mult, p->d_perm + p->cap);
+    k_scatter_perm<<<(n + 255) / 256, 256, 0, s>>>(n, mult, w.d_perm + w.cap);
     CK(cudaGetLastError());
-    *perm = p->d_perm + p->cap;
+    *perm = w.d_perm + w.cap;
     return SFB200_OK;
 }
 
 // Morton keys of the caller's points, radix-sorted with their indices; returns the permutation
 // (slot -> caller index) in device memory.
 template <typename TX>
-static int launch_order(sfb200_plan* p, const void* x, int n, cudaStream_t s, const int** perm)
+static int launch_order(sfb200_plan* p, Workspace& w, const void* x, int n, cudaStream_t s, const int** perm)
 {
     sfb200_ctx* ctx = p->ctx;
     const int tb = 256, nblk = (n + tb - 1) / tb;
-    CK(cudaMemsetAsync(p->d_box, 0xff, sizeof(unsigned) * 3, s));
-    CK(cudaMemsetAsync(p->d_box + 3, 0, sizeof(unsigned) * 3, s));
-    k_morton_box<TX><<<nblk, tb, 0, s>>>((const TX*)x, n, p->W, p->sphere, p->desc.angle_unit, p->d_box);
-    k_morton_keys<TX><<<nblk, tb, 0, s>>>((const TX*)x, n, p->W, p->sphere, p->desc.angle_unit, p->d_box,
-                                          p->d_keys, p->d_perm);
+    CK(cudaMemsetAsync(w.d_box, 0xff, sizeof(unsigned) * 3, s));
+    CK(cudaMemsetAsync(w.d_box + 3, 0, sizeof(unsigned) * 3, s));
+    k_morton_box<TX><<<nblk, tb, 0, s>>>((const TX*)x, n, p->W, p->sphere, p->desc.angle_unit, w.d_box);
+    k_morton_keys<TX><<<nblk, tb, 0, s>>>((const TX*)x, n, p->W, p->sphere, p->desc.angle_unit, w.d_box,
+                                          w.d_keys, w.d_perm);
     CK(cudaGetLastError());
-    size_t tmp = p->sort_tmp_bytes;
-    CK(cub::DeviceRadixSort::SortPairs(p->d_sort_tmp, tmp, p->d_keys, p->d_keys + p->cap, p->d_perm,
-                                       p->d_perm + p->cap, n, 0, 32, s));
-    *perm = p->d_perm + p->cap;
+    size_t tmp = w.sort_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(w.d_sort_tmp, tmp, w.d_keys, w.d_keys + w.cap, w.d_perm, w.d_perm + w.cap,
+                                       n, 0, 32, s));
+    *perm = w.d_perm + w.cap;
     return SFB200_OK;
 }
 
@@ -853,6 +910,246 @@ static long long tile_pairs(long long n, int T)
     return nt * (nt + 1) / 2;
 }
 
+// Copies (if on the host), orders and packs the points of one run into `w`, zeroes its histogram,
+// and builds the data-dependent tables of the FP32-bulk kernels. Everything is queued on stream s.
+static int prepare_inputs(sfb200_plan* p, Workspace& w, const void* x, const void* u, long long n, uint32_t flags,
+                          cudaStream_t s, int* launches)
+{
+    sfb200_ctx* ctx = p->ctx;
+    const bool dev_in = flags & SFB200_RUN_DEVICE_INPUT;
+    CK(cudaMemsetAsync(w.d_sums, 0, sizeof(double) * p->n_sums, s));
+    CK(cudaMemsetAsync(w.d_counts, 0, sizeof(unsigned long long) * p->n_counts, s));
+    CK(cudaMemsetAsync(w.d_aux, 0, sizeof(unsigned long long) * 4, s));
+    if (n < 2) return SFB200_OK;
+    int rc = ensure_workspace(p, w, n);
+    if (rc) return rc;
+    const size_t xs = p->desc.x_dtype == SFB200_F64 ? 8 : 4;
+    const size_t us = p->desc.u_dtype == SFB200_F64 ? 8 : 4;
+    const void* xin = x;
+    const void* uin = u;
+    if (!dev_in) {
+        CK(cudaMemcpyAsync(w.d_rawx, x, xs * p->W * n, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(w.d_rawu, u, us * p->D * n, cudaMemcpyHostToDevice, s));
+        xin = w.d_rawx;
+        uin = w.d_rawu;
+    }
+    const bool x64 = xs == 8, u64 = us == 8;
+    const int* perm = nullptr;
+    const int order = point_order(p, n);
+    if (order == 1) {
+        rc = x64 ? launch_order<double>(p, w, xin, (int)n, s, &perm) : launch_order<float>(p, w, xin, (int)n, s, &perm);
+        if (rc) return rc;
+        *launches += 2;  // box + keys (the radix sort's own launches are not counted)
+    } else if (order == 2) {
+        rc = launch_scatter(p, w, (int)n, s, &perm);
+        if (rc) return rc;
+        *launches += 1;
+    }
+    if (x64 && u64) launch_pack<double, double>(p, w, xin, uin, (int)n, perm, s);
+    else if (x64) launch_pack<double, float>(p, w, xin, uin, (int)n, perm, s);
+    else if (u64) launch_pack<float, double>(p, w, xin, uin, (int)n, perm, s);
+    else launch_pack<float, float>(p, w, xin, uin, (int)n, perm, s);
+    ++*launches;
+    CK(cudaGetLastError());
+    if (p->mixed) {
+        k_build_lut32<<<(p->lg32.ncell + 127) / 128, 128, 0, s>>>(p->d_ck, (int)p->ck.size(), p->wp, p->lg32,
+                                                                w.d_aux + 1, p->d_lut32);
+        ++*launches;
+        CK(cudaGetLastError());
+        if (p->joint) {
+            ValueWindowParams vw;
+            vw.nd = p->nb;
+            vw.D = p->D;
+            vw.order = p->vorder;
+            vw.sphere = p->sphere;
+            vw.x_f64 = x64;
+            vw.u_f64 = u64;
+            vw.df = p->df;
+            vw.l_only = p->l_only;
+            vw.inv_step = p->desc.value.kind == SFB200_BINS_LINEAR ? p->vlin.inv_step : 0.0;
+            vw.neg_f_inv = p->desc.value.kind == SFB200_BINS_LINEAR ? p->vlin.neg_f_inv : 0.0;
+            k_value_windows<<<1, 128, 0, s>>>(p->d_rowlo, vw, w.d_aux + 1, p->d_vwin);
+            ++*launches;
+            CK(cudaGetLastError());
+        }
+    }
+
+    return SFB200_OK;
+}
+
+// Tiles of the batched kernels (one per launch, shared by every slice of the launch): 256 points for
+// the 1D histograms; 512 for the joint histogram, whose large shared table leaves room for one or two
+// blocks per SM, so that each block carries more warps.
+static const int kBatchTile1D = 256;
+static const int kBatchTileJoint = 512;
+
+// Launch configuration of one run over n points: kernel, tile, block size, shared memory, grid and
+// the kernel arguments. `batch`: the batched (serving) form of the mixed kernels, with a fixed tile
+// so that slices of one variant share a launch.
+struct LaunchCfg {
+    KernelChoice kc{};
+    int T = 0, threads = 0;
+    size_t smem = 0;
+    long long ntp = 0, grid = 0;
+    PairArgs a{};
+};
+
+static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, LaunchCfg* out)
+{
+    sfb200_ctx* ctx = p->ctx;
+    const bool dlinear = p->desc.distance.kind == SFB200_BINS_LINEAR;
+    int lut_bytes = 0;
+    if (p->mixed) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
+    else if (p->mx) lut_bytes = p->lut64_bytes;  // exact table (flat) or chord table (sphere); 0 if linear
+    else if (!dlinear && !p->joint) lut_bytes = p->lut64_bytes;
+    int T;
+    bool smem_hist = true;
+    KernelChoice kc;
+    size_t smem;
+    int dev_smem_max = 0;
+    CK(cudaDeviceGetAttribute(&dev_smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    int flush_every = 0;
+    int hist_cols = 32;
+    if (p->joint) {
+        T = p->tile_ovr ? p->tile_ovr : (n >= 32768 ? 512 : (n >= 4096 ? 256 : 64));
+        if (batch) T = kBatchTileJoint;
+        smem = smem_bytes(p, T, lut_bytes, true, 0);
+        while (p->mx && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr) {
+            T /= 2;
+            smem = smem_bytes(p, T, lut_bytes, true, 0);
+        }
+        if (smem > (size_t)dev_smem_max) {
+            if (p->mixed || p->mx)
+                return set_err(ctx, SFB200_ERR_UNSUPPORTED,
+                               "joint histogram of %d x %d cells does not fit shared memory on the mixed path; use fp64",
+                               p->nb, p->nv);
+            smem_hist = false;
+            smem = smem_bytes(p, T, lut_bytes, false, 0);
+        }
+        kc = p->mx ? (batch ? pick_joint_mx_batch(p->sphere, p->D, p->opl) : pick_joint_mx(p->sphere, p->D, p->opl))
+                   : pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->df, p->opl);
+        // block cells hold at most 2^31 pairs between flushes (T^2 pairs per tile pair); the mixed
+        // kernel's packed cells fewer than 2^20
+        flush_every = (int)std::max<long long>(1, (p->mx ? (1ll << 20) - 1 : (1ll << 31)) / ((long long)T * T));
+    } else {
+        const int want = p->priv_ovr >= 0 ? p->priv_ovr : default_privatization(p);
+        if (p->mx && batch)
+            kc = p->sphere ? pick_sphere1d_mx_batch(p->D, p->opl) : pick_flat1d_mx_batch(p->D, p->opl);
+        else if (p->mx)
+            kc = p->sphere ? pick_sphere1d_mx(p->D, p->opl, want) : pick_flat1d_mx(p->D, p->opl, want);
+        else
+            kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, want)
+                           : pick_flat1d(p->D, p->mixed, p->df, p->opl, want);
+        if (batch) {
+            T = kBatchTile1D;
+        } else if (p->tile_ovr) {
+            T = p->tile_ovr;
+        } else {
+            T = 64;
+            for (int cand : {256, 128}) {
+                if (tile_pairs(n, cand) >= 4ll * ctx->nsm) { T = cand; break; }
+            }
+        }
+        if (T > kc.max_threads) T = kc.max_threads;
+        if (kc.priv == 3) {
+            // run-length table: the most columns (<= 32) that leave room for 3 blocks per SM,
+            // at least one column
+            hist_cols = p->cols_ovr ? p->cols_ovr : 32;
+            if (!p->cols_ovr) {
+                int smem_sm = 0;
+                CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+                while (hist_cols > 1 && smem_bytes(p, T, lut_bytes, true, 3, hist_cols) + 1024 > (size_t)smem_sm / 3)
+                    hist_cols /= 2;
+            }
+        }
+        smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols);
+        while (smem > (size_t)dev_smem_max && T > 32) {
+            T /= 2;
+            smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols);
+        }
+        if (smem > (size_t)dev_smem_max)
+            return set_err(ctx, SFB200_ERR_UNSUPPORTED, "%d bins x %d operators do not fit shared memory",
+                           p->nb, p->nops);
+        if (kc.priv == 3) {
+            // FP32 table cells are folded into FP64 before any of them holds more than ~4096
+            // pair terms (NW warps x T steps per tile pair add into one column)
+            flush_every = (p->mixed || p->mx) ? std::max(1, 4096 / ((T / 32) * T)) : 64;
+        } else if (kc.priv > 0) {
+            // FP32 copies are folded into FP64 before any lane-bin cell can hold more than ~512 terms
+            const int copies = kc.priv == 2 ? 1 : kc.priv;
+            flush_every = (p->mixed || p->mx) ? std::max(1, 512 * copies / (32 * T)) : 64;
+        }
+    }
+    if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this plan");
+    if (batch && T != (p->joint ? kBatchTileJoint : kBatchTile1D))
+        return set_err(ctx, SFB200_ERR_UNSUPPORTED, "histogram too large for the batched kernels' fixed tiles");
+    CK(cudaFuncSetAttribute(kc.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc.fn, T, smem));
+    if (occ < 1) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "kernel does not fit on an SM (%zu bytes shared)", smem);
+    if (p->bps_ovr) occ = std::min(occ, p->bps_ovr);
+    const long long ntp = tile_pairs(n, T);
+    const long long grid = std::min<long long>(ntp, (long long)ctx->nsm * occ);
+    // the warp-aggregated FP32 histogram counts in 32 bits per warp and bin without folding
+    if (!p->joint && kc.priv == 0 && (p->mixed || p->mx) && ((ntp + grid - 1) / grid) * 32ll * T >= (1ll << 32))
+        return set_err(ctx, SFB200_ERR_UNSUPPORTED,
+                       "privatization 0 would overflow its 32-bit counters at %lld points; use another", n);
+
+    PairArgs a{};
+    a.n = (int)n;
+    a.ntiles = (int)((n + T - 1) / T);
+    a.ntp = ntp;
+    a.X64 = w.d_X64;
+    a.U64 = w.d_U64;
+    a.XF = w.d_XF;
+    a.UF = w.d_UF;
+    a.XM = w.d_XM;
+    a.lut = p->mixed ? (const void*)p->d_lut32 : (const void*)p->d_lut64;
+    a.lg = p->mixed ? p->lg32 : p->lg64;
+    a.chord_wrel = kChordWrel;
+    a.chord_short = 0x1p-40;         // (near-)coincident: the reference frame is degenerate
+    a.chord_anti = 4.0 - 0x1p-40;    // (near-)antipodal: likewise
+    a.lut_bytes = lut_bytes;
+    a.edges = p->d_exact;
+    a.n_edges = p->desc.distance.n_edges;
+    a.dist_linear = dlinear;
+    a.dlin = p->dlin;
+    a.radius = p->desc.radius;
+    a.nb = p->nb;
+    a.nops = p->nops;
+    a.nv = p->nv;
+    a.val_linear = p->joint && p->desc.value.kind == SFB200_BINS_LINEAR;
+    a.vlin = p->vlin;
+    a.vedges = p->d_vedges;
+    a.n_vedges = p->joint ? p->desc.value.n_edges : 0;
+    a.vwin = p->d_vwin;
+    a.flush_every = flush_every;
+    a.hist_cols = hist_cols;
+    // per-pair relative value error: compensated du_L carries ~(6 order + 6) u; otherwise only
+    // the rounding of t itself (the rest is in the per-row absolute window)
+    a.vrel = (float)((p->l_only ? (6.0 * p->vorder + 6.0) * 1.25 : 4.0) * 0x1p-24);
+    // mixed: the FP32 value carries ~5 ulps per order of L / T (conversion, rsqrtf, scaling)
+    if (p->mx) a.vrel = (float)((5.0 * p->vorder + 3.0) * 1.25 * 0x1p-24);
+    a.vq = p->vq;
+    a.vq_inv = p->vq_inv;
+    a.vqc = p->vqc;
+    a.vqc_inv = p->vqc_inv;
+    a.vfine_lo = p->vfine_lo;
+    a.nfine = p->nfine;
+    a.gen = p->gen;
+    a.g_sums = w.d_sums;
+    a.g_counts = w.d_counts;
+    a.g_stats = w.d_aux;
+    out->kc = kc;
+    out->T = T;
+    out->threads = T;
+    out->smem = smem;
+    out->ntp = ntp;
+    out->grid = (long long)ctx->nsm * occ;  // resident blocks; a single run launches min(grid, ntp)
+    out->a = a;
+    return SFB200_OK;
+}
+
 extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t n, uint32_t flags,
                           double* sums, uint64_t* counts, void* stream)
 {
@@ -864,218 +1161,28 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
     if (n > 0 && (!x || !u)) return set_err(ctx, SFB200_ERR_INVALID_ARG, "x/u pointer is NULL");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    const bool dev_in = flags & SFB200_RUN_DEVICE_INPUT;
     const bool dev_out = flags & SFB200_RUN_DEVICE_OUTPUT;
     const bool accumulate = flags & SFB200_RUN_ACCUMULATE;
     int launches = 0;
-
-    CK(cudaMemsetAsync(p->d_sums, 0, sizeof(double) * p->n_sums, s));
-    CK(cudaMemsetAsync(p->d_counts, 0, sizeof(unsigned long long) * p->n_counts, s));
-    CK(cudaMemsetAsync(p->d_aux, 0, sizeof(unsigned long long) * 4, s));
     p->stats = sfb200_stats{};
     p->stats.pairs = n * (n - 1) / 2;
     p->stats_pending = false;
-
+    int rc = prepare_inputs(p, p->ws, x, u, n, flags, s, &launches);
+    if (rc) return rc;
     if (n >= 2) {
-        int rc = ensure_workspace(p, n);
+        LaunchCfg cfg;
+        rc = configure(p, p->ws, n, false, &cfg);
         if (rc) return rc;
-        const size_t xs = p->desc.x_dtype == SFB200_F64 ? 8 : 4;
-        const size_t us = p->desc.u_dtype == SFB200_F64 ? 8 : 4;
-        const void* xin = x;
-        const void* uin = u;
-        if (!dev_in) {
-            CK(cudaMemcpyAsync(p->d_rawx, x, xs * p->W * n, cudaMemcpyHostToDevice, s));
-            CK(cudaMemcpyAsync(p->d_rawu, u, us * p->D * n, cudaMemcpyHostToDevice, s));
-            xin = p->d_rawx;
-            uin = p->d_rawu;
-        }
-        const bool x64 = xs == 8, u64 = us == 8;
-        const int* perm = nullptr;
-        const int order = point_order(p, n);
-        if (order == 1) {
-            rc = x64 ? launch_order<double>(p, xin, (int)n, s, &perm) : launch_order<float>(p, xin, (int)n, s, &perm);
-            if (rc) return rc;
-            launches += 2;  // box + keys (the radix sort's own launches are not counted)
-        } else if (order == 2) {
-            rc = launch_scatter(p, (int)n, s, &perm);
-            if (rc) return rc;
-            launches += 1;
-        }
-        if (x64 && u64) launch_pack<double, double>(p, xin, uin, (int)n, perm, s);
-        else if (x64) launch_pack<double, float>(p, xin, uin, (int)n, perm, s);
-        else if (u64) launch_pack<float, double>(p, xin, uin, (int)n, perm, s);
-        else launch_pack<float, float>(p, xin, uin, (int)n, perm, s);
-        ++launches;
-        CK(cudaGetLastError());
-        if (p->mixed) {
-            k_build_lut32<<<(p->lg32.ncell + 127) / 128, 128, 0, s>>>(p->d_ck, (int)p->ck.size(), p->wp, p->lg32,
-                                                                    p->d_aux + 1, p->d_lut32);
-            ++launches;
-            CK(cudaGetLastError());
-            if (p->joint) {
-                ValueWindowParams vw;
-                vw.nd = p->nb;
-                vw.D = p->D;
-                vw.order = p->vorder;
-                vw.sphere = p->sphere;
-                vw.x_f64 = x64;
-                vw.u_f64 = u64;
-                vw.df = p->df;
-                vw.l_only = p->l_only;
-                vw.inv_step = p->desc.value.kind == SFB200_BINS_LINEAR ? p->vlin.inv_step : 0.0;
-                vw.neg_f_inv = p->desc.value.kind == SFB200_BINS_LINEAR ? p->vlin.neg_f_inv : 0.0;
-                k_value_windows<<<1, 128, 0, s>>>(p->d_rowlo, vw, p->d_aux + 1, p->d_vwin);
-                ++launches;
-                CK(cudaGetLastError());
-            }
-        }
-
-        // launch configuration
-        const bool dlinear = p->desc.distance.kind == SFB200_BINS_LINEAR;
-        int lut_bytes = 0;
-        if (p->mixed) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
-        else if (p->mx) lut_bytes = p->lut64_bytes;  // exact table (flat) or chord table (sphere); 0 if linear
-        else if (!dlinear && !p->joint) lut_bytes = p->lut64_bytes;
-        int T;
-        bool smem_hist = true;
-        KernelChoice kc;
-        size_t smem;
-        int dev_smem_max = 0;
-        CK(cudaDeviceGetAttribute(&dev_smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-        int flush_every = 0;
-        int hist_cols = 32;
-        if (p->joint) {
-            T = p->tile_ovr ? p->tile_ovr : (n >= 32768 ? 512 : (n >= 4096 ? 256 : 64));
-            smem = smem_bytes(p, T, lut_bytes, true, 0);
-            while (p->mx && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr) {
-                T /= 2;
-                smem = smem_bytes(p, T, lut_bytes, true, 0);
-            }
-            if (smem > (size_t)dev_smem_max) {
-                if (p->mixed || p->mx)
-                    return set_err(ctx, SFB200_ERR_UNSUPPORTED,
-                                   "joint histogram of %d x %d cells does not fit shared memory on the mixed path; use fp64",
-                                   p->nb, p->nv);
-                smem_hist = false;
-                smem = smem_bytes(p, T, lut_bytes, false, 0);
-            }
-            kc = p->mx ? pick_joint_mx(p->sphere, p->D, p->opl)
-                       : pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->df, p->opl);
-            // block cells hold at most 2^31 pairs between flushes (T^2 pairs per tile pair); the mixed
-            // kernel's packed cells fewer than 2^20
-            flush_every = (int)std::max<long long>(1, (p->mx ? (1ll << 20) - 1 : (1ll << 31)) / ((long long)T * T));
-        } else {
-            const int want = p->priv_ovr >= 0 ? p->priv_ovr : default_privatization(p);
-            if (p->mx)
-                kc = p->sphere ? pick_sphere1d_mx(p->D, p->opl, want) : pick_flat1d_mx(p->D, p->opl, want);
-            else
-                kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, want)
-                               : pick_flat1d(p->D, p->mixed, p->df, p->opl, want);
-            if (p->tile_ovr) {
-                T = p->tile_ovr;
-            } else {
-                T = 64;
-                for (int cand : {256, 128}) {
-                    if (tile_pairs(n, cand) >= 4ll * ctx->nsm) { T = cand; break; }
-                }
-            }
-            if (T > kc.max_threads) T = kc.max_threads;
-            if (kc.priv == 3) {
-                // run-length table: the most columns (<= 32) that leave room for 3 blocks per SM,
-                // at least one column
-                hist_cols = p->cols_ovr ? p->cols_ovr : 32;
-                if (!p->cols_ovr) {
-                    int smem_sm = 0;
-                    CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
-                    while (hist_cols > 1 && smem_bytes(p, T, lut_bytes, true, 3, hist_cols) + 1024 > (size_t)smem_sm / 3)
-                        hist_cols /= 2;
-                }
-            }
-            smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols);
-            while (smem > (size_t)dev_smem_max && T > 32) {
-                T /= 2;
-                smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols);
-            }
-            if (smem > (size_t)dev_smem_max)
-                return set_err(ctx, SFB200_ERR_UNSUPPORTED, "%d bins x %d operators do not fit shared memory",
-                               p->nb, p->nops);
-            if (kc.priv == 3) {
-                // FP32 table cells are folded into FP64 before any of them holds more than ~4096
-                // pair terms (NW warps x T steps per tile pair add into one column)
-                flush_every = (p->mixed || p->mx) ? std::max(1, 4096 / ((T / 32) * T)) : 64;
-            } else if (kc.priv > 0) {
-                // FP32 copies are folded into FP64 before any lane-bin cell can hold more than ~512 terms
-                const int copies = kc.priv == 2 ? 1 : kc.priv;
-                flush_every = (p->mixed || p->mx) ? std::max(1, 512 * copies / (32 * T)) : 64;
-            }
-        }
-        if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this plan");
-        CK(cudaFuncSetAttribute(kc.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int occ = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc.fn, T, smem));
-        if (occ < 1) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "kernel does not fit on an SM (%zu bytes shared)", smem);
-        if (p->bps_ovr) occ = std::min(occ, p->bps_ovr);
-        const long long ntp = tile_pairs(n, T);
-        const long long grid = std::min<long long>(ntp, (long long)ctx->nsm * occ);
-        // the warp-aggregated FP32 histogram counts in 32 bits per warp and bin without folding
-        if (!p->joint && kc.priv == 0 && (p->mixed || p->mx) && ((ntp + grid - 1) / grid) * 32ll * T >= (1ll << 32))
-            return set_err(ctx, SFB200_ERR_UNSUPPORTED,
-                           "privatization 0 would overflow its 32-bit counters at %lld points; use another", n);
-
-        PairArgs a{};
-        a.n = (int)n;
-        a.ntiles = (int)((n + T - 1) / T);
-        a.ntp = ntp;
-        a.X64 = p->d_X64;
-        a.U64 = p->d_U64;
-        a.XF = p->d_XF;
-        a.UF = p->d_UF;
-        a.XM = p->d_XM;
-        a.lut = p->mixed ? (const void*)p->d_lut32 : (const void*)p->d_lut64;
-        a.lg = p->mixed ? p->lg32 : p->lg64;
-        a.chord_wrel = kChordWrel;
-        a.chord_short = 0x1p-40;         // (near-)coincident: the reference frame is degenerate
-        a.chord_anti = 4.0 - 0x1p-40;    // (near-)antipodal: likewise
-        a.lut_bytes = lut_bytes;
-        a.edges = p->d_exact;
-        a.n_edges = p->desc.distance.n_edges;
-        a.dist_linear = dlinear;
-        a.dlin = p->dlin;
-        a.radius = p->desc.radius;
-        a.nb = p->nb;
-        a.nops = p->nops;
-        a.nv = p->nv;
-        a.val_linear = p->joint && p->desc.value.kind == SFB200_BINS_LINEAR;
-        a.vlin = p->vlin;
-        a.vedges = p->d_vedges;
-        a.n_vedges = p->joint ? p->desc.value.n_edges : 0;
-        a.vwin = p->d_vwin;
-        a.flush_every = flush_every;
-        a.hist_cols = hist_cols;
-        // per-pair relative value error: compensated du_L carries ~(6 order + 6) u; otherwise only
-        // the rounding of t itself (the rest is in the per-row absolute window)
-        a.vrel = (float)((p->l_only ? (6.0 * p->vorder + 6.0) * 1.25 : 4.0) * 0x1p-24);
-        // mixed: the FP32 value carries ~5 ulps per order of L / T (conversion, rsqrtf, scaling)
-        if (p->mx) a.vrel = (float)((5.0 * p->vorder + 3.0) * 1.25 * 0x1p-24);
-        a.vq = p->vq;
-        a.vq_inv = p->vq_inv;
-        a.vqc = p->vqc;
-        a.vqc_inv = p->vqc_inv;
-        a.vfine_lo = p->vfine_lo;
-        a.nfine = p->nfine;
-        a.gen = p->gen;
-        a.g_sums = p->d_sums;
-        a.g_counts = p->d_counts;
-        a.g_stats = p->d_aux;
-        void* args[] = {&a};
+        const long long grid = std::min(cfg.grid, cfg.ntp);
+        void* args[] = {&cfg.a};
         CK(cudaEventRecord(ctx->ev0, s));
-        CK(cudaLaunchKernel(kc.fn, dim3((unsigned)grid), dim3(T), args, smem, s));
+        CK(cudaLaunchKernel(cfg.kc.fn, dim3((unsigned)grid), dim3(cfg.threads), args, cfg.smem, s));
         CK(cudaEventRecord(ctx->ev1, s));
         ++launches;
         CK(cudaGetLastError());
-        p->stats.tile = T;
-        p->stats.threads = T;
-        p->stats.privatization = p->joint ? -1 : kc.priv;
+        p->stats.tile = cfg.T;
+        p->stats.threads = cfg.threads;
+        p->stats.privatization = p->joint ? -1 : cfg.kc.priv;
         p->stats.blocks = (int)grid;
         p->stats_pending = true;
     }
@@ -1083,7 +1190,7 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
     if (dev_out) {
         const long long m = std::max(p->n_sums, p->n_counts);
         if (m > 0) {
-            k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(p->d_sums, p->d_counts, p->n_sums, p->n_counts,
+            k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(p->ws.d_sums, p->ws.d_counts, p->n_sums, p->n_counts,
                                                                  sums, (unsigned long long*)counts, accumulate);
             ++launches;
             CK(cudaGetLastError());
@@ -1091,11 +1198,11 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         p->stats.kernel_launches = launches;
         return SFB200_OK;
     }
-    CK(cudaMemcpyAsync(p->h_sums.data(), p->d_sums, sizeof(double) * p->n_sums, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(p->h_counts.data(), p->d_counts, sizeof(unsigned long long) * p->n_counts,
+    CK(cudaMemcpyAsync(p->h_sums.data(), p->ws.d_sums, sizeof(double) * p->n_sums, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(p->h_counts.data(), p->ws.d_counts, sizeof(unsigned long long) * p->n_counts,
                        cudaMemcpyDeviceToHost, s));
     unsigned long long aux0 = 0;
-    CK(cudaMemcpyAsync(&aux0, p->d_aux, sizeof(aux0), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&aux0, p->ws.d_aux, sizeof(aux0), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     for (long long k = 0; k < p->n_sums; ++k) sums[k] = (accumulate ? sums[k] : 0.0) + p->h_sums[k];
     for (long long k = 0; k < p->n_counts; ++k) counts[k] = (accumulate ? counts[k] : 0ull) + p->h_counts[k];
@@ -1120,10 +1227,308 @@ extern "C" int sfb200_plan_last_stats(const sfb200_plan* pc, sfb200_stats* out)
         CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         p->stats.kernel_ms = ms;
         unsigned long long aux0 = 0;
-        CK(cudaMemcpy(&aux0, p->d_aux, sizeof(aux0), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&aux0, p->ws.d_aux, sizeof(aux0), cudaMemcpyDeviceToHost));
         p->stats.rechecked = (int64_t)aux0;
         p->stats_pending = false;
     }
     *out = p->stats;
+    return SFB200_OK;
+}
+
+// ------------------------------------------------------------------------------- serving
+
+struct sfb200_slice {
+    sfb200_plan* plan = nullptr;
+    Workspace w;
+    LaunchCfg cfg;
+    long long n = 0;
+    cudaEvent_t ready = nullptr;  // preparation finished (recorded on the preparation stream)
+};
+
+extern "C" int sfb200_slice_create(sfb200_plan* p, const void* x, const void* u, int64_t n, uint32_t flags,
+                                   void* stream, sfb200_slice** out)
+{
+    if (!p || !out) return SFB200_ERR_INVALID_ARG;
+    sfb200_ctx* ctx = p->ctx;
+    *out = nullptr;
+    if (!p->mx) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "batched slices need a plan of precision MIXED");
+    if (n < 0) return set_err(ctx, SFB200_ERR_INVALID_ARG, "negative point count");
+    if (n > (1ll << 31) - 1024) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "more than 2^31 points");
+    if (n > 0 && (!x || !u)) return set_err(ctx, SFB200_ERR_INVALID_ARG, "x/u pointer is NULL");
+    if (flags & ~SFB200_RUN_DEVICE_INPUT) return set_err(ctx, SFB200_ERR_INVALID_ARG, "slice flags: DEVICE_INPUT only");
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->prep_stream) CK(cudaStreamCreateWithFlags(&ctx->prep_stream, cudaStreamNonBlocking));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->prep_stream;
+    sfb200_slice* sl = new (std::nothrow) sfb200_slice();
+    if (!sl) return SFB200_ERR_OOM;
+    sl->plan = p;
+    sl->n = n;
+    int rc = ensure_workspace(p, sl->w, std::max<long long>(n, 2));
+    if (!rc) rc = alloc_outputs(p, sl->w);
+    int launches = 0;
+    if (!rc) rc = prepare_inputs(p, sl->w, x, u, n, flags, s, &launches);
+    if (!rc && n >= 2) rc = configure(p, sl->w, n, true, &sl->cfg);
+    cudaError_t e = cudaSuccess;
+    if (!rc) {
+        e = cudaEventCreateWithFlags(&sl->ready, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(sl->ready, s);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "slice event");
+    }
+    if (rc) {
+        cudaStreamSynchronize(s);
+        if (sl->ready) cudaEventDestroy(sl->ready);
+        free_workspace(sl->w, true);
+        delete sl;
+        return rc;
+    }
+    if (n < 2) sl->cfg.ntp = 0;
+    *out = sl;
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_slice_get_info(const sfb200_slice* sl, sfb200_slice_info* out)
+{
+    if (!sl || !out) return SFB200_ERR_INVALID_ARG;
+    out->n_points = sl->n;
+    out->pairs = sl->n * (sl->n - 1) / 2;
+    out->tile_pairs = sl->cfg.ntp;
+    out->device_bytes = (int64_t)sl->w.bytes;
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_slice_destroy(sfb200_slice* sl)
+{
+    if (!sl) return SFB200_ERR_INVALID_ARG;
+    sfb200_ctx* ctx = sl->plan->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->prep_stream) cudaStreamSynchronize(ctx->prep_stream);
+    if (sl->ready) cudaEventDestroy(sl->ready);
+    free_workspace(sl->w, true);
+    delete sl;
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_device_memory(sfb200_ctx* ctx, int64_t* free_bytes, int64_t* total_bytes)
+{
+    if (!ctx || !free_bytes || !total_bytes) return SFB200_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    size_t f = 0, t = 0;
+    CK(cudaMemGetInfo(&f, &t));
+    *free_bytes = (int64_t)f;
+    *total_bytes = (int64_t)t;
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_slice_read(sfb200_slice* sl, double* sums, uint64_t* counts, uint32_t flags, void* stream)
+{
+    if (!sl || !sums || !counts) return SFB200_ERR_INVALID_ARG;
+    sfb200_plan* p = sl->plan;
+    sfb200_ctx* ctx = p->ctx;
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    const bool accumulate = flags & SFB200_RUN_ACCUMULATE;
+    if (flags & SFB200_RUN_DEVICE_OUTPUT) {
+        const long long m = std::max(p->n_sums, p->n_counts);
+        k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(sl->w.d_sums, sl->w.d_counts, p->n_sums, p->n_counts,
+                                                             sums, (unsigned long long*)counts, accumulate);
+        CK(cudaGetLastError());
+        return SFB200_OK;
+    }
+    std::vector<double> hs(p->n_sums);
+    std::vector<unsigned long long> hc(p->n_counts);
+    CK(cudaMemcpyAsync(hs.data(), sl->w.d_sums, sizeof(double) * p->n_sums, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hc.data(), sl->w.d_counts, sizeof(unsigned long long) * p->n_counts, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (long long k = 0; k < p->n_sums; ++k) sums[k] = (accumulate ? sums[k] : 0.0) + hs[k];
+    for (long long k = 0; k < p->n_counts; ++k) counts[k] = (accumulate ? counts[k] : 0ull) + hc[k];
+    return SFB200_OK;
+}
+
+// Tile pairs per work item: small enough to balance the end of a round across SMs, large enough
+// that the per-item setup (table copy, histogram clear and merge) stays a few percent.
+static long long item_tile_pairs(const sfb200_plan* p) { return p->joint ? 1 : 4; }
+
+extern "C" int sfb200_batch_run(sfb200_ctx* ctx, int32_t n, sfb200_slice* const* slices, const int64_t* tp_begin,
+                                const int64_t* tp_end, void* stream)
+{
+    if (!ctx || n < 0 || (n > 0 && (!slices || !tp_begin || !tp_end))) return SFB200_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    // group the listed ranges by kernel; chunks of at most kBatchSlices slices per launch
+    struct Launch {
+        const void* fn;
+        int threads;
+        size_t smem;
+        int nslices;
+        BatchArgs args;
+        size_t item0, nitems;
+    };
+    std::vector<Launch> launches;
+    std::vector<WorkItem> items;
+    std::vector<int> order(n);
+    for (int k = 0; k < n; ++k) {
+        order[k] = k;
+        const sfb200_slice* sl = slices[k];
+        if (!sl || sl->plan->ctx != ctx) return set_err(ctx, SFB200_ERR_INVALID_ARG, "slice %d is NULL or of another context", k);
+        if (tp_begin[k] < 0 || tp_end[k] > sl->cfg.ntp || tp_begin[k] > tp_end[k])
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "slice %d: tile-pair range [%lld, %lld) outside [0, %lld)", k,
+                           (long long)tp_begin[k], (long long)tp_end[k], sl->cfg.ntp);
+        for (int j = 0; j < k; ++j)
+            if (slices[j] == sl) return set_err(ctx, SFB200_ERR_INVALID_ARG, "slice %d listed twice in one round", k);
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return reinterpret_cast<uintptr_t>(slices[a]->cfg.kc.fn) < reinterpret_cast<uintptr_t>(slices[b]->cfg.kc.fn);
+    });
+    for (int oi = 0; oi < n; ++oi) {
+        const int k = order[oi];
+        const sfb200_slice* sl = slices[k];
+        if (tp_end[k] <= tp_begin[k]) continue;
+        if (launches.empty() || launches.back().fn != sl->cfg.kc.fn || launches.back().nslices == kBatchSlices) {
+            Launch L{};
+            L.fn = sl->cfg.kc.fn;
+            L.threads = sl->cfg.threads;
+            L.item0 = items.size();
+            launches.push_back(L);
+        }
+        Launch& L = launches.back();
+        const int j = L.nslices++;
+        L.args.s[j] = sl->cfg.a;
+        L.smem = std::max(L.smem, sl->cfg.smem);
+        const long long step = item_tile_pairs(sl->plan);
+        for (long long q = tp_begin[k]; q < tp_end[k]; q += step)
+            items.push_back(WorkItem{j, 0, q, std::min<long long>(q + step, tp_end[k])});
+        L.nitems = items.size() - L.item0;
+    }
+    if (launches.empty()) return SFB200_OK;
+    // the previous round must have consumed the item buffer; the slices must be prepared
+    if (!ctx->round_done) {
+        CK(cudaEventCreateWithFlags(&ctx->round_done, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+        for (int k = 0; k < sfb200_ctx::kLanes; ++k) {
+            CK(cudaStreamCreateWithFlags(&ctx->lane[k], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&ctx->join[k], cudaEventDisableTiming));
+        }
+    }
+    if (ctx->round_pending) CK(cudaEventSynchronize(ctx->round_done));
+    for (int k = 0; k < n; ++k) CK(cudaStreamWaitEvent(s, slices[k]->ready, 0));
+    // buffers (before any capture)
+    if (items.size() > ctx->items_cap) {
+        CK(cudaStreamSynchronize(s));
+        if (ctx->h_items) cudaFreeHost(ctx->h_items);
+        cudaFree(ctx->d_items);
+        ctx->h_items = nullptr;
+        ctx->d_items = nullptr;
+        ctx->items_cap = 0;
+        const size_t cap = std::max<size_t>(items.size() * 2, 4096);
+        CK(cudaMallocHost(&ctx->h_items, cap * sizeof(WorkItem)));
+        CK(cudaMalloc(&ctx->d_items, cap * sizeof(WorkItem)));
+        ctx->items_cap = cap;
+    }
+    if ((int)launches.size() > ctx->counters_cap) {
+        CK(cudaStreamSynchronize(s));
+        cudaFree(ctx->d_counters);
+        ctx->d_counters = nullptr;
+        const int cap = std::max<int>((int)launches.size() * 2, 64);
+        CK(cudaMalloc(&ctx->d_counters, cap * sizeof(unsigned)));
+        ctx->counters_cap = cap;
+    }
+    std::memcpy(ctx->h_items, items.data(), items.size() * sizeof(WorkItem));
+    const WorkItem* d_items = static_cast<const WorkItem*>(ctx->d_items);
+    for (size_t l = 0; l < launches.size(); ++l) {
+        Launch& L = launches[l];
+        CK(cudaFuncSetAttribute(L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+        L.args.items = d_items + L.item0;
+        L.args.n_items = (int)L.nitems;
+        L.args.counter = ctx->d_counters + l;
+    }
+    // grids (before any capture): at most the resident blocks, at most one block per item
+    std::vector<long long> grids(launches.size());
+    for (size_t l = 0; l < launches.size(); ++l) {
+        int occ = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, launches[l].fn, launches[l].threads, launches[l].smem));
+        grids[l] = std::min<long long>((long long)launches[l].nitems, (long long)ctx->nsm * std::max(occ, 1));
+    }
+    // item copy and counter reset on s, then the kernels forked over the lanes (they run
+    // concurrently and share the SMs), joined back into s
+    const int nlanes = (int)std::min<size_t>(launches.size(), sfb200_ctx::kLanes);
+    auto enqueue = [&]() -> cudaError_t {
+        cudaError_t e = cudaMemcpyAsync(ctx->d_items, ctx->h_items, items.size() * sizeof(WorkItem),
+                                        cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_counters, 0, launches.size() * sizeof(unsigned), s);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->fork, s);
+        for (int k = 0; k < nlanes && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(ctx->lane[k], ctx->fork, 0);
+        for (size_t l = 0; l < launches.size() && e == cudaSuccess; ++l) {
+            Launch& L = launches[l];
+            void* args[] = {&L.args};
+            e = cudaLaunchKernel(L.fn, dim3((unsigned)grids[l]), dim3(L.threads), args, L.smem,
+                                 ctx->lane[l % sfb200_ctx::kLanes]);
+        }
+        for (int k = 0; k < nlanes && e == cudaSuccess; ++k) {
+            e = cudaEventRecord(ctx->join[k], ctx->lane[k]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->join[k], 0);
+        }
+        return e;
+    };
+    if (ctx->batch_graph) {
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            const cudaError_t e1 = enqueue();
+            e = cudaStreamEndCapture(s, &graph);
+            if (e1 != cudaSuccess) e = e1;
+        }
+        if (e == cudaSuccess && ctx->batch_exec) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(ctx->batch_exec, graph, &info) != cudaSuccess) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(ctx->batch_exec);
+                ctx->batch_exec = nullptr;
+            }
+        }
+        if (e == cudaSuccess && !ctx->batch_exec) e = cudaGraphInstantiate(&ctx->batch_exec, graph, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(ctx->batch_exec, s);
+        if (graph) cudaGraphDestroy(graph);
+        if (e == cudaSuccess) {
+            CK(cudaEventRecord(ctx->round_done, s));
+            ctx->round_pending = true;
+            return SFB200_OK;
+        }
+        // capture or replay refused: run this and later rounds with plain launches
+        cudaGetLastError();
+        ctx->batch_graph = false;
+        if (ctx->batch_exec) {
+            cudaGraphExecDestroy(ctx->batch_exec);
+            ctx->batch_exec = nullptr;
+        }
+    }
+    CK(enqueue());
+    CK(cudaEventRecord(ctx->round_done, s));
+    ctx->round_pending = true;
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_batch_wait(sfb200_ctx* ctx)
+{
+    if (!ctx) return SFB200_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->round_pending) CK(cudaEventSynchronize(ctx->round_done));
+    ctx->round_pending = false;
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_batch_query(sfb200_ctx* ctx, int32_t* done)
+{
+    if (!ctx || !done) return SFB200_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    *done = 1;
+    if (!ctx->round_pending) return SFB200_OK;
+    const cudaError_t e = cudaEventQuery(ctx->round_done);
+    if (e == cudaErrorNotReady) {
+        *done = 0;
+        return SFB200_OK;
+    }
+    CK(e);
+    ctx->round_pending = false;
     return SFB200_OK;
 }

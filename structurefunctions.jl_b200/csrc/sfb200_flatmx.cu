@@ -48,4 +48,29 @@ KernelChoice pick_flat1d_mx(int D, int opl, int priv)
     return {nullptr, 0, 0};
 }
 
+// Batched (serving) form: run-length histogram only.
+template <int D>
+static KernelChoice flat1d_mx_batch_by_list(int opl)
+{
+    switch (opl) {
+    case OPL_L2: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_L2>, 3>), 256, 3};
+    case OPL_L3: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_L3>, 3>), 256, 3};
+    case OPL_L1: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_L1>, 3>), 256, 3};
+    case OPL_QUAD: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, 3>), 256, 3};
+    case OPL_GEN1: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_GEN>, 3>), 256, 3};
+    case OPL_GEN2: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_GEN, OC_GEN>, 3>), 256, 3};
+    case OPL_GEN4: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, 3>), 256, 3};
+    case OPL_GEN8:
+        return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN>, 3>), 256, 3};
+    }
+    return {nullptr, 0, 0};
+}
+
+KernelChoice pick_flat1d_mx_batch(int D, int opl)
+{
+    if (D == 2) return flat1d_mx_batch_by_list<2>(opl);
+    if (D == 3) return flat1d_mx_batch_by_list<3>(opl);
+    return {nullptr, 0, 0};
+}
+
 }  // namespace sfb

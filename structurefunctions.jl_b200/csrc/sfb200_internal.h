@@ -39,5 +39,9 @@ KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, bool df,
 KernelChoice pick_flat1d_mx(int D, int opl, int priv);
 KernelChoice pick_sphere1d_mx(int D, int opl, int priv);
 KernelChoice pick_joint_mx(bool sphere, int D, int opl);
+// Batched (serving) forms of the mixed kernels: BatchArgs parameter, run-length histogram.
+KernelChoice pick_flat1d_mx_batch(int D, int opl);
+KernelChoice pick_sphere1d_mx_batch(int D, int opl);
+KernelChoice pick_joint_mx_batch(bool sphere, int D, int opl);
 
 }  // namespace sfb

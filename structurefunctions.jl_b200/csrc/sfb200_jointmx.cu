@@ -22,4 +22,22 @@ KernelChoice pick_joint_mx(bool sphere, int D, int opl)
     return D == 2 ? jointmx_by_list<false, 2>(opl) : jointmx_by_list<false, 3>(opl);
 }
 
+template <bool SPHERE, int D>
+static KernelChoice jointmx_batch_by_list(int opl)
+{
+    switch (opl) {
+    case OPL_L1: return {reinterpret_cast<const void*>(&k_joint_mx_batch<SPHERE, D, OpList<OC_L1>>), 512, 0};
+    case OPL_L2: return {reinterpret_cast<const void*>(&k_joint_mx_batch<SPHERE, D, OpList<OC_L2>>), 512, 0};
+    case OPL_L3: return {reinterpret_cast<const void*>(&k_joint_mx_batch<SPHERE, D, OpList<OC_L3>>), 512, 0};
+    case OPL_GEN1: return {reinterpret_cast<const void*>(&k_joint_mx_batch<SPHERE, D, OpList<OC_GEN>>), 512, 0};
+    }
+    return {nullptr, 0, 0};
+}
+
+KernelChoice pick_joint_mx_batch(bool sphere, int D, int opl)
+{
+    if (sphere) return D == 2 ? jointmx_batch_by_list<true, 2>(opl) : jointmx_batch_by_list<true, 3>(opl);
+    return D == 2 ? jointmx_batch_by_list<false, 2>(opl) : jointmx_batch_by_list<false, 3>(opl);
+}
+
 }  // namespace sfb

@@ -72,6 +72,41 @@ struct PairArgs {
     unsigned long long* g_stats; // [0] rechecked pairs
 };
 
+// ---------------------------------------------------------------------------- batched launches
+// One launch serves many independent point sets ("slices"): the arguments of up to kBatchSlices
+// slices travel in the kernel parameter block (constant bank, uniform per block), and the blocks of a
+// persistent grid pull work items -- a slice and a range of its tile pairs -- from a device counter.
+struct WorkItem {
+    int slice;
+    int pad;
+    long long p0, p1;  // tile pairs [p0, p1) of the slice
+};
+
+constexpr int kBatchSlices = 48;  // 48 x sizeof(PairArgs) stays below the 32 KB parameter limit
+
+struct BatchArgs {
+    const WorkItem* items;
+    int n_items;
+    unsigned* counter;  // zeroed before the launch
+    PairArgs s[kBatchSlices];
+};
+static_assert(sizeof(BatchArgs) <= 32000, "batch arguments must fit the kernel parameter block");
+
+template <class RUN>
+__device__ __forceinline__ void batch_items(const BatchArgs& b, RUN run)
+{
+    __shared__ int s_item;
+    for (;;) {
+        __syncthreads();  // the previous item (and its use of shared memory) is finished
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(b.counter, 1u);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= b.n_items) break;
+        const WorkItem w = b.items[it];
+        run(b.s[w.slice], w.p0, w.p1);
+    }
+}
+
 // Exact FP64 bin of a flat pair from r^2 (src/BinEdges.jl:515-517).
 __device__ __forceinline__ int flat_exact_bin(const PairArgs& a, double r2)
 {

@@ -166,7 +166,7 @@ __device__ __forceinline__ void flat_values_fp64(const double (&dx)[D], const do
 // warp in lockstep with out-of-range pairs sent to the dropped row.
 // ================================================================================================
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256) k_flat1d_mx(const PairArgs a)
+__device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, long long p1, long long ps)
 {
     constexpr int NV = OPS::n;
     constexpr int NP = D;  // double2 per j record: x(D) u(D)
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(256) k_flat1d_mx(const PairArgs a)
     op_unscale(OPS{}, a.gen, ku, unscale);
 
     int iter = 0;
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+    for (long long p = p0; p < p1; p += ps, ++iter) {
         hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
@@ -256,6 +256,19 @@ __global__ void __launch_bounds__(256) k_flat1d_mx(const PairArgs a)
         }
     }
     hist.merge(a.g_sums, a.g_counts, a.nops, a.nb, unscale);
+}
+
+template <int D, class OPS, int PRIV>
+__global__ void __launch_bounds__(256) k_flat1d_mx(const PairArgs a)
+{
+    flat1d_mx_run<D, OPS, PRIV>(a, blockIdx.x, a.ntp, gridDim.x);
+}
+
+// Batched form: work items (slice, tile-pair range) pulled from a device counter.
+template <int D, class OPS, int PRIV>
+__global__ void __launch_bounds__(256) k_flat1d_mx_batch(const BatchArgs b)
+{
+    batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { flat1d_mx_run<D, OPS, PRIV>(a, q0, q1, 1); });
 }
 
 // ================================================================================================
@@ -356,7 +369,7 @@ __device__ __forceinline__ double sphere_primitives_mx(const double* ra, const d
 }
 
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
+__device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0, long long p1, long long ps)
 {
     constexpr int NV = OPS::n;
     constexpr int NP = 5;  // double2 per record: p(3) U(3) W(3) up/pad(1)
@@ -381,7 +394,7 @@ __global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
     constexpr int NF = 9 + (D == 3);  // stored fields
 
     int iter = 0;
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+    for (long long p = p0; p < p1; p += ps, ++iter) {
         hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
@@ -449,6 +462,19 @@ __global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 
+template <int D, class OPS, int PRIV>
+__global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
+{
+    sphere1d_mx_run<D, OPS, PRIV>(a, blockIdx.x, a.ntp, gridDim.x);
+}
+
+// Batched form: work items (slice, tile-pair range) pulled from a device counter.
+template <int D, class OPS, int PRIV>
+__global__ void __launch_bounds__(256, 3) k_sphere1d_mx_batch(const BatchArgs b)
+{
+    batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { sphere1d_mx_run<D, OPS, PRIV>(a, q0, q1, 1); });
+}
+
 // ================================================================================================
 // Joint (distance x value) histogram
 //
@@ -490,7 +516,7 @@ __device__ __forceinline__ void joint_flush_packed(const PairArgs& a, unsigned l
 }
 
 template <bool SPHERE, int D, class OPS>
-__global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
+__device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, long long p1, long long ps)
 {
     constexpr int NP = SPHERE ? 5 : D;
     constexpr int NF = SPHERE ? 9 + (D == 3) : 2 * D;  // stored fields per record
@@ -527,7 +553,7 @@ __global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
     };
 
     int iter = 0;
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+    for (long long p = p0; p < p1; p += ps, ++iter) {
         if (iter && iter % a.flush_every == 0) {
             __syncthreads();
             joint_flush_packed(a, hcell, hfine, ncell);
@@ -640,6 +666,19 @@ __global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
     __syncthreads();
     joint_flush_packed(a, hcell, hfine, ncell);
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
+}
+
+template <bool SPHERE, int D, class OPS>
+__global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
+{
+    joint_mx_run<SPHERE, D, OPS>(a, blockIdx.x, a.ntp, gridDim.x);
+}
+
+// Batched form: work items (slice, tile-pair range) pulled from a device counter.
+template <bool SPHERE, int D, class OPS>
+__global__ void __launch_bounds__(512) k_joint_mx_batch(const BatchArgs b)
+{
+    batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { joint_mx_run<SPHERE, D, OPS>(a, q0, q1, 1); });
 }
 
 }  // namespace sfb

@@ -93,6 +93,15 @@ class Stats(C.Structure):
     ]
 
 
+class SliceInfo(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_int64),
+        ("pairs", C.c_int64),
+        ("tile_pairs", C.c_int64),
+        ("device_bytes", C.c_int64),
+    ]
+
+
 # Every symbol include/sfb200.h declares (checked by the CPU test suite against the built library).
 EXPORTED_SYMBOLS = (
     "sfb200_abi_version",
@@ -107,6 +116,14 @@ EXPORTED_SYMBOLS = (
     "sfb200_plan_last_stats",
     "sfb200_plan_set_launch",
     "sfb200_plan_set_option",
+    "sfb200_slice_create",
+    "sfb200_slice_get_info",
+    "sfb200_batch_run",
+    "sfb200_slice_read",
+    "sfb200_slice_destroy",
+    "sfb200_device_memory",
+    "sfb200_batch_wait",
+    "sfb200_batch_query",
 )
 
 # sfb200_option

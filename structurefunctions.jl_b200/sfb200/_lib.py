@@ -51,6 +51,22 @@ def load():
         lib.sfb200_plan_set_launch.restype = C.c_int
         lib.sfb200_plan_set_option.argtypes = [P, C.c_int, C.c_int64]
         lib.sfb200_plan_set_option.restype = C.c_int
+        lib.sfb200_slice_create.argtypes = [P, P, P, C.c_int64, C.c_uint32, P, C.POINTER(P)]
+        lib.sfb200_slice_create.restype = C.c_int
+        lib.sfb200_slice_get_info.argtypes = [P, C.POINTER(_abi.SliceInfo)]
+        lib.sfb200_slice_get_info.restype = C.c_int
+        lib.sfb200_batch_run.argtypes = [P, C.c_int32, C.POINTER(P), C.POINTER(C.c_int64), C.POINTER(C.c_int64), P]
+        lib.sfb200_batch_run.restype = C.c_int
+        lib.sfb200_slice_read.argtypes = [P, P, P, C.c_uint32, P]
+        lib.sfb200_slice_read.restype = C.c_int
+        lib.sfb200_slice_destroy.argtypes = [P]
+        lib.sfb200_slice_destroy.restype = C.c_int
+        lib.sfb200_device_memory.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        lib.sfb200_device_memory.restype = C.c_int
+        lib.sfb200_batch_wait.argtypes = [P]
+        lib.sfb200_batch_wait.restype = C.c_int
+        lib.sfb200_batch_query.argtypes = [P, C.POINTER(C.c_int32)]
+        lib.sfb200_batch_query.restype = C.c_int
         if lib.sfb200_abi_version() != _abi.ABI_VERSION:
             raise OSError(f"libsfb200.so ABI {lib.sfb200_abi_version()} != {_abi.ABI_VERSION}")
         _lib = lib
@@ -100,6 +116,63 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+def device_memory(ctx):
+    """(free, total) device bytes of the context's device."""
+    f, t = C.c_int64(), C.c_int64()
+    check(load().sfb200_device_memory(ctx.ptr, C.byref(f), C.byref(t)), ctx.ptr)
+    return f.value, t.value
+
+
+class Slice:
+    """One point set resident on the device with its own histogram (sfb200_slice_*)."""
+
+    def __init__(self, plan, x_ptr, u_ptr, n, flags=0, stream=None):
+        self.plan = plan
+        ptr = C.c_void_p()
+        check(load().sfb200_slice_create(plan.ptr, x_ptr, u_ptr, int(n), int(flags), stream, C.byref(ptr)),
+              plan.ctx.ptr, "slice")
+        self.ptr = ptr
+        info = _abi.SliceInfo()
+        check(load().sfb200_slice_get_info(ptr, C.byref(info)), plan.ctx.ptr)
+        self.n_points, self.pairs = info.n_points, info.pairs
+        self.tile_pairs, self.device_bytes = info.tile_pairs, info.device_bytes
+
+    def read(self, sums_ptr, counts_ptr, flags=0, stream=None):
+        check(load().sfb200_slice_read(self.ptr, sums_ptr, counts_ptr, int(flags), stream), self.plan.ctx.ptr, "read")
+
+    def close(self):
+        if self.ptr:
+            load().sfb200_slice_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_run(ctx, slices, begins, ends, stream=None):
+    """One round of sfb200_batch_run over (slice, [begin, end)) tile-pair ranges."""
+    n = len(slices)
+    arr = (C.c_void_p * max(n, 1))(*[s.ptr for s in slices])
+    b = (C.c_int64 * max(n, 1))(*[int(v) for v in begins])
+    e = (C.c_int64 * max(n, 1))(*[int(v) for v in ends])
+    check(load().sfb200_batch_run(ctx.ptr, n, arr, b, e, stream), ctx.ptr, "batch")
+
+
+def batch_wait(ctx):
+    """Block until the context's last round has finished."""
+    check(load().sfb200_batch_wait(ctx.ptr), ctx.ptr, "batch wait")
+
+
+def batch_done(ctx):
+    """True when the context's last round has finished (non-blocking)."""
+    d = C.c_int32()
+    check(load().sfb200_batch_query(ctx.ptr, C.byref(d)), ctx.ptr, "batch query")
+    return bool(d.value)
 
 
 class Plan:

@@ -151,6 +151,66 @@ def config(name, n=None):
     raise KeyError(name)
 
 
+def _serving_request(seed, k, n_min, n_max):
+    """Request k of the serving workload (its own generator, seeded by (seed, k))."""
+    rng = np.random.default_rng([seed, k])
+    n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+    kind = int(rng.integers(0, 3))
+    nb = int(rng.integers(32, 65))
+    ops = (OP.L2SF,) if rng.random() < 0.5 else (OP.L3SF,)
+    joint = rng.random() < 0.5
+    if kind == 0:
+        x = rng.random((2, n))
+        u = planar_field(x, 32, 64.0, rng, 0.01)
+        edges, metric = log_edges(1e-3, math.sqrt(2.0), nb), Euclidean()
+    elif kind == 1:
+        x = rng.random((3, n))
+        u = solenoidal_field(x, 64, 128.0, rng)
+        edges, metric = log_edges(1e-4, math.sqrt(3.0), nb), Euclidean()
+    else:
+        x = sphere_points(n, rng)
+        u = sphere_field(x, 48, 200, rng).astype(np.float32)
+        x = x.astype(np.float32)
+        edges, metric = log_edges(1.0, 20000.0, nb), Haversine(6371.0)
+    vb = None
+    if joint:
+        sigma = math.sqrt(2.0) * float(np.std(u.astype(np.float64)))
+        vb = LinearBinEdges(-5.0 * sigma, 5.0 * sigma, 257)
+    return {"x": x, "u": u, "ops": ops, "edges": edges, "metric": metric, "value_bins": vb,
+            "kind": ("flat2", "flat3", "sphere")[kind], "n": n}
+
+
+def _serving_chunk(args):
+    seed, ks, n_min, n_max = args
+    return [_serving_request(seed, k, n_min, n_max) for k in ks]
+
+
+def serving_requests(count=2000, rate=200.0, seed=4, n_min=1000, n_max=100000, workers=0):
+    """The batched-serving workload: `count` requests with Poisson arrivals (`rate` per second).
+
+    Each request: N log-uniform in [n_min, n_max]; geometry uniformly 2D planar (c0's field), 3D
+    planar (c1's field) or spherical (c2's field, Float32); 32-64 log distance bins over the geometry's
+    range; order 2 or 3 (L2SF or L3SF); half of them also ask for the joint du_L histogram with 256
+    linear value bins over [-5 sigma, 5 sigma]. Request k draws from its own generator (seed, k), so
+    the set does not depend on `workers` (processes generating in parallel; 0 = in this process).
+    Returns a list of dicts with keys `t` (arrival, seconds), `x`, `u`, `ops`, `edges`, `metric`,
+    `value_bins` (None or LinearBinEdges), `kind`, `n`.
+    """
+    arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, count))
+    if workers and workers > 1:
+        import concurrent.futures as cf
+        import multiprocessing as mp
+
+        chunks = [list(range(a, min(a + 25, count))) for a in range(0, count, 25)]
+        with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as pool:
+            reqs = [r for part in pool.map(_serving_chunk, [(seed, c, n_min, n_max) for c in chunks]) for r in part]
+    else:
+        reqs = [_serving_request(seed, k, n_min, n_max) for k in range(count)]
+    for r, t in zip(reqs, arrivals):
+        r["t"] = float(t)
+    return reqs
+
+
 # Algorithmic flops per pair: the reference's FP64 formula as restated by the oracle, counting +, -,
 # x, / and sqrt as 1, FMA as 2, one add per accumulated sum; binning compares and recheck work are
 # not counted. These are the roofline numerators.

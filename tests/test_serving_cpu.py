@@ -1,0 +1,182 @@
+"""The continuous-batching loop (sfb200.serving.Server) driven by a simulated executor, on the CPU.
+
+The executor mirrors the library's slice / round contract: a request becomes `tile_pairs` units of
+work (256-point tiles), a round runs tile-pair ranges of several slices, and a slice's result is
+readable once every unit ran. The simulation records every range, so the tests can check the
+invariants the GPU path relies on: each tile pair of each request runs exactly once, in order;
+admission honours the slot count and the memory reserve; every admitted slice progresses in every
+round; short requests are not held behind long ones; a bad request fails alone.
+"""
+import threading
+
+import numpy as np
+import pytest
+
+from sfb200.serving import Request, Server
+
+T = 256
+
+
+class FakeHandle:
+    def __init__(self, req, nbytes):
+        nt = (req.n + T - 1) // T
+        self.tile_pairs = nt * (nt + 1) // 2 if req.n >= 2 else 0
+        self.pairs = req.n * (req.n - 1) // 2
+        self.device_bytes = nbytes
+        self.req = req
+        self.ranges = []
+
+
+class FakeExecutor:
+    def __init__(self, memory=10_000_000, bytes_per_point=100, fail_n=None):
+        self.memory = memory
+        self.used = 0
+        self.bpp = bytes_per_point
+        self.fail_n = fail_n
+        self.rounds = []
+        self.live = 0
+        self.max_live = 0
+        self.admissions = []  # (slices live before, free bytes after)
+
+    def estimate_bytes(self, req):
+        return req.n * self.bpp
+
+    def free_bytes(self):
+        return self.memory - self.used
+
+    def create(self, req):
+        if self.fail_n is not None and req.n == self.fail_n:
+            raise ValueError("rejected")
+        h = FakeHandle(req, self.estimate_bytes(req))
+        before = self.live
+        self.used += h.device_bytes
+        self.live += 1
+        self.max_live = max(self.max_live, self.live)
+        self.admissions.append((before, self.free_bytes()))
+        return h
+
+    def run_round(self, work):
+        self.rounds.append([(h, b, e) for h, b, e in work])
+        for h, b, e in work:
+            h.ranges.append((b, e))
+
+    def wait_round(self):
+        pass
+
+    def read(self, h):
+        # the "histogram": how many times each tile pair ran (must be all ones)
+        cover = np.zeros(h.tile_pairs, dtype=np.int64)
+        for b, e in h.ranges:
+            cover[b:e] += 1
+        return cover.astype(np.float64), np.array([h.req.n], dtype=np.uint64)
+
+    def destroy(self, h):
+        self.used -= h.device_bytes
+        self.live -= 1
+
+
+def req(n, tag=None):
+    x = np.zeros((2, n))
+    return Request((), x, x, [0.0, 1.0], tag=tag)
+
+
+def test_every_tile_pair_runs_exactly_once_in_order():
+    ex = FakeExecutor()
+    srv = Server(ex, max_slots=4, round_pairs=5e5, memory_reserve=0)
+    sizes = [1, 2, 300, 1000, 5000, 20000, 700, 2, 256, 257]
+    tickets = [srv.submit(req(n)) for n in sizes]
+    srv.run_until_idle()
+    for t, n in zip(tickets, sizes):
+        sums, counts = t.wait(0)
+        assert int(counts[0]) == n
+        assert np.all(sums == 1.0)  # every unit exactly once
+    handles = {}
+    for r in ex.rounds:
+        for h, b, e in r:
+            assert 0 <= b < e <= h.tile_pairs
+            handles[id(h)] = h
+    for h in handles.values():  # a slice's ranges are contiguous and increasing
+        ends = [0] + [e for _, e in h.ranges]
+        assert [b for b, _ in h.ranges] == ends[:-1]
+    assert ex.live == 0 and ex.used == 0
+
+
+def test_slots_bound_concurrency():
+    ex = FakeExecutor()
+    srv = Server(ex, max_slots=3, round_pairs=1e5, memory_reserve=0)
+    for n in [3000] * 10:
+        srv.submit(req(n))
+    srv.run_until_idle()
+    assert ex.max_live <= 3
+    assert max(len(r) for r in ex.rounds) <= 3
+
+
+def test_memory_reserve_bounds_admission():
+    ex = FakeExecutor(memory=2_000_000, bytes_per_point=100)
+    srv = Server(ex, max_slots=64, round_pairs=1e5, memory_reserve=500_000)
+    ts = [srv.submit(req(5000)) for _ in range(8)]  # 500 kB each
+    srv.run_until_idle()
+    assert all(t.done() for t in ts)
+    # an admission next to live slices never pushed free memory below the reserve (an idle device
+    # admits the head request regardless, so that a request larger than the reserve still runs)
+    assert all(free >= 500_000 for before, free in ex.admissions if before > 0)
+    assert ex.max_live == 3
+
+
+def test_every_active_slice_progresses_each_round():
+    ex = FakeExecutor()
+    srv = Server(ex, max_slots=8, round_pairs=1.0, min_units=2, memory_reserve=0)  # budget ~ nothing extra
+    for n in [4000, 6000, 8000]:
+        srv.submit(req(n))
+    srv.run_until_idle()
+    # while all three were active, each round advanced each of them by >= 2 units (or to its end)
+    first = ex.rounds[0]
+    assert len(first) == 3
+    for h, b, e in first:
+        assert e - b == min(2, h.tile_pairs)
+
+
+def test_short_request_overtakes_long_one():
+    ex = FakeExecutor()
+    srv = Server(ex, max_slots=8, round_pairs=2e6, memory_reserve=0)
+    big = srv.submit(req(60000))
+    small = srv.submit(req(500))
+    srv.run_until_idle()
+    assert small.rounds == 1
+    assert big.rounds > 1
+    assert small.t_done <= big.t_done
+
+
+def test_invalid_request_fails_alone():
+    ex = FakeExecutor(fail_n=777)
+    srv = Server(ex, max_slots=4, round_pairs=1e6, memory_reserve=0)
+    good = srv.submit(req(1000))
+    bad = srv.submit(req(777))
+    also = srv.submit(req(2000))
+    srv.run_until_idle()
+    with pytest.raises(ValueError):
+        bad.wait(0)
+    assert good.wait(0)[1][0] == 1000
+    assert also.wait(0)[1][0] == 2000
+
+
+def test_threaded_arrivals_complete():
+    ex = FakeExecutor()
+    srv = Server(ex, max_slots=5, round_pairs=3e5, memory_reserve=0).start()
+    rng = np.random.default_rng(4)
+    sizes = rng.integers(2, 9000, 60)
+    tickets = []
+
+    def feeder():
+        for n in sizes:
+            tickets.append(srv.submit(req(int(n))))
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    th.join()
+    srv.stop()
+    assert len(tickets) == len(sizes)
+    for t, n in zip(tickets, sizes):
+        sums, counts = t.wait(5)
+        assert int(counts[0]) == n and np.all(sums == 1.0)
+        assert t.latency >= 0

@@ -1,0 +1,106 @@
+"""Batched serving on the GPU: every request's result is the same alone and in the mix.
+
+A mix of requests (2D / 3D planar, spherical, 1D and joint histograms, several sizes) goes through
+the continuous-batching loop at once; each result is compared with the same request run alone
+(sfb200_run through its plan) and with the CPU oracle: counts identical, sums within the mixed
+tolerance of the oracle's per-bin sum |v|.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle_py
+import sfb200 as SF
+from helpers import TOL_MIXED, compare
+from sfb200 import _lib, synthetic
+from sfb200.api import plan_description
+from sfb200.serving import GpuExecutor, Request, Server
+
+pytestmark = pytest.mark.gpu
+
+
+def make_requests(seed=21, count=18):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(count):
+        n = int(rng.integers(300, 3500))
+        kind = k % 3
+        joint = k % 2 == 1
+        ops = (SF.L2SF,) if rng.random() < 0.5 else (SF.L3SF,)
+        nb = int(rng.integers(24, 40))
+        if kind == 0:
+            x = rng.random((2, n))
+            u = synthetic.planar_field(x, 32, 64.0, rng, 0.01)
+            edges, metric = synthetic.log_edges(1e-3, math.sqrt(2.0), nb), None
+        elif kind == 1:
+            x = rng.random((3, n))
+            u = synthetic.solenoidal_field(x, 64, 128.0, rng)
+            edges, metric = synthetic.log_edges(1e-4, math.sqrt(3.0), nb), None
+        else:
+            x = synthetic.sphere_points(n, rng).astype(np.float32)
+            u = synthetic.sphere_field(x.astype(np.float64), 48, 200, rng).astype(np.float32)
+            edges, metric = synthetic.log_edges(1.0, 20000.0, nb), SF.Haversine(6371.0)
+        vb = None
+        if joint:
+            ops = (SF.ProjectedStructureFunctionType(1, 0),)
+            sigma = math.sqrt(2.0) * float(np.std(u.astype(np.float64)))
+            vb = SF.LinearBinEdges(-5.0 * sigma, 5.0 * sigma, 65)
+        reqs.append(Request(ops, x, u, edges, vb, metric, tag=k))
+    return reqs
+
+
+def oracle_of(r):
+    desc, keep = plan_description(r.ops, r.u.shape[0], r.distance_bins, r.value_bins, r.metric, "fp64",
+                                  r.x.dtype, r.u.dtype)
+    return oracle_py.run(desc, r.x, r.u, with_abs=True)
+
+
+def test_results_same_alone_and_in_the_mix():
+    reqs = make_requests()
+    ex = GpuExecutor(0)
+    try:
+        srv = Server(ex, max_slots=12, round_pairs=2e6).start()  # small rounds: many interleavings
+        tickets = [srv.submit(r) for r in reqs]
+        srv.stop()
+        assert srv.rounds > 1
+        for r, t in zip(reqs, tickets):
+            mix_s, mix_c = t.wait(60)
+            # alone: the same plan through sfb200_run
+            desc, keep = plan_description(r.ops, r.u.shape[0], r.distance_bins, r.value_bins, r.metric, "mixed",
+                                          r.x.dtype, r.u.dtype)
+            plan = _lib.Plan(ex.ctx, desc, keep)
+            s = np.zeros(plan.n_sums)
+            c = np.zeros(plan.n_counts, dtype=np.uint64)
+            xa, ua = np.asfortranarray(r.x), np.asfortranarray(r.u)
+            plan.run(xa.ctypes.data, ua.ctypes.data, r.n, 0, s.ctypes.data, c.ctypes.data)
+            plan.close()
+            assert np.array_equal(mix_c, c), f"request {r.tag}: counts differ between the mix and alone"
+            rs, rc, ra = oracle_of(r)
+            if r.value_bins is None:
+                compare(mix_s, mix_c, rs, rc, ra, TOL_MIXED)
+                compare(s, c, rs, rc, ra, TOL_MIXED)
+            else:
+                compare(mix_s, mix_c, rs, rc, ra, TOL_MIXED)
+                compare(s, c, rs, rc, ra, TOL_MIXED)
+            # alone vs mix: only the summation order differs
+            scale = np.maximum(ra, 1e-300)
+            assert float(np.max(np.abs(mix_s - s) / scale)) <= 2 * TOL_MIXED
+    finally:
+        ex.close()
+
+
+def test_round_graph_replay_and_ranges_split_across_rounds():
+    """One request split into many rounds gives the single-launch result (tile-pair coverage)."""
+    r = make_requests(seed=5, count=1)[0]
+    ex = GpuExecutor(0)
+    try:
+        srv = Server(ex, max_slots=4, round_pairs=1.0, min_units=1)  # one tile pair per round
+        t = srv.submit(r)
+        srv.run_until_idle()
+        s, c = t.wait(60)
+        assert t.rounds == srv.rounds and t.rounds > 3
+        rs, rc, ra = oracle_of(r)
+        compare(s, c, rs, rc, ra, TOL_MIXED)
+    finally:
+        ex.close()
