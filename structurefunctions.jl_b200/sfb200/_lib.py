@@ -6,6 +6,7 @@ is no CPU fallback: if the library or a CUDA device is missing, every entry poin
 import ctypes as C
 import os
 import threading
+import weakref
 
 from . import _abi
 from .errors import ArgumentError, DeviceError, DimensionMismatch
@@ -90,7 +91,12 @@ def check(rc, ctx_ptr=None, what=""):
 
 
 class Context:
-    """A CUDA device context of the library (one stream, one workspace pool)."""
+    """A CUDA device context of the library (one stream, one workspace pool).
+
+    Plans and slices created on a context are released with it: closing the context first closes
+    its slices, then its plans, so that no later finaliser reaches a destroyed context (objects in a
+    reference cycle are finalised in no particular order).
+    """
 
     def __init__(self, device=0):
         lib = load()
@@ -101,13 +107,23 @@ class Context:
                               "(no CUDA device, or the device is unusable)")
         self.ptr = ptr
         self.device = int(device)
+        self._children = weakref.WeakSet()
 
     @property
     def stream(self):
         return load().sfb200_ctx_stream(self.ptr)
 
+    def _adopt(self, obj):
+        self._children.add(obj)
+
     def close(self):
         if self.ptr:
+            children = list(self._children)
+            for obj in children:
+                if isinstance(obj, Slice):
+                    obj.close()
+            for obj in children:
+                obj.close()
             load().sfb200_ctx_destroy(self.ptr)
             self.ptr = None
 
@@ -134,6 +150,7 @@ class Slice:
         check(load().sfb200_slice_create(plan.ptr, x_ptr, u_ptr, int(n), int(flags), stream, C.byref(ptr)),
               plan.ctx.ptr, "slice")
         self.ptr = ptr
+        plan.ctx._adopt(self)
         info = _abi.SliceInfo()
         check(load().sfb200_slice_get_info(ptr, C.byref(info)), plan.ctx.ptr)
         self.n_points, self.pairs = info.n_points, info.pairs
@@ -144,7 +161,8 @@ class Slice:
 
     def close(self):
         if self.ptr:
-            load().sfb200_slice_destroy(self.ptr)
+            if self.plan.ptr and self.plan.ctx.ptr:  # else released with its context
+                load().sfb200_slice_destroy(self.ptr)
             self.ptr = None
 
     def __del__(self):
@@ -185,6 +203,7 @@ class Plan:
         ptr = C.c_void_p()
         check(lib.sfb200_plan_create(ctx.ptr, C.byref(desc), C.byref(ptr)), ctx.ptr, "plan")
         self.ptr = ptr
+        ctx._adopt(self)
         ns, nc = C.c_int64(), C.c_int64()
         check(lib.sfb200_plan_output_sizes(ptr, C.byref(ns), C.byref(nc)), ctx.ptr)
         self.n_sums, self.n_counts = ns.value, nc.value
@@ -207,7 +226,8 @@ class Plan:
 
     def close(self):
         if self.ptr:
-            load().sfb200_plan_destroy(self.ptr)
+            if self.ctx.ptr:  # else released with its context
+                load().sfb200_plan_destroy(self.ptr)
             self.ptr = None
 
     def __del__(self):
