@@ -257,6 +257,22 @@ SFB200_API int sfb200_batch_query(sfb200_ctx* ctx, int32_t* done);
 /* Free and total device memory of the context's device (cudaMemGetInfo), for admission control. */
 SFB200_API int sfb200_device_memory(sfb200_ctx* ctx, int64_t* free_bytes, int64_t* total_bytes);
 
+/* ------------------------------------------------------------------------------ no allocation
+ * sfb200_run over device inputs and device outputs that allocates no device memory: for callers that
+ * must not allocate while they run -- a loop that reserved its whole device budget up front, or a
+ * process sharing the device, where an allocation could fail under memory pressure or make the device
+ * wait. No counterpart in the reference. Scratch is one fixed array per device inside the library
+ * (3.4 MiB, held by every device that loads the library until the process exits): flat (Euclidean)
+ * 1D plans of precision MIXED or FP64 only, at most 65536 points, at most 32768 sums (bins x
+ * operators) and 4096 bins; larger calls return SFB200_ERR_UNSUPPORTED. Points are taken in the
+ * caller's order. x, u, sums and counts are device pointers; flags may only hold
+ * SFB200_RUN_ACCUMULATE. The first call on a device looks up the scratch array's device address (and
+ * loads the kernels it uses), so make that first call before any stream capture. All calls on one
+ * device share the scratch: calls that overlap on the GPU (from several streams or threads) race on
+ * it and must be serialised by the caller. */
+SFB200_API int sfb200_run_noalloc(sfb200_plan* plan, const void* x, const void* u, int64_t n, uint32_t flags,
+                                  double* sums, uint64_t* counts, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

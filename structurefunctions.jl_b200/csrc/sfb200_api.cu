@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -1530,5 +1531,106 @@ extern "C" int sfb200_batch_query(sfb200_ctx* ctx, int32_t* done)
     }
     CK(e);
     ctx->round_pending = false;
+    return SFB200_OK;
+}
+
+// ------------------------------------------------------------------------------- no allocation
+//
+// sfb200_run_noalloc: the mixed / FP64 flat 1D run without any device allocation, for callers that
+// must not allocate device memory while they run -- a loop that reserved its whole device budget up
+// front, or a process sharing the device where an allocation could fail under memory pressure or
+// make the device wait (cudaMalloc / cudaFree may synchronise it). Its scratch (packed points and the
+// accumulators) is one file-scope device array of fixed size, so at most kNoAllocMaxPoints points and
+// kNoAllocMaxSums / kNoAllocMaxCounts histogram entries fit. Every call zeroes the accumulators it
+// uses; the packed points are overwritten. All calls on a device share the one array: calls whose work
+// overlaps on the GPU (different streams or host threads) race on it, so callers serialise them.
+
+static constexpr long long kNoAllocMaxPoints = 1ll << 16;          // points per call
+static constexpr long long kNoAllocMaxSums = 32768;                // nb x n_ops doubles
+static constexpr long long kNoAllocMaxCounts = 4096;               // nb counts
+static constexpr long long kNoAllocWords =                         // 8-byte words of scratch
+    2 * 3 * kNoAllocMaxPoints + kNoAllocMaxSums + kNoAllocMaxCounts + 8;
+
+// 3.4 MiB, held by every device that loads the library: X64 (D x N), U64 (D x N), sums, counts, aux
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
+
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_ptr[64] = {};  // per device, looked up once with that device current
+
+// Device address of the scratch array on ctx's device (which the caller has made current). The
+// first call on a device looks it up; later calls reuse it. Host code only ever passes this address
+// to kernels: the array's name on the host is a host-side stand-in, not a device address.
+static int noalloc_scratch(sfb200_ctx* ctx, void** out)
+{
+    if (ctx->device < 0 || ctx->device >= 64) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[ctx->device]) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) return cuda_fail(ctx, e, "scratch address");
+        g_noalloc_ptr[ctx->device] = ptr;
+    }
+    *out = g_noalloc_ptr[ctx->device];
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_run_noalloc(sfb200_plan* p, const void* x, const void* u, int64_t n, uint32_t flags,
+                                  double* sums, uint64_t* counts, void* stream)
+{
+    if (!p) return SFB200_ERR_INVALID_ARG;
+    sfb200_ctx* ctx = p->ctx;
+    if (p->sphere || p->joint || p->mixed)
+        return set_err(ctx, SFB200_ERR_UNSUPPORTED, "sfb200_run_noalloc takes flat 1D plans of precision MIXED or FP64");
+    if (flags & ~SFB200_RUN_ACCUMULATE)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "sfb200_run_noalloc: inputs and outputs are device pointers; "
+                                                    "only SFB200_RUN_ACCUMULATE may be set");
+    if (n < 0) return set_err(ctx, SFB200_ERR_INVALID_ARG, "negative point count");
+    if (n > kNoAllocMaxPoints)
+        return set_err(ctx, SFB200_ERR_UNSUPPORTED, "sfb200_run_noalloc: %lld points exceed its fixed scratch of %lld",
+                       (long long)n, kNoAllocMaxPoints);
+    if (p->n_sums > kNoAllocMaxSums || p->n_counts > kNoAllocMaxCounts)
+        return set_err(ctx, SFB200_ERR_UNSUPPORTED,
+                       "sfb200_run_noalloc: %lld sums / %lld counts exceed its fixed scratch of %lld / %lld",
+                       p->n_sums, p->n_counts, kNoAllocMaxSums, kNoAllocMaxCounts);
+    if (!sums || !counts) return set_err(ctx, SFB200_ERR_INVALID_ARG, "sums/counts pointer is NULL");
+    if (n > 0 && (!x || !u)) return set_err(ctx, SFB200_ERR_INVALID_ARG, "x/u pointer is NULL");
+    CK(cudaSetDevice(ctx->device));
+    void* base = nullptr;
+    int rc = noalloc_scratch(ctx, &base);
+    if (rc) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    // a workspace view of the scratch: X64 | U64 | sums | counts | aux
+    unsigned long long* words = static_cast<unsigned long long*>(base);
+    const long long D = p->D;
+    Workspace w;
+    w.cap = n;
+    w.d_X64 = reinterpret_cast<double*>(words);
+    w.d_U64 = reinterpret_cast<double*>(words + D * std::max<long long>(n, 1));
+    w.d_sums = reinterpret_cast<double*>(words + 2 * 3 * kNoAllocMaxPoints);
+    w.d_counts = words + 2 * 3 * kNoAllocMaxPoints + kNoAllocMaxSums;
+    w.d_aux = words + 2 * 3 * kNoAllocMaxPoints + kNoAllocMaxSums + kNoAllocMaxCounts;
+    // the array keeps the previous call's contents: the accumulators must start at zero
+    CK(cudaMemsetAsync(w.d_sums, 0, sizeof(double) * p->n_sums, s));
+    CK(cudaMemsetAsync(w.d_counts, 0, sizeof(unsigned long long) * p->n_counts, s));
+    CK(cudaMemsetAsync(w.d_aux, 0, sizeof(unsigned long long) * 4, s));
+    if (n >= 2) {
+        // caller's point order (no sort buffers); inputs read from the caller's device arrays
+        const bool x64 = p->desc.x_dtype == SFB200_F64, u64 = p->desc.u_dtype == SFB200_F64;
+        if (x64 && u64) launch_pack<double, double>(p, w, x, u, (int)n, nullptr, s);
+        else if (x64) launch_pack<double, float>(p, w, x, u, (int)n, nullptr, s);
+        else if (u64) launch_pack<float, double>(p, w, x, u, (int)n, nullptr, s);
+        else launch_pack<float, float>(p, w, x, u, (int)n, nullptr, s);
+        CK(cudaGetLastError());
+        LaunchCfg cfg;
+        rc = configure(p, w, n, false, &cfg);
+        if (rc) return rc;
+        const long long grid = std::min(cfg.grid, cfg.ntp);
+        void* args[] = {&cfg.a};
+        CK(cudaLaunchKernel(cfg.kc.fn, dim3((unsigned)grid), dim3(cfg.threads), args, cfg.smem, s));
+    }
+    const long long m = std::max(p->n_sums, p->n_counts);
+    k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(w.d_sums, w.d_counts, p->n_sums, p->n_counts, sums,
+                                                         (unsigned long long*)counts, flags & SFB200_RUN_ACCUMULATE);
+    CK(cudaGetLastError());
     return SFB200_OK;
 }

@@ -68,6 +68,8 @@ def load():
         lib.sfb200_batch_wait.restype = C.c_int
         lib.sfb200_batch_query.argtypes = [P, C.POINTER(C.c_int32)]
         lib.sfb200_batch_query.restype = C.c_int
+        lib.sfb200_run_noalloc.argtypes = [P, P, P, C.c_int64, C.c_uint32, P, P, P]
+        lib.sfb200_run_noalloc.restype = C.c_int
         if lib.sfb200_abi_version() != _abi.ABI_VERSION:
             raise OSError(f"libsfb200.so ABI {lib.sfb200_abi_version()} != {_abi.ABI_VERSION}")
         _lib = lib
