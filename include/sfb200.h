@@ -208,7 +208,13 @@ typedef enum {
     SFB200_OPT_POINT_ORDER = 1,
     /* Columns of the run-length histogram table (privatization 3): 0 automatic, else 1, 2, 4, 8,
      * 16 or 32. */
-    SFB200_OPT_HIST_COLUMNS = 2
+    SFB200_OPT_HIST_COLUMNS = 2,
+    /* Multi-GPU sharding of sfb200_run: value = (count << 32) | index; the run then covers only
+     * shard `index` of `count` equal contiguous ranges of the upper-triangle tile pairs (its outputs
+     * hold that shard's partial histogram; the caller adds the shards, e.g. with one all-reduce).
+     * Default 1 << 32 (one shard: everything). The partition of the pair set into tile pairs is
+     * the reference's (i < j) pair set exactly, so the shard sums add up to the full histogram. */
+    SFB200_OPT_SHARD = 3
 } sfb200_option;
 
 /* Set a plan option (autotuning; no counterpart in the reference). */

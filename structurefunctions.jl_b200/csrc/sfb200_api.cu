@@ -108,6 +108,7 @@ struct sfb200_plan {
     double vqc = 1.0, vqc_inv = 1.0;  // mixed joint: coarse scale of the packed cells
     int vfine_lo = 1, nfine = 0;      // mixed joint: value bins with exact offsets
     int order_ovr = -1;   // -1 auto, 0 caller order, 1 Morton order
+    int shard_index = 0, shard_count = 1;  // sfb200_run covers shard shard_index of shard_count
     int cols_ovr = 0;     // run-length histogram columns (0 auto)
 };
 
@@ -723,6 +724,12 @@ extern "C" int sfb200_plan_set_option(sfb200_plan* p, int option, int64_t value)
         if (value < -1 || value > 2) return set_err(ctx, SFB200_ERR_INVALID_ARG, "point order must be -1, 0, 1 or 2");
         p->order_ovr = (int)value;
         return SFB200_OK;
+    case SFB200_OPT_SHARD:
+        if (value < 0 || (value & 0xffffffffll) >= (value >> 32) || (value >> 32) > 65536)
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "shard: index (low 32 bits) must be below the count (high 32 bits)");
+        p->shard_index = (int)(value & 0xffffffffll);
+        p->shard_count = (int)(value >> 32);
+        return SFB200_OK;
     case SFB200_OPT_HIST_COLUMNS:
         if (value < 0 || value > 32 || (value & (value - 1)))
             return set_err(ctx, SFB200_ERR_INVALID_ARG, "histogram columns must be 0 (auto) or a power of two <= 32");
@@ -1148,6 +1155,10 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     out->ntp = ntp;
     out->grid = (long long)ctx->nsm * occ;  // resident blocks; a single run launches min(grid, ntp)
     out->a = a;
+    // this plan's shard of the tile pairs (equal-size contiguous ranges; the batched form walks
+    // explicit item ranges instead)
+    out->a.tp_lo = batch ? 0 : ntp * p->shard_index / p->shard_count;
+    out->a.tp_hi = batch ? ntp : ntp * (p->shard_index + 1) / p->shard_count;
     return SFB200_OK;
 }
 
@@ -1174,12 +1185,14 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         LaunchCfg cfg;
         rc = configure(p, p->ws, n, false, &cfg);
         if (rc) return rc;
-        const long long grid = std::min(cfg.grid, cfg.ntp);
+        const long long grid = std::min(cfg.grid, cfg.a.tp_hi - cfg.a.tp_lo);
         void* args[] = {&cfg.a};
         CK(cudaEventRecord(ctx->ev0, s));
-        CK(cudaLaunchKernel(cfg.kc.fn, dim3((unsigned)grid), dim3(cfg.threads), args, cfg.smem, s));
+        if (grid > 0) {
+            CK(cudaLaunchKernel(cfg.kc.fn, dim3((unsigned)grid), dim3(cfg.threads), args, cfg.smem, s));
+            ++launches;
+        }
         CK(cudaEventRecord(ctx->ev1, s));
-        ++launches;
         CK(cudaGetLastError());
         p->stats.tile = cfg.T;
         p->stats.threads = cfg.threads;
@@ -1624,9 +1637,9 @@ extern "C" int sfb200_run_noalloc(sfb200_plan* p, const void* x, const void* u, 
         LaunchCfg cfg;
         rc = configure(p, w, n, false, &cfg);
         if (rc) return rc;
-        const long long grid = std::min(cfg.grid, cfg.ntp);
+        const long long grid = std::min(cfg.grid, cfg.a.tp_hi - cfg.a.tp_lo);
         void* args[] = {&cfg.a};
-        CK(cudaLaunchKernel(cfg.kc.fn, dim3((unsigned)grid), dim3(cfg.threads), args, cfg.smem, s));
+        if (grid > 0) CK(cudaLaunchKernel(cfg.kc.fn, dim3((unsigned)grid), dim3(cfg.threads), args, cfg.smem, s));
     }
     const long long m = std::max(p->n_sums, p->n_counts);
     k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(w.d_sums, w.d_counts, p->n_sums, p->n_counts, sums,

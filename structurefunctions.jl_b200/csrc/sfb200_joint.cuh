@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(512) k_joint_fp64(const PairArgs a)
         for (int k = threadIdx.x; k < ncell; k += T) { hs[k] = 0.0; hc[k] = 0u; }
     }
     int iter = 0;
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+    for (long long p = a.tp_lo + blockIdx.x; p < a.tp_hi; p += gridDim.x, ++iter) {
         if constexpr (SMEM) {
             if (iter && iter % a.flush_every == 0) {
                 __syncthreads();
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
     const float tmax = (float)(a.vlin.n - 1);
 
     int iter = 0;
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+    for (long long p = a.tp_lo + blockIdx.x; p < a.tp_hi; p += gridDim.x, ++iter) {
         if (iter && iter % a.flush_every == 0) {
             __syncthreads();
             joint_flush_mixed(a, hres, hc, ncell);

@@ -31,6 +31,8 @@ struct PairArgs {
     int n;             // points
     int ntiles;        // ceil(n / T)
     long long ntp;     // ntiles (ntiles + 1) / 2
+    long long tp_lo;   // this launch walks tile pairs [tp_lo, tp_hi) (a shard of [0, ntp))
+    long long tp_hi;
     const double* X64; // FP64 SoA positions / sphere basis
     const double* U64; // FP64 SoA velocities
     const float* XF;   // FP32 SoA (mixed)
@@ -167,7 +169,7 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
 
     int iter = 0;
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+    for (long long p = a.tp_lo + blockIdx.x; p < a.tp_hi; p += gridDim.x, ++iter) {
         hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
@@ -313,7 +315,7 @@ __global__ void __launch_bounds__(256) k_flat1d_mixed(const PairArgs a)
     unsigned long long my_recheck = 0;
 
     int iter = 0;
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+    for (long long p = a.tp_lo + blockIdx.x; p < a.tp_hi; p += gridDim.x, ++iter) {
         hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
@@ -465,7 +467,7 @@ __global__ void __launch_bounds__(256) k_sphere1d_fp64(const PairArgs a)
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
 
     int iter = 0;
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+    for (long long p = a.tp_lo + blockIdx.x; p < a.tp_hi; p += gridDim.x, ++iter) {
         hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;
@@ -567,7 +569,7 @@ __global__ void __launch_bounds__(256) k_sphere1d_mixed(const PairArgs a)
     unsigned long long my_recheck = 0;
 
     int iter = 0;
-    for (long long p = blockIdx.x; p < a.ntp; p += gridDim.x, ++iter) {
+    for (long long p = a.tp_lo + blockIdx.x; p < a.tp_hi; p += gridDim.x, ++iter) {
         hist.close_runs(lane);
         if (PRIV && iter && a.flush_every && iter % a.flush_every == 0) hist.fold();
         int ti, tj;

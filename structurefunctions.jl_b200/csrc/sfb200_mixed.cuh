@@ -261,7 +261,7 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
 template <int D, class OPS, int PRIV>
 __global__ void __launch_bounds__(256) k_flat1d_mx(const PairArgs a)
 {
-    flat1d_mx_run<D, OPS, PRIV>(a, blockIdx.x, a.ntp, gridDim.x);
+    flat1d_mx_run<D, OPS, PRIV>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.
@@ -465,7 +465,7 @@ __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0,
 template <int D, class OPS, int PRIV>
 __global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
 {
-    sphere1d_mx_run<D, OPS, PRIV>(a, blockIdx.x, a.ntp, gridDim.x);
+    sphere1d_mx_run<D, OPS, PRIV>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.
@@ -671,7 +671,7 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
 template <bool SPHERE, int D, class OPS>
 __global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
 {
-    joint_mx_run<SPHERE, D, OPS>(a, blockIdx.x, a.ntp, gridDim.x);
+    joint_mx_run<SPHERE, D, OPS>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.

@@ -130,3 +130,4 @@ EXPORTED_SYMBOLS = (
 # sfb200_option
 OPT_POINT_ORDER = 1
 OPT_HIST_COLUMNS = 2
+OPT_SHARD = 3

@@ -204,6 +204,23 @@ def test_joint_point_order(precision, tol):
         compare(gs, gc, rs, rc, ra, tol)
 
 
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+@pytest.mark.parametrize("count", [2, 3, 8])
+def test_tile_pair_shards_add_up(precision, tol, count):
+    """The shards of SFB200_OPT_SHARD (one per GPU in a multi-GPU run), run one after another and
+    added, give the oracle's histogram."""
+    for name, n in (("c1", 3000), ("c2", 2000), ("c3", 2500)):
+        w = synthetic.config(name, n=n)
+        tot_s, tot_c = None, None
+        for k in range(count):
+            gs, gc, st = run_gpu(w.ops, w.x, w.u, w.distance_bins.edges, metric=w.metric, value_bins=w.value_bins,
+                                 precision=precision, options={_abi.OPT_SHARD: (count << 32) | k})
+            tot_s = gs if tot_s is None else tot_s + gs
+            tot_c = gc if tot_c is None else tot_c + gc
+        rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges, metric=w.metric, value_bins=w.value_bins)
+        compare(tot_s, tot_c, rs, rc, ra, tol)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
 def test_tiny_and_empty(precision):
     be = SF.B200Backend(precision=precision)
