@@ -17,7 +17,7 @@ import weakref
 
 import numpy as np
 
-from . import _abi, _lib
+from . import _abi, _lib, autotune
 from .bins import AbstractBinEdges, as_bin_edges
 from .errors import ArgumentError, DimensionMismatch
 from .metrics import Euclidean, pair_geometry_for
@@ -50,15 +50,17 @@ class B200Backend:
     precision: "mixed" (FP64 differences, squared distance and projection numerators; FP32
     normalisation, powers and accumulation; FP64 merge), "fp64" (every pair in FP64) or "fp32"
     (FP32 bulk with an FP64 recheck of bin membership). Plans are cached per (operator set, bins,
-    metric, dtypes).
+    metric, dtypes). With `autotune=True` the first call of each plan shape and size class times the
+    launch candidates on its own inputs (sfb200.autotune) and keeps the fastest.
     """
 
-    def __init__(self, device=0, precision="mixed", tile=0):
+    def __init__(self, device=0, precision="mixed", tile=0, autotune=False):
         if precision not in _abi.PRECISIONS:
             raise ArgumentError("precision must be 'mixed', 'fp64' or 'fp32'")
         self.device = int(device)
         self.precision = precision
         self.tile = int(tile)
+        self.autotune = bool(autotune)
         self._plans = {}
 
     def __repr__(self):
@@ -261,6 +263,15 @@ def _run(backend, ops, x, u, distance_bins, value_bins, distance_metric):
     sums = np.zeros(plan.n_sums, dtype=np.float64)
     counts = np.zeros(plan.n_counts, dtype=np.uint64)
     flags = _abi.RUN_DEVICE_INPUT if xdev else 0
+    if backend.autotune and n >= 2:
+        skey = autotune.shape_key(desc, n)
+        if getattr(plan, "_tuned_key", None) != skey:
+            choice = autotune.lookup(skey)
+            if choice is not None:
+                autotune.apply(plan, choice)
+            else:
+                autotune.tune(plan, desc, lambda: plan.run(xp, up, n, flags, sums.ctypes.data, counts.ctypes.data), n)
+            plan._tuned_key = skey
     plan.run(xp, up, n, flags, sums.ctypes.data, counts.ctypes.data)
     return sums, counts, plan, xcode, ucode
 

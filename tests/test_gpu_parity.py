@@ -221,6 +221,25 @@ def test_tile_pair_shards_add_up(precision, tol, count):
         compare(tot_s, tot_c, rs, rc, ra, tol)
 
 
+def test_autotuned_backend_gives_the_oracle_histogram():
+    """B200Backend(autotune=True): the first call times the launch candidates, applies the fastest
+    (cached per shape), and the result still equals the oracle's."""
+    from sfb200 import autotune
+
+    autotune.clear()
+    be = SF.B200Backend(autotune=True)
+    for name, n in (("c1", 3000), ("c0", 4096)):
+        w = synthetic.config(name, n=n)
+        op = w.ops[0]
+        r = SF.calculate_structure_function(op, w.x, w.u, w.distance_bins.edges, backend=be,
+                                            output_type=SF.StructureFunctionSumsAndCounts)
+        desc, keep = plan_description((op,), w.u.shape[0], w.distance_bins.edges, None, None, "mixed", w.x.dtype,
+                                      w.u.dtype)
+        assert autotune.lookup(autotune.shape_key(desc, n)) is not None
+        rs, rc, ra = run_oracle((op,), w.x, w.u, w.distance_bins.edges)
+        compare(np.asarray(r.sums, dtype=np.float64), r.counts, rs, rc, ra, TOL_MIXED)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
 def test_tiny_and_empty(precision):
     be = SF.B200Backend(precision=precision)
