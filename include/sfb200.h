@@ -233,9 +233,15 @@ SFB200_API int sfb200_plan_set_option(sfb200_plan* plan, int option, int64_t val
  * group as one persistent launch whose blocks pull (slice, tile-pair range) items from a device
  * counter; the round is captured as a CUDA graph and replayed with updated parameters. Every tile
  * pair of a slice must be covered exactly once over the rounds; the result then equals sfb200_run's
- * (counts identical, sums up to summation order). Rounds on one context must not overlap: a round's
- * item list lives in a host buffer that the next call rewrites, so wait for the stream (or an event
- * recorded after the round) before the next sfb200_batch_run. */
+ * (counts identical, sums up to summation order). Rounds are double-buffered: the next round may be
+ * queued while one runs (the host prepares it meanwhile, and the device starts it as soon as the
+ * running one ends); queuing a third waits for the first. Rounds queued on the same stream run one
+ * after the other, so one slice may take part in consecutive rounds.
+ *
+ * Slice memory comes from a stream-ordered pool of the context: creating a slice allocates one block
+ * in order on its preparation stream, destroying it frees the block in order after its preparation,
+ * every round queued so far and its last read, without waiting on the host. Freed blocks stay in the
+ * pool for later slices; sfb200_device_memory counts them as free. */
 typedef struct sfb200_slice sfb200_slice;
 
 typedef struct {
@@ -254,13 +260,21 @@ SFB200_API int sfb200_slice_get_info(const sfb200_slice* slice, sfb200_slice_inf
 SFB200_API int sfb200_batch_run(sfb200_ctx* ctx, int32_t n, sfb200_slice* const* slices, const int64_t* tp_begin,
                                 const int64_t* tp_end, void* stream);
 /* Copy a slice's histogram out (host buffers: synchronous; SFB200_RUN_DEVICE_OUTPUT: queued on the
- * stream; SFB200_RUN_ACCUMULATE adds into the caller's buffers). */
+ * stream; SFB200_RUN_ACCUMULATE adds into the caller's buffers). The copy waits for the slice's
+ * preparation and for the last round that listed it, not for rounds queued after that one; a NULL
+ * stream means a side stream of the context that carries no rounds. Destroying a slice frees its
+ * memory in the same order. */
 SFB200_API int sfb200_slice_read(sfb200_slice* slice, double* sums, uint64_t* counts, uint32_t flags, void* stream);
 SFB200_API int sfb200_slice_destroy(sfb200_slice* slice);
-/* Wait for the last round of the context (blocking) / ask whether it has finished (*done = 0 or 1). */
+/* Wait for every queued round of the context (blocking) / ask whether all have finished (*done = 0
+ * or 1). */
 SFB200_API int sfb200_batch_wait(sfb200_ctx* ctx);
 SFB200_API int sfb200_batch_query(sfb200_ctx* ctx, int32_t* done);
-/* Free and total device memory of the context's device (cudaMemGetInfo), for admission control. */
+/* Wait for the oldest unfinished round only; *round (if not NULL) receives its number (rounds are
+ * numbered 1, 2, ... in the order sfb200_batch_run queued them; 0 if none was unfinished). */
+SFB200_API int sfb200_batch_wait_oldest(sfb200_ctx* ctx, int64_t* round);
+/* Free and total device memory of the context's device (cudaMemGetInfo, plus blocks the context's
+ * slice pool holds unused), for admission control. */
 SFB200_API int sfb200_device_memory(sfb200_ctx* ctx, int64_t* free_bytes, int64_t* total_bytes);
 
 /* ------------------------------------------------------------------------------ no allocation

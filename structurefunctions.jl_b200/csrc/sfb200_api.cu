@@ -28,22 +28,33 @@ struct sfb200_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
-    // batched rounds: work items (pinned host staging + device copy), launch counters, the graph
-    void* h_items = nullptr;
-    void* d_items = nullptr;
-    size_t items_cap = 0;       // WorkItem capacity of both buffers
-    unsigned* d_counters = nullptr;
-    int counters_cap = 0;
-    cudaGraphExec_t batch_exec = nullptr;
+    // batched rounds, double-buffered so that the next round can be enqueued while one runs: per
+    // buffer the work items (pinned host staging + device copy), launch counters, the graph and the
+    // event recorded after the round (the buffer is free again once it has fired)
+    static constexpr int kRoundBufs = 2;
+    struct RoundBuf {
+        void* h_items = nullptr;
+        void* d_items = nullptr;
+        size_t items_cap = 0;   // WorkItem capacity of both copies
+        unsigned* d_counters = nullptr;
+        int counters_cap = 0;
+        cudaGraphExec_t exec = nullptr;
+        cudaEvent_t done = nullptr;
+        bool pending = false;
+        unsigned long long seq = 0;  // round number of the last round enqueued from this buffer
+    } rb[kRoundBufs];
+    unsigned long long rounds_enqueued = 0;
     bool batch_graph = true;    // capture rounds as a graph (cleared if capture is refused)
-    cudaEvent_t round_done = nullptr;  // recorded after each round (the item buffer is free again)
-    bool round_pending = false;
+    // slice memory: a stream-ordered pool owned by the context (freed blocks stay reserved for the
+    // next slices instead of going back to the driver)
+    cudaMemPool_t pool = nullptr;
     // the kernels of one round run concurrently on these streams (fork / join through events)
     static constexpr int kLanes = 8;
     cudaStream_t lane[kLanes] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[kLanes] = {};
     cudaStream_t prep_stream = nullptr;  // slice preparation, overlapping the running round
+    cudaStream_t side_stream = nullptr;  // reads and frees of finished slices (not behind later rounds)
 };
 
 // Device buffers of one run over n <= cap points: raw inputs, the packed SoA layout, the point
@@ -67,6 +78,7 @@ struct Workspace {
     unsigned long long* d_counts = nullptr;
     unsigned long long* d_aux = nullptr;  // [0] rechecked pairs, [1] |x| bound, [2] |u| bound
     size_t bytes = 0;                     // device bytes held
+    void* block = nullptr;                // slices: every buffer above lies in this one pooled block
 };
 
 struct sfb200_plan {
@@ -177,17 +189,26 @@ extern "C" int sfb200_ctx_destroy(sfb200_ctx* ctx)
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->prep_stream) cudaStreamSynchronize(ctx->prep_stream);
-    if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
-    if (ctx->round_done) cudaEventDestroy(ctx->round_done);
+    for (auto& b : ctx->rb) {
+        if (b.done) cudaEventSynchronize(b.done);
+        if (b.exec) cudaGraphExecDestroy(b.exec);
+        if (b.done) cudaEventDestroy(b.done);
+        if (b.h_items) cudaFreeHost(b.h_items);
+        cudaFree(b.d_items);
+        cudaFree(b.d_counters);
+    }
     if (ctx->fork) cudaEventDestroy(ctx->fork);
     for (int k = 0; k < sfb200_ctx::kLanes; ++k) {
+        if (ctx->lane[k]) cudaStreamSynchronize(ctx->lane[k]);
         if (ctx->join[k]) cudaEventDestroy(ctx->join[k]);
         if (ctx->lane[k]) cudaStreamDestroy(ctx->lane[k]);
     }
     if (ctx->prep_stream) cudaStreamDestroy(ctx->prep_stream);
-    if (ctx->h_items) cudaFreeHost(ctx->h_items);
-    cudaFree(ctx->d_items);
-    cudaFree(ctx->d_counters);
+    if (ctx->side_stream) {
+        cudaStreamSynchronize(ctx->side_stream);
+        cudaStreamDestroy(ctx->side_stream);
+    }
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SFB200_OK;
@@ -397,8 +418,15 @@ static LinearParams linear_of(const sfb200_bins& b)
 }
 
 // Frees the input / layout buffers of a workspace (its histogram buffers with `outputs`).
-static void free_workspace(Workspace& w, bool outputs)
+// Releases the buffers of w (with `outputs`, the histogram too). A pooled slice block is freed in
+// order on stream s, after the work already enqueued there.
+static void free_workspace(Workspace& w, bool outputs, cudaStream_t s = nullptr)
 {
+    if (w.block) {
+        cudaFreeAsync(w.block, s);
+        w = Workspace{};
+        return;
+    }
     cudaFree(w.d_rawx); cudaFree(w.d_rawu);
     cudaFree(w.d_X64); cudaFree(w.d_U64); cudaFree(w.d_XF); cudaFree(w.d_UF); cudaFree(w.d_XM);
     cudaFree(w.d_keys); cudaFree(w.d_perm); cudaFree(w.d_box); cudaFree(w.d_sort_tmp);
@@ -742,20 +770,15 @@ extern "C" int sfb200_plan_set_option(sfb200_plan* p, int option, int64_t value)
 // ------------------------------------------------------------------------------- run
 
 // Grows the input / layout buffers of `w` to n points (its histogram buffers are sized by the plan).
-static int ensure_workspace(sfb200_plan* p, Workspace& w, long long n)
+// The buffers of a workspace over `cap` points (and, with `outputs`, the histogram), in order,
+// through alloc(&ptr, bytes). Shared by the per-buffer allocation of plans and the one pooled block
+// of a slice.
+template <class Alloc>
+static int workspace_layout(sfb200_plan* p, Workspace& w, long long cap, bool outputs, Alloc&& alloc)
 {
     sfb200_ctx* ctx = p->ctx;
-    if (n <= w.cap) return SFB200_OK;
-    if (w.cap) CK(cudaStreamSynchronize(ctx->stream));  // old buffers may still be in use
-    free_workspace(w, false);
-    const long long cap = std::max<long long>(n, 1024);
     const int nx64 = p->sphere ? 8 : p->D;
     const int nxf = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 2 * p->D : p->D);
-    size_t bytes = 0;
-    auto alloc = [&](void** ptr, size_t b) {
-        bytes += b;
-        return cudaMalloc(ptr, b);
-    };
     CK(alloc(&w.d_rawx, sizeof(double) * p->W * cap));
     CK(alloc(&w.d_rawu, sizeof(double) * p->D * cap));
     CK(alloc((void**)&w.d_X64, sizeof(double) * nx64 * cap));
@@ -768,23 +791,72 @@ static int ensure_workspace(sfb200_plan* p, Workspace& w, long long n)
     CK(alloc((void**)&w.d_keys, sizeof(unsigned) * 2 * cap));
     CK(alloc((void**)&w.d_perm, sizeof(int) * 2 * cap));
     CK(alloc((void**)&w.d_box, sizeof(unsigned) * 6));
-    size_t tmp = 0;
+    size_t tmp = 0;  // size query only: launches nothing
     CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, w.d_keys, w.d_keys + cap, w.d_perm, w.d_perm + cap,
                                        (int)cap, 0, 32, ctx->stream));
     CK(alloc(&w.d_sort_tmp, std::max<size_t>(tmp, 16)));
     w.sort_tmp_bytes = tmp;
+    if (outputs) {
+        CK(alloc((void**)&w.d_sums, sizeof(double) * std::max<long long>(p->n_sums, 1)));
+        CK(alloc((void**)&w.d_counts, sizeof(unsigned long long) * std::max<long long>(p->n_counts, 1)));
+        CK(alloc((void**)&w.d_aux, sizeof(unsigned long long) * 4));
+    }
+    return SFB200_OK;
+}
+
+// Grows the buffers of `w` (a plan's) to at least n points (contents are not kept).
+static int ensure_workspace(sfb200_plan* p, Workspace& w, long long n)
+{
+    sfb200_ctx* ctx = p->ctx;
+    if (n <= w.cap) return SFB200_OK;
+    if (w.cap) CK(cudaStreamSynchronize(ctx->stream));  // old buffers may still be in use
+    free_workspace(w, false);
+    const long long cap = std::max<long long>(n, 1024);
+    size_t bytes = 0;
+    const int rc = workspace_layout(p, w, cap, false, [&](void** ptr, size_t b) {
+        bytes += b;
+        return cudaMalloc(ptr, b);
+    });
+    if (rc) return rc;
     w.cap = cap;
     w.bytes = bytes + (size_t)(p->n_sums + p->n_counts + 4) * 8;
     return SFB200_OK;
 }
 
-// Allocates the histogram buffers of `w` for plan p.
-static int alloc_outputs(sfb200_plan* p, Workspace& w)
+// All buffers of a slice over n points as one block from the context's pool, allocated in order on
+// stream s (it may be used by work enqueued on s, or on streams that wait for s, from here on).
+static int slice_workspace(sfb200_plan* p, Workspace& w, long long n, cudaStream_t s)
 {
     sfb200_ctx* ctx = p->ctx;
-    CK(cudaMalloc(&w.d_sums, sizeof(double) * std::max<long long>(p->n_sums, 1)));
-    CK(cudaMalloc(&w.d_counts, sizeof(unsigned long long) * std::max<long long>(p->n_counts, 1)));
-    CK(cudaMalloc(&w.d_aux, sizeof(unsigned long long) * 4));
+    if (!ctx->pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ctx->device;
+        CK(cudaMemPoolCreate(&ctx->pool, &props));
+        unsigned long long keep = ~0ull;  // keep freed blocks for the next slices
+        CK(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    const long long cap = std::max<long long>(n, 2);
+    // first pass: offsets from 0 (256-byte aligned); second pass: the same offsets in the block
+    size_t off = 0;
+    Workspace probe;
+    int rc = workspace_layout(p, probe, cap, true, [&](void** ptr, size_t b) {
+        *ptr = reinterpret_cast<void*>(off + 256);  // non-null stand-in, never dereferenced
+        off += (b + 255) & ~(size_t)255;
+        return cudaSuccess;
+    });
+    if (rc) return rc;
+    CK(cudaMallocFromPoolAsync(&w.block, off, ctx->pool, s));
+    off = 0;
+    rc = workspace_layout(p, w, cap, true, [&](void** ptr, size_t b) {
+        *ptr = static_cast<char*>(w.block) + off;
+        off += (b + 255) & ~(size_t)255;
+        return cudaSuccess;
+    });
+    if (rc) return rc;
+    w.cap = cap;
+    w.bytes = off;
     return SFB200_OK;
 }
 
@@ -884,7 +956,8 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
     if (p->mx) {
         const int rec = p->sphere ? 10 : 2 * p->D;  // doubles per j record
         if (p->joint)
-            return (size_t)lut_bytes + (size_t)rec * T * 8 + ((size_t)p->nb * p->nv + (size_t)p->nb * p->nfine) * 8;
+            return (size_t)lut_bytes + (size_t)rec * T * 8 + ((size_t)p->nb * p->nv + (size_t)p->nb * p->nfine) * 8 +
+                   (size_t)p->nv * 12;  // + value-bin centres (FP64 and FP32)
         return (size_t)lut_bytes + (size_t)rec * T * 8 + hist_bytes(true, NV, priv, NW, NBP, lc);
     }
     if (p->joint) {
@@ -1257,7 +1330,28 @@ struct sfb200_slice {
     LaunchCfg cfg;
     long long n = 0;
     cudaEvent_t ready = nullptr;  // preparation finished (recorded on the preparation stream)
+    cudaEvent_t used = nullptr;   // recorded after the last read (on the reader's stream)
+    unsigned long long last_round = 0;  // number of the last round that listed this slice (0: none)
 };
+
+// Orders stream s after the last round that listed slice sl, if that round may still be running.
+// Only that round is waited for, not the rounds queued after it. (A round buffer's event is only
+// re-recorded once the round that used it before has completed, so a buffer that has moved on to a
+// later round, or is no longer pending, means the slice's round is done.)
+static int wait_slice_round(sfb200_ctx* ctx, const sfb200_slice* sl, cudaStream_t s)
+{
+    if (!sl->last_round) return SFB200_OK;
+    const auto& b = ctx->rb[(sl->last_round - 1) % sfb200_ctx::kRoundBufs];
+    if (b.pending && b.seq == sl->last_round) CK(cudaStreamWaitEvent(s, b.done, 0));
+    return SFB200_OK;
+}
+
+static int side_stream(sfb200_ctx* ctx, cudaStream_t* out)
+{
+    if (!ctx->side_stream) CK(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
+    *out = ctx->side_stream;
+    return SFB200_OK;
+}
 
 extern "C" int sfb200_slice_create(sfb200_plan* p, const void* x, const void* u, int64_t n, uint32_t flags,
                                    void* stream, sfb200_slice** out)
@@ -1277,8 +1371,7 @@ extern "C" int sfb200_slice_create(sfb200_plan* p, const void* x, const void* u,
     if (!sl) return SFB200_ERR_OOM;
     sl->plan = p;
     sl->n = n;
-    int rc = ensure_workspace(p, sl->w, std::max<long long>(n, 2));
-    if (!rc) rc = alloc_outputs(p, sl->w);
+    int rc = slice_workspace(p, sl->w, n, s);
     int launches = 0;
     if (!rc) rc = prepare_inputs(p, sl->w, x, u, n, flags, s, &launches);
     if (!rc && n >= 2) rc = configure(p, sl->w, n, true, &sl->cfg);
@@ -1291,7 +1384,7 @@ extern "C" int sfb200_slice_create(sfb200_plan* p, const void* x, const void* u,
     if (rc) {
         cudaStreamSynchronize(s);
         if (sl->ready) cudaEventDestroy(sl->ready);
-        free_workspace(sl->w, true);
+        free_workspace(sl->w, true, s);
         delete sl;
         return rc;
     }
@@ -1314,11 +1407,18 @@ extern "C" int sfb200_slice_destroy(sfb200_slice* sl)
 {
     if (!sl) return SFB200_ERR_INVALID_ARG;
     sfb200_ctx* ctx = sl->plan->ctx;
-    cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    if (ctx->prep_stream) cudaStreamSynchronize(ctx->prep_stream);
+    CK(cudaSetDevice(ctx->device));
+    // free in stream order after the preparation, the slice's last round and its last read; the host
+    // does not wait
+    cudaStream_t s = nullptr;
+    int rc = side_stream(ctx, &s);
+    if (rc) return rc;
+    if (sl->ready) CK(cudaStreamWaitEvent(s, sl->ready, 0));
+    if ((rc = wait_slice_round(ctx, sl, s))) return rc;
+    if (sl->used) CK(cudaStreamWaitEvent(s, sl->used, 0));
+    free_workspace(sl->w, true, s);
     if (sl->ready) cudaEventDestroy(sl->ready);
-    free_workspace(sl->w, true);
+    if (sl->used) cudaEventDestroy(sl->used);
     delete sl;
     return SFB200_OK;
 }
@@ -1329,6 +1429,12 @@ extern "C" int sfb200_device_memory(sfb200_ctx* ctx, int64_t* free_bytes, int64_
     CK(cudaSetDevice(ctx->device));
     size_t f = 0, t = 0;
     CK(cudaMemGetInfo(&f, &t));
+    if (ctx->pool) {  // blocks the context's pool holds but no slice uses are free for slices
+        unsigned long long reserved = 0, used = 0;
+        CK(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+        CK(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used));
+        if (reserved > used) f += (size_t)(reserved - used);
+    }
     *free_bytes = (int64_t)f;
     *total_bytes = (int64_t)t;
     return SFB200_OK;
@@ -1340,19 +1446,31 @@ extern "C" int sfb200_slice_read(sfb200_slice* sl, double* sums, uint64_t* count
     sfb200_plan* p = sl->plan;
     sfb200_ctx* ctx = p->ctx;
     CK(cudaSetDevice(ctx->device));
-    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!s) {
+        const int rc = side_stream(ctx, &s);
+        if (rc) return rc;
+    }
     const bool accumulate = flags & SFB200_RUN_ACCUMULATE;
+    CK(cudaStreamWaitEvent(s, sl->ready, 0));  // a slice with no tile pairs is read without a round
+    {
+        const int rc = wait_slice_round(ctx, sl, s);
+        if (rc) return rc;
+    }
+    if (!sl->used) CK(cudaEventCreateWithFlags(&sl->used, cudaEventDisableTiming));
     if (flags & SFB200_RUN_DEVICE_OUTPUT) {
         const long long m = std::max(p->n_sums, p->n_counts);
         k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(sl->w.d_sums, sl->w.d_counts, p->n_sums, p->n_counts,
                                                              sums, (unsigned long long*)counts, accumulate);
         CK(cudaGetLastError());
+        CK(cudaEventRecord(sl->used, s));
         return SFB200_OK;
     }
     std::vector<double> hs(p->n_sums);
     std::vector<unsigned long long> hc(p->n_counts);
     CK(cudaMemcpyAsync(hs.data(), sl->w.d_sums, sizeof(double) * p->n_sums, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(hc.data(), sl->w.d_counts, sizeof(unsigned long long) * p->n_counts, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(sl->used, s));
     CK(cudaStreamSynchronize(s));
     for (long long k = 0; k < p->n_sums; ++k) sums[k] = (accumulate ? sums[k] : 0.0) + hs[k];
     for (long long k = 0; k < p->n_counts; ++k) counts[k] = (accumulate ? counts[k] : 0ull) + hc[k];
@@ -1415,46 +1533,47 @@ extern "C" int sfb200_batch_run(sfb200_ctx* ctx, int32_t n, sfb200_slice* const*
         L.nitems = items.size() - L.item0;
     }
     if (launches.empty()) return SFB200_OK;
-    // the previous round must have consumed the item buffer; the slices must be prepared
-    if (!ctx->round_done) {
-        CK(cudaEventCreateWithFlags(&ctx->round_done, cudaEventDisableTiming));
+    // lanes and events on first use; this round's buffer must have been consumed by the round that
+    // used it before (two rounds back); the slices must be prepared
+    if (!ctx->fork) {
         CK(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
         for (int k = 0; k < sfb200_ctx::kLanes; ++k) {
             CK(cudaStreamCreateWithFlags(&ctx->lane[k], cudaStreamNonBlocking));
             CK(cudaEventCreateWithFlags(&ctx->join[k], cudaEventDisableTiming));
         }
+        for (auto& b : ctx->rb) CK(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
     }
-    if (ctx->round_pending) CK(cudaEventSynchronize(ctx->round_done));
+    sfb200_ctx::RoundBuf& B = ctx->rb[ctx->rounds_enqueued % sfb200_ctx::kRoundBufs];
+    if (B.pending) CK(cudaEventSynchronize(B.done));
+    B.pending = false;
     for (int k = 0; k < n; ++k) CK(cudaStreamWaitEvent(s, slices[k]->ready, 0));
     // buffers (before any capture)
-    if (items.size() > ctx->items_cap) {
-        CK(cudaStreamSynchronize(s));
-        if (ctx->h_items) cudaFreeHost(ctx->h_items);
-        cudaFree(ctx->d_items);
-        ctx->h_items = nullptr;
-        ctx->d_items = nullptr;
-        ctx->items_cap = 0;
+    if (items.size() > B.items_cap) {
+        if (B.h_items) cudaFreeHost(B.h_items);
+        cudaFree(B.d_items);
+        B.h_items = nullptr;
+        B.d_items = nullptr;
+        B.items_cap = 0;
         const size_t cap = std::max<size_t>(items.size() * 2, 4096);
-        CK(cudaMallocHost(&ctx->h_items, cap * sizeof(WorkItem)));
-        CK(cudaMalloc(&ctx->d_items, cap * sizeof(WorkItem)));
-        ctx->items_cap = cap;
+        CK(cudaMallocHost(&B.h_items, cap * sizeof(WorkItem)));
+        CK(cudaMalloc(&B.d_items, cap * sizeof(WorkItem)));
+        B.items_cap = cap;
     }
-    if ((int)launches.size() > ctx->counters_cap) {
-        CK(cudaStreamSynchronize(s));
-        cudaFree(ctx->d_counters);
-        ctx->d_counters = nullptr;
+    if ((int)launches.size() > B.counters_cap) {
+        cudaFree(B.d_counters);
+        B.d_counters = nullptr;
         const int cap = std::max<int>((int)launches.size() * 2, 64);
-        CK(cudaMalloc(&ctx->d_counters, cap * sizeof(unsigned)));
-        ctx->counters_cap = cap;
+        CK(cudaMalloc(&B.d_counters, cap * sizeof(unsigned)));
+        B.counters_cap = cap;
     }
-    std::memcpy(ctx->h_items, items.data(), items.size() * sizeof(WorkItem));
-    const WorkItem* d_items = static_cast<const WorkItem*>(ctx->d_items);
+    std::memcpy(B.h_items, items.data(), items.size() * sizeof(WorkItem));
+    const WorkItem* d_items = static_cast<const WorkItem*>(B.d_items);
     for (size_t l = 0; l < launches.size(); ++l) {
         Launch& L = launches[l];
         CK(cudaFuncSetAttribute(L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
         L.args.items = d_items + L.item0;
         L.args.n_items = (int)L.nitems;
-        L.args.counter = ctx->d_counters + l;
+        L.args.counter = B.d_counters + l;
     }
     // grids (before any capture): at most the resident blocks, at most one block per item
     std::vector<long long> grids(launches.size());
@@ -1467,9 +1586,9 @@ extern "C" int sfb200_batch_run(sfb200_ctx* ctx, int32_t n, sfb200_slice* const*
     // concurrently and share the SMs), joined back into s
     const int nlanes = (int)std::min<size_t>(launches.size(), sfb200_ctx::kLanes);
     auto enqueue = [&]() -> cudaError_t {
-        cudaError_t e = cudaMemcpyAsync(ctx->d_items, ctx->h_items, items.size() * sizeof(WorkItem),
+        cudaError_t e = cudaMemcpyAsync(B.d_items, B.h_items, items.size() * sizeof(WorkItem),
                                         cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_counters, 0, launches.size() * sizeof(unsigned), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(B.d_counters, 0, launches.size() * sizeof(unsigned), s);
         if (e == cudaSuccess) e = cudaEventRecord(ctx->fork, s);
         for (int k = 0; k < nlanes && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(ctx->lane[k], ctx->fork, 0);
         for (size_t l = 0; l < launches.size() && e == cudaSuccess; ++l) {
@@ -1484,6 +1603,14 @@ extern "C" int sfb200_batch_run(sfb200_ctx* ctx, int32_t n, sfb200_slice* const*
         }
         return e;
     };
+    auto finish = [&]() -> int {
+        CK(cudaEventRecord(B.done, s));
+        B.pending = true;
+        B.seq = ++ctx->rounds_enqueued;
+        for (int k = 0; k < n; ++k)
+            if (tp_end[k] > tp_begin[k]) slices[k]->last_round = B.seq;
+        return SFB200_OK;
+    };
     if (ctx->batch_graph) {
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
@@ -1492,42 +1619,54 @@ extern "C" int sfb200_batch_run(sfb200_ctx* ctx, int32_t n, sfb200_slice* const*
             e = cudaStreamEndCapture(s, &graph);
             if (e1 != cudaSuccess) e = e1;
         }
-        if (e == cudaSuccess && ctx->batch_exec) {
+        if (e == cudaSuccess && B.exec) {
             cudaGraphExecUpdateResultInfo info;
-            if (cudaGraphExecUpdate(ctx->batch_exec, graph, &info) != cudaSuccess) {
+            if (cudaGraphExecUpdate(B.exec, graph, &info) != cudaSuccess) {
                 cudaGetLastError();
-                cudaGraphExecDestroy(ctx->batch_exec);
-                ctx->batch_exec = nullptr;
+                cudaGraphExecDestroy(B.exec);
+                B.exec = nullptr;
             }
         }
-        if (e == cudaSuccess && !ctx->batch_exec) e = cudaGraphInstantiate(&ctx->batch_exec, graph, 0);
-        if (e == cudaSuccess) e = cudaGraphLaunch(ctx->batch_exec, s);
+        if (e == cudaSuccess && !B.exec) e = cudaGraphInstantiate(&B.exec, graph, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(B.exec, s);
         if (graph) cudaGraphDestroy(graph);
-        if (e == cudaSuccess) {
-            CK(cudaEventRecord(ctx->round_done, s));
-            ctx->round_pending = true;
-            return SFB200_OK;
-        }
+        if (e == cudaSuccess) return finish();
         // capture or replay refused: run this and later rounds with plain launches
         cudaGetLastError();
         ctx->batch_graph = false;
-        if (ctx->batch_exec) {
-            cudaGraphExecDestroy(ctx->batch_exec);
-            ctx->batch_exec = nullptr;
+        for (auto& b : ctx->rb)
+            if (b.exec && &b != &B) CK(cudaEventSynchronize(b.done));
+        for (auto& b : ctx->rb) {
+            if (b.exec) cudaGraphExecDestroy(b.exec);
+            b.exec = nullptr;
         }
     }
     CK(enqueue());
-    CK(cudaEventRecord(ctx->round_done, s));
-    ctx->round_pending = true;
-    return SFB200_OK;
+    return finish();
 }
 
 extern "C" int sfb200_batch_wait(sfb200_ctx* ctx)
 {
     if (!ctx) return SFB200_ERR_INVALID_ARG;
     CK(cudaSetDevice(ctx->device));
-    if (ctx->round_pending) CK(cudaEventSynchronize(ctx->round_done));
-    ctx->round_pending = false;
+    for (auto& b : ctx->rb) {
+        if (b.pending) CK(cudaEventSynchronize(b.done));
+        b.pending = false;
+    }
+    return SFB200_OK;
+}
+
+extern "C" int sfb200_batch_wait_oldest(sfb200_ctx* ctx, int64_t* round)
+{
+    if (!ctx) return SFB200_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    sfb200_ctx::RoundBuf* oldest = nullptr;
+    for (auto& b : ctx->rb)
+        if (b.pending && (!oldest || b.seq < oldest->seq)) oldest = &b;
+    if (round) *round = oldest ? (int64_t)oldest->seq : 0;
+    if (!oldest) return SFB200_OK;
+    CK(cudaEventSynchronize(oldest->done));
+    oldest->pending = false;
     return SFB200_OK;
 }
 
@@ -1536,14 +1675,16 @@ extern "C" int sfb200_batch_query(sfb200_ctx* ctx, int32_t* done)
     if (!ctx || !done) return SFB200_ERR_INVALID_ARG;
     CK(cudaSetDevice(ctx->device));
     *done = 1;
-    if (!ctx->round_pending) return SFB200_OK;
-    const cudaError_t e = cudaEventQuery(ctx->round_done);
-    if (e == cudaErrorNotReady) {
-        *done = 0;
-        return SFB200_OK;
+    for (auto& b : ctx->rb) {
+        if (!b.pending) continue;
+        const cudaError_t e = cudaEventQuery(b.done);
+        if (e == cudaErrorNotReady) {
+            *done = 0;
+            continue;
+        }
+        CK(e);
+        b.pending = false;
     }
-    CK(e);
-    ctx->round_pending = false;
     return SFB200_OK;
 }
 

@@ -79,6 +79,14 @@ __device__ __forceinline__ void op_unscale(OpList<K...>, const GenOps& g, int ku
 
 __device__ __forceinline__ bool f32_range_ok(float v) { return v >= 0x1p-100f && v <= 0x1p100f; }
 
+// A finite FP32 number that is zero or normal (not subnormal, infinite or NaN). Written out with
+// comparisons: the C library's isnormal has no device implementation.
+__device__ __forceinline__ bool f32_zero_or_normal(float v)
+{
+    const float m = fabsf(v);
+    return m == 0.f || (m >= 0x1p-126f && m <= 0x1.fffffep127f);
+}
+
 // Approximate reciprocal square root (rsqrt.approx) for arguments known to be normal: no
 // denormal handling is needed around it.
 __device__ __forceinline__ float rsqrt_normal(float x)
@@ -483,34 +491,60 @@ __global__ void __launch_bounds__(256, 3) k_sphere1d_mx_batch(const BatchArgs b)
 // (|t| + |first / step|) * vrel from an integer; closer pairs, sphere pairs in the chord ambiguity
 // band and every pair of a vector value axis are recomputed in FP64 with the reference formula.
 //
-// Cells are one 64-bit word each, updated with a single shared atomic per pair: the count in the
+// Cells are one 64-bit word each (two native 32-bit atomics per pair, see SplitWords): the count in the
 // top 20 bits and, below, the sum of the pair offsets from the value-bin centre in fixed point
 // (quantum 2^-21 of the largest half bin width or finer; the packed word decodes exactly while the
 // cell holds fewer than 2^20 pairs and the offset sum stays below 2^43 in magnitude, so blocks flush
 // at least every 2^20 - 1 pairs). That quantum is far below the 1e-6 tolerance for every value bin
 // whose values stay at least a half width away from zero; the bins closer to zero (where a value
 // can be tiny next to the quantum) keep their offsets in a separate 64-bit word at 2^-30.
+//
+// Offsets are taken from C_b, the value-bin centre rounded to FP32 in the scaled units of the FP32
+// value (per block in shared memory, with its exact FP64 image for the flush). In every coarse bin
+// the values lie within a half width of a centre at least three half widths from zero, so the FP32
+// subtraction v - C_b is exact (Sterbenz) and its fixed-point image is one FP32 multiply by a power
+// of two and one conversion; the FP64 route remains for rechecked pairs and the bins near zero.
 // ================================================================================================
-__device__ __forceinline__ void joint_flush_packed(const PairArgs& a, unsigned long long* hcell,
-                                                   unsigned long long* hfine, int ncell)
+// A 64-bit shared word kept as two 32-bit halves (lo[k], hi[k]) in separate arrays, so that every
+// update is a native 32-bit shared atomic (a 64-bit shared atomic add is a compare-and-swap loop on
+// this architecture) and neighbouring cells fall in different banks. The low add returns the old
+// half, so the carry it produced is known exactly and goes into the high add with the value's own
+// high half: the pair (hi, lo) always holds the exact 64-bit modular sum once the adds are done.
+struct SplitWords {
+    unsigned* lo;
+    unsigned* hi;
+    __device__ __forceinline__ void add(int k, unsigned long long v) const
+    {
+        const unsigned l = (unsigned)v;
+        const unsigned old = atomicAdd(&lo[k], l);
+        const unsigned h = (unsigned)(v >> 32) + (old + l < old ? 1u : 0u);
+        if (h) atomicAdd(&hi[k], h);
+    }
+    __device__ __forceinline__ unsigned long long take(int k) const  // read and clear (no other writer)
+    {
+        const unsigned long long w = ((unsigned long long)hi[k] << 32) | lo[k];
+        lo[k] = 0u;
+        hi[k] = 0u;
+        return w;
+    }
+};
+
+__device__ __forceinline__ void joint_flush_packed(const PairArgs& a, const SplitWords& hcell,
+                                                   const SplitWords& hfine, int ncell, const double* vcen)
 {
     const int nd = a.nb;
     for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
-        const unsigned long long w = hcell[k];
-        if (!w) continue;
+        if (!(hcell.lo[k] | hcell.hi[k])) continue;
+        const unsigned long long w = hcell.take(k);
         const unsigned long long cnt = (w + (1ull << 43)) >> 44;
         const long long off = (long long)(w - (cnt << 44));
         const int vb = k / nd + 1;
-        double s = (double)cnt * value_center(a, vb) + (double)off * a.vqc_inv;
+        double s = (double)cnt * vcen[vb - 1] + (double)off * a.vqc_inv;
         const int f = vb - a.vfine_lo;
-        if ((unsigned)f < (unsigned)a.nfine) {
-            unsigned long long* fw = hfine + (k - (vb - 1) * nd) + nd * f;
-            s += (double)(long long)*fw * a.vq_inv;
-            *fw = 0ull;
-        }
+        if ((unsigned)f < (unsigned)a.nfine)
+            s += (double)(long long)hfine.take((k - (vb - 1) * nd) + nd * f) * a.vq_inv;
         atomicAdd(&a.g_sums[k], s);
         atomicAdd(&a.g_counts[k], cnt);
-        hcell[k] = 0ull;
     }
     __syncthreads();
 }
@@ -527,13 +561,17 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     const int ncell = nd * nv;
     LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
     double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);                                 // T * 2NP
-    unsigned long long* hcell = reinterpret_cast<unsigned long long*>(srec + (size_t)2 * NP * T);  // ncell
-    unsigned long long* hfine = hcell + ncell;                                                     // nd * nfine
+    unsigned* words = reinterpret_cast<unsigned*>(srec + (size_t)2 * NP * T);
+    const int nfw = nd * a.nfine;
+    const SplitWords hcell{words, words + ncell};                                  // 2 x ncell
+    const SplitWords hfine{words + 2 * ncell, words + 2 * ncell + nfw};            // 2 x nd * nfine
+    double* vcen = reinterpret_cast<double*>(words + 2 * (ncell + nfw));           // nv
+    float* vc32 = reinterpret_cast<float*>(vcen + nv);                             // nv
     __shared__ unsigned long long s_recheck;
 
     for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
-    for (int k = threadIdx.x; k < ncell + nd * a.nfine; k += T) hcell[k] = 0ull;
+    for (int k = threadIdx.x; k < 2 * (ncell + nfw); k += T) words[k] = 0u;
     if (threadIdx.x == 0) s_recheck = 0ull;
     unsigned my_recheck = 0;
     const int ku = pow2_exponent_above(a.g_stats[2]);
@@ -545,6 +583,19 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     const bool vfast = a.val_linear && isfinite(vinv) && vinv != 0.f;
     const float vnegf = (float)a.vlin.neg_f_inv;
     const float tmax = (float)(a.vlin.n - 1);
+    // centres C_b in the FP32 value's units and their exact FP64 images; FP32 offsets need every
+    // centre and the fixed-point scale to be normal FP32 numbers
+    const float vqcs = (float)(a.vqc * unscale[0]);
+    bool cok = vfast && vqcs != 0.f && f32_zero_or_normal(vqcs);
+    for (int k = threadIdx.x; k < nv; k += T) {
+        const double c64 = value_center(a, k + 1);
+        const float c = (float)(c64 / unscale[0]);
+        const bool normal = f32_zero_or_normal(c);
+        vc32[k] = c;
+        vcen[k] = normal ? (double)c * unscale[0] : c64;  // any finite reference centre is exact
+        cok = cok && normal;
+    }
+    const bool qfast = __syncthreads_and(cok) != 0;
 
     // field c of point k as staged: sphere XM (velocity fields scaled), flat x then u (u scaled)
     auto field = [&](int c, int k) -> double {
@@ -556,7 +607,7 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     for (long long p = p0; p < p1; p += ps, ++iter) {
         if (iter && iter % a.flush_every == 0) {
             __syncthreads();
-            joint_flush_packed(a, hcell, hfine, ncell);
+            joint_flush_packed(a, hcell, hfine, ncell, vcen);
         }
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
@@ -576,7 +627,14 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
         __syncthreads();
         if (!iv) continue;
         const bool diag = ti == tj;
-        for (int jj = diag ? (int)threadIdx.x + 1 : 0; jj < jn; ++jj) {
+        // one pair (i, j0 + jj): its cell and packed increment (cell < 0: nothing to add) and, in a
+        // bin near zero, its fine offset
+        struct JointAdd {
+            int cell, fidx;
+            long long q, fq;
+        };
+        auto eval_pair = [&](int jj) -> JointAdd {
+            JointAdd r{-1, -1, 0, 0};
             double rb[2 * NP];
             load_rec2<NP>(srec + jj * 2 * NP, rb);
             float L, Tt, T2, Q;
@@ -598,7 +656,7 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                 if (a.dist_linear) db = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
                 else db = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
                 // flat bins are exact: a pair outside the distance range needs no value
-                if (db < 1 || db > nd) continue;
+                if (db < 1 || db > nd) return r;
                 fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q);
             }
             float v[1];
@@ -606,13 +664,13 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
             const float val = v[0];
             int vb = 0;
             if (vfast) {
+                // t within wt of an integer (an edge; the range ends are edges too) or NaN: exact route
                 const float t = fmaf(val, vinv, vnegf);
                 const float fl = floorf(t);
                 const float fr = t - fl;
                 const float wt = (fabsf(t) + fabsf(vnegf)) * a.vrel;
-                vb = (t <= 0.f) ? 0 : ((t > tmax) ? a.vlin.n : (int)fl + 1);
-                slow = slow || !fine || fr < wt || fr > 1.f - wt || fabsf(t) < wt || fabsf(t - tmax) < wt ||
-                       !(t == t);
+                vb = (int)fminf(fmaxf(fl, -1.f), tmax) + 1;  // 0 below the range, nv + 1 above
+                slow = slow || !fine || !(fr > wt && fr < 1.f - wt);
             } else {
                 slow = true;  // vector value edges (or an unrepresentable index scale): exact FP64 search
             }
@@ -650,21 +708,42 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                 ++my_recheck;
             }
             if (ok && db >= 1 && db <= nd && vb >= 1 && vb <= nv) {
-                const int cell = (db - 1) + nd * (vb - 1);
-                const double off = (slow ? v64 : (double)val * unscale[0]) - value_center(a, vb);
+                r.cell = (db - 1) + nd * (vb - 1);
                 const int f = vb - a.vfine_lo;
-                if ((unsigned)f < (unsigned)a.nfine) {
-                    atomicAdd(&hcell[cell], 1ull << 44);
-                    atomicAdd(&hfine[(db - 1) + nd * f], (unsigned long long)__double2ll_rn(off * a.vq));
+                const bool fine_bin = (unsigned)f < (unsigned)a.nfine;
+                if (qfast && !slow && !fine_bin) {
+                    r.q = __float2int_rn((val - vc32[vb - 1]) * vqcs);  // exact difference, power-of-2 scale
                 } else {
-                    atomicAdd(&hcell[cell], (1ull << 44) + (unsigned long long)__double2ll_rn(off * a.vqc));
+                    const double off = (slow ? v64 : (double)val * unscale[0]) - vcen[vb - 1];
+                    if (fine_bin) {
+                        r.fidx = (db - 1) + nd * f;
+                        r.fq = __double2ll_rn(off * a.vq);
+                    } else {
+                        r.q = __double2ll_rn(off * a.vqc);
+                    }
                 }
             }
+            return r;
+        };
+        auto commit = [&](const JointAdd& r) {
+            if (r.cell < 0) return;
+            if (r.fidx >= 0) hfine.add(r.fidx, (unsigned long long)r.fq);
+            hcell.add(r.cell, (1ull << 44) + (unsigned long long)r.q);
+        };
+        int jj = diag ? (int)threadIdx.x + 1 : 0;
+        if constexpr (!SPHERE) {  // two independent pairs in flight per thread (latency hiding)
+            for (; jj + 1 < jn; jj += 2) {
+                const JointAdd r0 = eval_pair(jj);
+                const JointAdd r1 = eval_pair(jj + 1);
+                commit(r0);
+                commit(r1);
+            }
         }
+        for (; jj < jn; ++jj) commit(eval_pair(jj));
     }
     if (my_recheck) atomicAdd(&s_recheck, (unsigned long long)my_recheck);
     __syncthreads();
-    joint_flush_packed(a, hcell, hfine, ncell);
+    joint_flush_packed(a, hcell, hfine, ncell, vcen);
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 

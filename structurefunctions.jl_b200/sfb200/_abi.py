@@ -124,6 +124,7 @@ EXPORTED_SYMBOLS = (
     "sfb200_device_memory",
     "sfb200_batch_wait",
     "sfb200_batch_query",
+    "sfb200_batch_wait_oldest",
     "sfb200_run_noalloc",
 )
 

@@ -68,6 +68,8 @@ def load():
         lib.sfb200_batch_wait.restype = C.c_int
         lib.sfb200_batch_query.argtypes = [P, C.POINTER(C.c_int32)]
         lib.sfb200_batch_query.restype = C.c_int
+        lib.sfb200_batch_wait_oldest.argtypes = [P, C.POINTER(C.c_int64)]
+        lib.sfb200_batch_wait_oldest.restype = C.c_int
         lib.sfb200_run_noalloc.argtypes = [P, P, P, C.c_int64, C.c_uint32, P, P, P]
         lib.sfb200_run_noalloc.restype = C.c_int
         if lib.sfb200_abi_version() != _abi.ABI_VERSION:
@@ -184,12 +186,19 @@ def batch_run(ctx, slices, begins, ends, stream=None):
 
 
 def batch_wait(ctx):
-    """Block until the context's last round has finished."""
+    """Block until every queued round of the context has finished."""
     check(load().sfb200_batch_wait(ctx.ptr), ctx.ptr, "batch wait")
 
 
+def batch_wait_oldest(ctx):
+    """Block until the oldest unfinished round has finished; returns its number (0: none was)."""
+    r = C.c_int64()
+    check(load().sfb200_batch_wait_oldest(ctx.ptr, C.byref(r)), ctx.ptr, "batch wait")
+    return int(r.value)
+
+
 def batch_done(ctx):
-    """True when the context's last round has finished (non-blocking)."""
+    """True when every queued round of the context has finished (non-blocking)."""
     d = C.c_int32()
     check(load().sfb200_batch_query(ctx.ptr, C.byref(d)), ctx.ptr, "batch query")
     return bool(d.value)

@@ -14,6 +14,9 @@ busy with all of them at once:
   round's pair budget shortest-remaining-first, and runs all of it as one batched launch (one
   persistent kernel per kernel variant, replayed from a CUDA graph). Requests that arrive while a
   round runs join the next one: continuous batching, not a queue in front of one-at-a-time launches.
+- Pipelining. Up to `depth` rounds are queued at once (the library double-buffers them): while one
+  runs on the device the next is already queued behind it, so the device does not idle while the
+  host completes, admits and plans between rounds.
 - Completion. A slice whose tile pairs are all done is read back, its ticket completed with the
   latency (arrival to result) and the slice released.
 
@@ -96,18 +99,20 @@ class _Active:
     units: int          # tile pairs in total
     done: int = 0       # tile pairs completed (always a prefix [0, done))
     pairs_per_unit: float = 1.0
+    issued: int = 0     # tile pairs queued in rounds so far (a prefix [0, issued), issued >= done)
 
     @property
     def remaining(self):
-        return self.units - self.done
+        return self.units - self.issued
 
 
 class Server:
     """Continuous-batching loop over an executor (see the module documentation)."""
 
     def __init__(self, executor, max_slots=48, memory_reserve=1 << 30, round_pairs=1.5e9, min_units=1,
-                 clock=time.perf_counter):
+                 depth=2, clock=time.perf_counter):
         self.ex = executor
+        self.depth = max(1, int(depth)) if hasattr(executor, "wait_oldest") else 1
         self.max_slots = int(max_slots)
         self.memory_reserve = int(memory_reserve)
         self.round_pairs = float(round_pairs)
@@ -174,21 +179,23 @@ class Server:
                 self._active.append(a)
 
     def _plan_round(self):
-        """Tile-pair ranges of this round: min_units each, then shortest remaining first."""
+        """Tile-pair ranges of this round: min_units each, then shortest remaining first (over the
+        slices with tile pairs not yet queued)."""
         budget = self.round_pairs
-        give = {id(a): 0 for a in self._active}
-        for a in self._active:
+        ready = [a for a in self._active if a.remaining > 0]
+        give = {id(a): 0 for a in ready}
+        for a in ready:
             k = min(a.remaining, self.min_units)
             give[id(a)] = k
             budget -= k * a.pairs_per_unit
-        for a in sorted(self._active, key=lambda a: a.remaining * a.pairs_per_unit):
+        for a in sorted(ready, key=lambda a: a.remaining * a.pairs_per_unit):
             if budget <= 0:
                 break
             extra = min(a.remaining - give[id(a)], int(budget // a.pairs_per_unit) + 1)
             if extra > 0:
                 give[id(a)] += extra
                 budget -= extra * a.pairs_per_unit
-        return [(a, a.done, a.done + give[id(a)]) for a in self._active if give[id(a)] > 0]
+        return [(a, a.issued, a.issued + give[id(a)]) for a in ready if give[id(a)] > 0]
 
     def _complete(self, a):
         t = a.ticket
@@ -202,32 +209,42 @@ class Server:
         t._event.set()
 
     def _loop(self):
+        inflight = collections.deque()  # queued rounds, oldest first: lists of (active, begin, end)
         while True:
             self._admit()
-            if not self._active:
-                with self._cv:
-                    if self._pending:
-                        continue
-                    if self._stop:
-                        return
-                    self._cv.wait(timeout=0.005)
+            if len(inflight) < self.depth and any(a.remaining > 0 for a in self._active):
+                plan = self._plan_round()
+                self.ex.run_round([(a.handle, b, e) for a, b, e in plan])
+                for a, b, e in plan:
+                    a.issued = e
+                inflight.append(plan)
+                self.rounds += 1
+                self.round_log.append((len(plan), sum((e - b) * a.pairs_per_unit for a, b, e in plan)))
                 continue
-            plan = self._plan_round()
-            self.ex.run_round([(a.handle, b, e) for a, b, e in plan])
-            self.rounds += 1
-            self.round_log.append((len(plan), sum((e - b) * a.pairs_per_unit for a, b, e in plan)))
-            # admit arrivals while the round runs (their preparation overlaps it)
-            self._admit()
-            self.ex.wait_round()
-            finished = []
-            for a, b, e in plan:
-                a.done = e
-                a.ticket.rounds += 1
-                if a.done >= a.units:
-                    finished.append(a)
-            for a in finished:
-                self._active.remove(a)
-                self._complete(a)
+            if inflight:
+                # admit arrivals while the queued rounds run (their preparation overlaps them)
+                self._admit()
+                if self.depth > 1:
+                    self.ex.wait_oldest()
+                else:
+                    self.ex.wait_round()
+                plan = inflight.popleft()
+                finished = []
+                for a, b, e in plan:
+                    a.done = e
+                    a.ticket.rounds += 1
+                    if a.done >= a.units:
+                        finished.append(a)
+                for a in finished:
+                    self._active.remove(a)
+                    self._complete(a)
+                continue
+            with self._cv:
+                if self._pending:
+                    continue
+                if self._stop:
+                    return
+                self._cv.wait(timeout=0.005)
 
 
 # ---------------------------------------------------------------------------------- GPU executor
@@ -287,6 +304,9 @@ class GpuExecutor:
 
     def wait_round(self):
         _lib.batch_wait(self.ctx)
+
+    def wait_oldest(self):
+        _lib.batch_wait_oldest(self.ctx)
 
     def read(self, h):
         sums = np.zeros(h.n_sums)

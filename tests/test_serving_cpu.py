@@ -5,8 +5,11 @@ work (256-point tiles), a round runs tile-pair ranges of several slices, and a s
 readable once every unit ran. The simulation records every range, so the tests can check the
 invariants the GPU path relies on: each tile pair of each request runs exactly once, in order;
 admission honours the slot count and the memory reserve; every admitted slice progresses in every
-round; short requests are not held behind long ones; a bad request fails alone.
+round; short requests are not held behind long ones; a bad request fails alone; with pipelined
+rounds, no more than `depth` rounds are queued at once, rounds complete oldest first, and a slice is
+read only after every round that touched it has completed.
 """
+import collections
 import threading
 
 import numpy as np
@@ -34,6 +37,8 @@ class FakeExecutor:
         self.bpp = bytes_per_point
         self.fail_n = fail_n
         self.rounds = []
+        self.inflight = collections.deque()
+        self.max_inflight = 0
         self.live = 0
         self.max_live = 0
         self.admissions = []  # (slices live before, free bytes after)
@@ -57,13 +62,19 @@ class FakeExecutor:
 
     def run_round(self, work):
         self.rounds.append([(h, b, e) for h, b, e in work])
+        self.inflight.append(self.rounds[-1])
+        self.max_inflight = max(self.max_inflight, len(self.inflight))
         for h, b, e in work:
             h.ranges.append((b, e))
 
     def wait_round(self):
-        pass
+        self.inflight.clear()
+
+    def wait_oldest(self):
+        self.inflight.popleft()
 
     def read(self, h):
+        assert all(h is not g for r in self.inflight for g, _, _ in r), "read while a round is queued"
         # the "histogram": how many times each tile pair ran (must be all ones)
         cover = np.zeros(h.tile_pairs, dtype=np.int64)
         for b, e in h.ranges:
@@ -180,3 +191,37 @@ def test_threaded_arrivals_complete():
         sums, counts = t.wait(5)
         assert int(counts[0]) == n and np.all(sums == 1.0)
         assert t.latency >= 0
+
+
+class SerialExecutor(FakeExecutor):
+    """An executor that can only wait for all queued rounds: the loop runs one round at a time."""
+
+    def __getattribute__(self, name):
+        if name == "wait_oldest":
+            raise AttributeError(name)
+        return super().__getattribute__(name)
+
+
+@pytest.mark.parametrize("depth", [1, 2, 3])
+def test_pipelined_rounds_stay_within_depth(depth):
+    ex = FakeExecutor()
+    srv = Server(ex, max_slots=6, round_pairs=2e5, memory_reserve=0, depth=depth)
+    sizes = [9000, 300, 4000, 12000, 2, 700, 5000, 256]
+    tickets = [srv.submit(req(n)) for n in sizes]
+    srv.run_until_idle()
+    assert ex.max_inflight == depth
+    assert not ex.inflight
+    for t, n in zip(tickets, sizes):
+        sums, counts = t.wait(0)
+        assert int(counts[0]) == n and np.all(sums == 1.0)
+    assert ex.live == 0
+
+
+def test_executor_without_wait_oldest_runs_one_round_at_a_time():
+    ex = SerialExecutor()
+    srv = Server(ex, max_slots=4, round_pairs=2e5, memory_reserve=0, depth=2)
+    assert srv.depth == 1
+    ts = [srv.submit(req(n)) for n in (3000, 5000, 100)]
+    srv.run_until_idle()
+    assert ex.max_inflight == 1
+    assert all(np.all(t.wait(0)[0] == 1.0) for t in ts)

@@ -56,11 +56,13 @@ def oracle_of(r):
     return oracle_py.run(desc, r.x, r.u, with_abs=True)
 
 
-def test_results_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("depth", [1, 2])
+def test_results_same_alone_and_in_the_mix(depth):
     reqs = make_requests()
     ex = GpuExecutor(0)
     try:
-        srv = Server(ex, max_slots=12, round_pairs=2e6).start()  # small rounds: many interleavings
+        # small rounds: many interleavings; depth 2 queues the next round while one runs
+        srv = Server(ex, max_slots=12, round_pairs=2e6, depth=depth).start()
         tickets = [srv.submit(r) for r in reqs]
         srv.stop()
         assert srv.rounds > 1
@@ -102,5 +104,34 @@ def test_round_graph_replay_and_ranges_split_across_rounds():
         assert t.rounds == srv.rounds and t.rounds > 3
         rs, rc, ra = oracle_of(r)
         compare(s, c, rs, rc, ra, TOL_MIXED)
+    finally:
+        ex.close()
+
+
+def test_queued_rounds_on_one_slice_complete_in_order():
+    """Three rounds over one slice queued back to back: queuing the third waits for the first (two
+    buffers), the other two finish oldest first, the slice's result covers every tile pair once, and
+    the slice memory is released without a host wait and counted free again."""
+    import torch
+
+    r = make_requests(seed=9, count=1)[0]
+    ex = GpuExecutor(0)
+    try:
+        h = ex.create(r)
+        units = h.tile_pairs
+        assert units >= 3
+        cuts = [0, units // 3, 2 * units // 3, units]
+        for b, e in zip(cuts, cuts[1:]):
+            _lib.batch_run(ex.ctx, [h.slice], [b], [e])
+        assert _lib.batch_wait_oldest(ex.ctx) == 2  # rounds are numbered from 1 per context
+        assert _lib.batch_wait_oldest(ex.ctx) == 3
+        assert _lib.batch_wait_oldest(ex.ctx) == 0 and _lib.batch_done(ex.ctx)
+        s, c = ex.read(h)
+        rs, rc, ra = oracle_of(r)
+        compare(s, c, rs, rc, ra, TOL_MIXED)
+        free_before = ex.free_bytes()
+        ex.destroy(h)
+        torch.cuda.synchronize()
+        assert ex.free_bytes() >= free_before + h.device_bytes - (2 << 20)
     finally:
         ex.close()
