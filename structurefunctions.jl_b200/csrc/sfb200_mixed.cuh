@@ -503,7 +503,8 @@ __global__ void __launch_bounds__(256, 3) k_sphere1d_mx_batch(const BatchArgs b)
 // value (per block in shared memory, with its exact FP64 image for the flush). In every coarse bin
 // the values lie within a half width of a centre at least three half widths from zero, so the FP32
 // subtraction v - C_b is exact (Sterbenz) and its fixed-point image is one FP32 multiply by a power
-// of two and one conversion; the FP64 route remains for rechecked pairs and the bins near zero.
+// of two and one conversion. In the bins near zero the difference is taken exactly as the FP32 sum
+// s + e (TwoSum) and both parts are converted; the FP64 route remains for rechecked pairs only.
 // ================================================================================================
 // A 64-bit shared word kept as two 32-bit halves (lo[k], hi[k]) in separate arrays, so that every
 // update is a native 32-bit shared atomic (a 64-bit shared atomic add is a compare-and-swap loop on
@@ -513,12 +514,14 @@ __global__ void __launch_bounds__(256, 3) k_sphere1d_mx_batch(const BatchArgs b)
 struct SplitWords {
     unsigned* lo;
     unsigned* hi;
-    __device__ __forceinline__ void add(int k, unsigned long long v) const
+    // adds HI * 2^32 + q (q sign-extended to 64 bits); with HI != 0 the high add always happens
+    template <unsigned HI>
+    __device__ __forceinline__ void add(int k, int q) const
     {
-        const unsigned l = (unsigned)v;
+        const unsigned l = (unsigned)q;
         const unsigned old = atomicAdd(&lo[k], l);
-        const unsigned h = (unsigned)(v >> 32) + (old + l < old ? 1u : 0u);
-        if (h) atomicAdd(&hi[k], h);
+        const unsigned h = HI + (q < 0 ? 0xffffffffu : 0u) + (old + l < old ? 1u : 0u);
+        if (HI != 0u || h != 0u) atomicAdd(&hi[k], h);
     }
     __device__ __forceinline__ unsigned long long take(int k) const  // read and clear (no other writer)
     {
@@ -586,7 +589,8 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     // centres C_b in the FP32 value's units and their exact FP64 images; FP32 offsets need every
     // centre and the fixed-point scale to be normal FP32 numbers
     const float vqcs = (float)(a.vqc * unscale[0]);
-    bool cok = vfast && vqcs != 0.f && f32_zero_or_normal(vqcs);
+    const float vqfs = (float)(a.vq * unscale[0]);
+    bool cok = vfast && vqcs != 0.f && f32_zero_or_normal(vqcs) && vqfs != 0.f && f32_zero_or_normal(vqfs);
     for (int k = threadIdx.x; k < nv; k += T) {
         const double c64 = value_center(a, k + 1);
         const float c = (float)(c64 / unscale[0]);
@@ -630,8 +634,7 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
         // one pair (i, j0 + jj): its cell and packed increment (cell < 0: nothing to add) and, in a
         // bin near zero, its fine offset
         struct JointAdd {
-            int cell, fidx;
-            long long q, fq;
+            int cell, fidx, q, fq;
         };
         auto eval_pair = [&](int jj) -> JointAdd {
             JointAdd r{-1, -1, 0, 0};
@@ -662,8 +665,8 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
             float v[1];
             eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
             const float val = v[0];
-            int vb = 0;
-            if (vfast) {
+            int vb = 0, q = 0, fq = 0;
+            if (qfast) {
                 // t within wt of an integer (an edge; the range ends are edges too) or NaN: exact route
                 const float t = fmaf(val, vinv, vnegf);
                 const float fl = floorf(t);
@@ -671,14 +674,21 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                 const float wt = (fabsf(t) + fabsf(vnegf)) * a.vrel;
                 vb = (int)fminf(fmaxf(fl, -1.f), tmax) + 1;  // 0 below the range, nv + 1 above
                 slow = slow || !fine || !(fr > wt && fr < 1.f - wt);
+                // offset from the bin centre as the exact FP32 sum s + e (TwoSum; e = 0 in the coarse
+                // bins, where the subtraction is exact), then both fixed-point images
+                const float c = vc32[min(max(vb, 1), nv) - 1];
+                const float sd = val - c;
+                const float bv = sd - val;
+                const float e = (val - (sd - bv)) + (-c - bv);
+                q = __float2int_rn(sd * vqcs);
+                fq = __float2int_rn(sd * vqfs) + __float2int_rn(e * vqfs);
             } else {
-                slow = true;  // vector value edges (or an unrepresentable index scale): exact FP64 search
+                slow = true;  // vector value edges (or an unrepresentable FP32 scale): exact FP64 route
             }
-            double v64 = 0.0;
             bool ok = true;
             if (slow) {
                 const int j = j0 + jj;
-                double du64[D];
+                double du64[D], v64;
                 if constexpr (!SPHERE) {
                     double dx64[D];
 #pragma unroll
@@ -705,30 +715,29 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                     v64 = x_sphere_value<D>(a.gen.op[0], du64);
                 }
                 vb = value_exact_bin(a, v64);
+                if (vb >= 1 && vb <= nv) {
+                    const double off = v64 - vcen[vb - 1];  // exact: both within a bin of each other
+                    q = __double2int_rn(off * a.vqc);
+                    fq = __double2int_rn(off * a.vq);
+                }
                 ++my_recheck;
             }
             if (ok && db >= 1 && db <= nd && vb >= 1 && vb <= nv) {
                 r.cell = (db - 1) + nd * (vb - 1);
                 const int f = vb - a.vfine_lo;
-                const bool fine_bin = (unsigned)f < (unsigned)a.nfine;
-                if (qfast && !slow && !fine_bin) {
-                    r.q = __float2int_rn((val - vc32[vb - 1]) * vqcs);  // exact difference, power-of-2 scale
+                if ((unsigned)f < (unsigned)a.nfine) {  // near zero: the offset goes to the fine word
+                    r.fidx = (db - 1) + nd * f;
+                    r.fq = fq;
                 } else {
-                    const double off = (slow ? v64 : (double)val * unscale[0]) - vcen[vb - 1];
-                    if (fine_bin) {
-                        r.fidx = (db - 1) + nd * f;
-                        r.fq = __double2ll_rn(off * a.vq);
-                    } else {
-                        r.q = __double2ll_rn(off * a.vqc);
-                    }
+                    r.q = q;
                 }
             }
             return r;
         };
         auto commit = [&](const JointAdd& r) {
             if (r.cell < 0) return;
-            if (r.fidx >= 0) hfine.add(r.fidx, (unsigned long long)r.fq);
-            hcell.add(r.cell, (1ull << 44) + (unsigned long long)r.q);
+            if (r.fidx >= 0) hfine.add<0u>(r.fidx, r.fq);
+            hcell.add<1u << 12>(r.cell, r.q);  // count (bit 44 of the word) and coarse offset
         };
         int jj = diag ? (int)threadIdx.x + 1 : 0;
         if constexpr (!SPHERE) {  // two independent pairs in flight per thread (latency hiding)
@@ -748,14 +757,14 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
 }
 
 template <bool SPHERE, int D, class OPS>
-__global__ void __launch_bounds__(512) k_joint_mx(const PairArgs a)
+__global__ void __launch_bounds__(512, 1) k_joint_mx(const PairArgs a)
 {
     joint_mx_run<SPHERE, D, OPS>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.
 template <bool SPHERE, int D, class OPS>
-__global__ void __launch_bounds__(512) k_joint_mx_batch(const BatchArgs b)
+__global__ void __launch_bounds__(512, 1) k_joint_mx_batch(const BatchArgs b)
 {
     batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { joint_mx_run<SPHERE, D, OPS>(a, q0, q1, 1); });
 }
