@@ -552,6 +552,56 @@ __device__ __forceinline__ void joint_flush_packed(const PairArgs& a, const Spli
     __syncthreads();
 }
 
+// Exact FP64 route of one joint pair (i, j) (the reference formula for the distance bin, the value
+// and the value bin), kept out of line: the pair loop only branches to it for the rare pairs that
+// need it. `a` points to the kernel's parameters in place (grid constants); q, fq are the coarse and
+// fine fixed-point offsets from the value-bin centre.
+struct JointExact {
+    int db, vb, q, fq;
+    bool ok;
+};
+
+template <bool SPHERE, int D>
+__device__ __noinline__ JointExact joint_exact_pair(const PairArgs* ap, int i, int j, const double* vcen)
+{
+    const PairArgs& a = *ap;
+    const int n = a.n;
+    JointExact r{0, 0, 0, 0, true};
+    double du64[D], v64;
+    if constexpr (!SPHERE) {
+        double dx64[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            dx64[d] = SFB_SUB(a.X64[(size_t)d * n + j], a.X64[(size_t)d * n + i]);
+            du64[d] = SFB_SUB(a.U64[(size_t)d * n + j], a.U64[(size_t)d * n + i]);
+        }
+        const double r264 = x_dot<D>(dx64, dx64);
+        r.db = flat_exact_bin(a, r264);
+        v64 = x_sf_raw<D>(a.gen.op[0], du64, dx64, r264);
+    } else {
+        SphPoint A, B;
+        load_sph64(a.X64, n, i, A);
+        load_sph64(a.X64, n, j, B);
+        double rr, tA[2], tB[2], uA[D], uB[D];
+        r.ok = x_sphere_frame(A, B, a.radius, rr, tA, tB);
+        r.db = sphere_exact_bin(a, rr);
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            uA[d] = a.U64[(size_t)d * n + i];
+            uB[d] = a.U64[(size_t)d * n + j];
+        }
+        x_sphere_delta<D>(tA, tB, uA, uB, du64);
+        v64 = x_sphere_value<D>(a.gen.op[0], du64);
+    }
+    r.vb = value_exact_bin(a, v64);
+    if (r.vb >= 1 && r.vb <= a.nv) {
+        const double off = v64 - vcen[r.vb - 1];  // exact: both within a bin of each other
+        r.q = __double2int_rn(off * a.vqc);
+        r.fq = __double2int_rn(off * a.vq);
+    }
+    return r;
+}
+
 template <bool SPHERE, int D, class OPS>
 __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, long long p1, long long ps)
 {
@@ -687,39 +737,12 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
             }
             bool ok = true;
             if (slow) {
-                const int j = j0 + jj;
-                double du64[D], v64;
-                if constexpr (!SPHERE) {
-                    double dx64[D];
-#pragma unroll
-                    for (int d = 0; d < D; ++d) {
-                        dx64[d] = SFB_SUB(a.X64[(size_t)d * n + j], a.X64[(size_t)d * n + i]);
-                        du64[d] = SFB_SUB(a.U64[(size_t)d * n + j], a.U64[(size_t)d * n + i]);
-                    }
-                    const double r264 = x_dot<D>(dx64, dx64);
-                    db = flat_exact_bin(a, r264);
-                    v64 = x_sf_raw<D>(a.gen.op[0], du64, dx64, r264);
-                } else {
-                    SphPoint A, B;
-                    load_sph64(a.X64, n, i, A);
-                    load_sph64(a.X64, n, j, B);
-                    double r, tA[2], tB[2], uA[D], uB[D];
-                    ok = x_sphere_frame(A, B, a.radius, r, tA, tB);
-                    db = sphere_exact_bin(a, r);
-#pragma unroll
-                    for (int d = 0; d < D; ++d) {
-                        uA[d] = a.U64[(size_t)d * n + i];
-                        uB[d] = a.U64[(size_t)d * n + j];
-                    }
-                    x_sphere_delta<D>(tA, tB, uA, uB, du64);
-                    v64 = x_sphere_value<D>(a.gen.op[0], du64);
-                }
-                vb = value_exact_bin(a, v64);
-                if (vb >= 1 && vb <= nv) {
-                    const double off = v64 - vcen[vb - 1];  // exact: both within a bin of each other
-                    q = __double2int_rn(off * a.vqc);
-                    fq = __double2int_rn(off * a.vq);
-                }
+                const JointExact x = joint_exact_pair<SPHERE, D>(&a, i, j0 + jj, vcen);
+                db = x.db;
+                vb = x.vb;
+                q = x.q;
+                fq = x.fq;
+                ok = x.ok;
                 ++my_recheck;
             }
             if (ok && db >= 1 && db <= nd && vb >= 1 && vb <= nv) {
@@ -757,14 +780,14 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
 }
 
 template <bool SPHERE, int D, class OPS>
-__global__ void __launch_bounds__(512, 1) k_joint_mx(const PairArgs a)
+__global__ void __launch_bounds__(512, 1) k_joint_mx(const __grid_constant__ PairArgs a)
 {
     joint_mx_run<SPHERE, D, OPS>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.
 template <bool SPHERE, int D, class OPS>
-__global__ void __launch_bounds__(512, 1) k_joint_mx_batch(const BatchArgs b)
+__global__ void __launch_bounds__(512, 1) k_joint_mx_batch(const __grid_constant__ BatchArgs b)
 {
     batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { joint_mx_run<SPHERE, D, OPS>(a, q0, q1, 1); });
 }
