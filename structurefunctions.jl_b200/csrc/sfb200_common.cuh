@@ -87,6 +87,13 @@ __device__ __forceinline__ int count_below(const double* __restrict__ tab, int n
     return lo;
 }
 
+// count_below kept out of line, for the rare table cells that hold more than one edge: the pair
+// loops only branch to it.
+static __device__ __noinline__ int count_below_ool(const double* __restrict__ tab, int n, double key)
+{
+    return count_below(tab, n, key);
+}
+
 // LinearBinEdges search, src/BinEdges.jl:114-131, returning the bin (searchsortedfirst - 1).
 // NaN keys return n (out of range); the reference throws there.
 struct LinearParams {

@@ -128,7 +128,7 @@ __device__ __forceinline__ int sphere_exact_bin(const PairArgs& a, double r)
 __device__ __forceinline__ int lut64_bin(const LutEntry64* lut, const PairArgs& a, double key)
 {
     const LutEntry64 e = lut[lut_cell64(key, a.lg)];
-    if (e.mult & LUT_FLAG_SLOW) return count_below(a.edges, a.n_edges, key);
+    if (e.mult & LUT_FLAG_SLOW) return count_below_ool(a.edges, a.n_edges, key);
     return e.base + (key > e.e ? e.mult : 0);
 }
 

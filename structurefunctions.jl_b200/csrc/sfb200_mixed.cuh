@@ -166,6 +166,32 @@ __device__ __forceinline__ void flat_values_fp64(const double (&dx)[D], const do
     for (int o = 0; o < NV; ++o) v[o] = f32(v64[o]);
 }
 
+// flat_values_fp64 out of line (pairs with r^2 outside the FP32 range are rare): scalar arguments,
+// the operator descriptors read in place from the kernel parameters (grid constants).
+template <int D, class OPS>
+struct FlatValues {
+    float v[OPS::n];
+};
+
+template <int D, class OPS>
+__device__ __noinline__ FlatValues<D, OPS> flat_values_fp64_ool(double dx0, double dx1, double dx2, double du0,
+                                                                double du1, double du2, double r2, double h2,
+                                                                const GenOps* g)
+{
+    double dx[D], du[D];
+    dx[0] = dx0;
+    dx[1] = dx1;
+    du[0] = du0;
+    du[1] = du1;
+    if constexpr (D == 3) {
+        dx[2] = dx2;
+        du[2] = du2;
+    }
+    FlatValues<D, OPS> r;
+    flat_values_fp64<D, OPS>(dx, du, r2, h2, *g, r.v);
+    return r;
+}
+
 // ================================================================================================
 // Flat (Euclidean) 1D
 //
@@ -241,7 +267,12 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
             float L, Tt, T2, Q;
             const bool fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q);
             eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
-            if (!fine) flat_values_fp64<D, OPS>(dx, du, r2, h2, a.gen, v);
+            if (!fine) {
+                const FlatValues<D, OPS> f = flat_values_fp64_ool<D, OPS>(
+                    dx[0], dx[1], D == 3 ? dx[D - 1] : 0.0, du[0], du[1], D == 3 ? du[D - 1] : 0.0, r2, h2, &a.gen);
+#pragma unroll
+                for (int o = 0; o < NV; ++o) v[o] = f.v[o];
+            }
         };
         if constexpr (Hist::RUN) {
             if (iv) {
@@ -267,14 +298,14 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
 }
 
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256) k_flat1d_mx(const PairArgs a)
+__global__ void __launch_bounds__(256) k_flat1d_mx(const __grid_constant__ PairArgs a)
 {
     flat1d_mx_run<D, OPS, PRIV>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256) k_flat1d_mx_batch(const BatchArgs b)
+__global__ void __launch_bounds__(256) k_flat1d_mx_batch(const __grid_constant__ BatchArgs b)
 {
     batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { flat1d_mx_run<D, OPS, PRIV>(a, q0, q1, 1); });
 }
