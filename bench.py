@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4"])
     ap.add_argument("--requests", type=int, default=2000, help="c4: number of requests")
     ap.add_argument("--rate", type=float, default=200.0, help="c4: Poisson arrival rate per second")
+    ap.add_argument("--slots", type=int, default=256, help="c4: slices resident at once (admission slots)")
+    ap.add_argument("--round-pairs", type=float, default=1.5e9, help="c4: pair budget of one batched round")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample length")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
@@ -511,7 +513,7 @@ def run_serving(args):
     # ---- batched
     ex = GpuExecutor(local)
     clocks = ClockSampler(local)
-    srv = Server(ex, max_slots=48, round_pairs=1.5e9).start()
+    srv = Server(ex, max_slots=args.slots, round_pairs=args.round_pairs).start()
     for q in warm:
         for r in subrequests(q):
             srv.submit(r).wait(120)
@@ -620,7 +622,7 @@ def run_serving(args):
                                "the 256-value-bin joint histogram",
                    "total_pairs": int(total_pairs), "step": "one request (1D and, if asked, joint histogram)",
                    "l2": "inputs of a request are copied from host memory at admission (no flush needed)",
-                   "max_slots": 48, "round_pairs": 1.5e9, "generation_s": t_gen},
+                   "max_slots": args.slots, "round_pairs": args.round_pairs, "generation_s": t_gen},
         "latency": {"raw_ms": {k: v * 1e3 for k, v in _percentiles(lat_b).items()},
                     "slowdown": _percentiles(slow_b),
                     "slowdown_p99_over_p50": float(np.percentile(slow_b, 99) / np.percentile(slow_b, 50)),

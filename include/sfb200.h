@@ -165,7 +165,8 @@ SFB200_API int sfb200_abi_version(void);
  * Replaces: the GPU workspace object of ext/gpu/workspace.jl:25-56. */
 SFB200_API int sfb200_ctx_create(int device, sfb200_ctx** out);
 SFB200_API int sfb200_ctx_destroy(sfb200_ctx* ctx);
-/* Last error text of this context (never NULL). */
+/* Text of the calling thread's last failed call on this context (never NULL; empty if that thread's
+ * last failure was on another context). Kept per thread, so threads sharing a context do not race. */
 SFB200_API const char* sfb200_last_error(const sfb200_ctx* ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order work. */
 SFB200_API void* sfb200_ctx_stream(sfb200_ctx* ctx);

@@ -11,6 +11,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -27,7 +28,6 @@ struct sfb200_ctx {
     int nsm = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::string err;
     // batched rounds, double-buffered so that the next round can be enqueued while one runs: per
     // buffer the work items (pinned host staging + device copy), launch counters, the graph and the
     // event recorded after the round (the buffer is free again once it has fired)
@@ -126,6 +126,30 @@ struct sfb200_plan {
 
 // ------------------------------------------------------------------------------- errors
 
+// The message of the calling thread's last failed call and the context it was made on: per thread,
+// so that threads sharing a context (slice preparation beside the round loop) never race on it.
+static thread_local std::string t_err;
+static thread_local const sfb200_ctx* t_err_ctx = nullptr;
+
+static int set_err(sfb200_ctx* ctx, int code, const char* fmt, ...);
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` (per device; never lowers it).
+// The limit is process-wide per function, and threads may configure and launch the same kernel at
+// once (slice preparation beside the round loop): lowering it could fail another thread's launch
+// between its own raise and its launch.
+static int raise_smem_limit(sfb200_ctx* ctx, const void* fn, size_t bytes)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void*, size_t> limit[64];
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = limit[ctx->device & 63][fn];
+    if (bytes <= cur) return 0;
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return set_err(ctx, SFB200_ERR_CUDA, "shared memory limit: %s", cudaGetErrorString(e));
+    cur = bytes;
+    return 0;
+}
+
 static int set_err(sfb200_ctx* ctx, int code, const char* fmt, ...)
 {
     if (ctx) {
@@ -134,7 +158,8 @@ static int set_err(sfb200_ctx* ctx, int code, const char* fmt, ...)
         va_start(ap, fmt);
         vsnprintf(buf, sizeof(buf), fmt, ap);
         va_end(ap);
-        ctx->err = buf;
+        t_err = buf;
+        t_err_ctx = ctx;
     }
     return code;
 }
@@ -154,7 +179,8 @@ extern "C" int sfb200_abi_version(void) { return SFB200_ABI_VERSION; }
 
 extern "C" const char* sfb200_last_error(const sfb200_ctx* ctx)
 {
-    return ctx ? ctx->err.c_str() : "null context";
+    if (!ctx) return "null context";
+    return t_err_ctx == ctx ? t_err.c_str() : "";
 }
 
 // ------------------------------------------------------------------------------- context
@@ -1164,7 +1190,10 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this plan");
     if (batch && T != (p->joint ? kBatchTileJoint : kBatchTile1D))
         return set_err(ctx, SFB200_ERR_UNSUPPORTED, "histogram too large for the batched kernels' fixed tiles");
-    CK(cudaFuncSetAttribute(kc.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    {
+        const int rc = raise_smem_limit(ctx, kc.fn, smem);
+        if (rc) return rc;
+    }
     int occ = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc.fn, T, smem));
     if (occ < 1) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "kernel does not fit on an SM (%zu bytes shared)", smem);
@@ -1570,7 +1599,8 @@ extern "C" int sfb200_batch_run(sfb200_ctx* ctx, int32_t n, sfb200_slice* const*
     const WorkItem* d_items = static_cast<const WorkItem*>(B.d_items);
     for (size_t l = 0; l < launches.size(); ++l) {
         Launch& L = launches[l];
-        CK(cudaFuncSetAttribute(L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+        const int rc = raise_smem_limit(ctx, L.fn, L.smem);
+        if (rc) return rc;
         L.args.items = d_items + L.item0;
         L.args.n_items = (int)L.nitems;
         L.args.counter = B.d_counters + l;

@@ -8,7 +8,9 @@ busy with all of them at once:
   minus a reserve, checked against an estimate of the request's footprint before its buffers are
   created). Admission is first come, first served, so a large request cannot be passed over forever.
 - Residency. An admitted request becomes a slice: its points are packed on the device and its
-  histogram lives there until the request completes.
+  histogram lives there until the request completes. Slices are prepared (host-to-device copy,
+  ordering, packing) on `prepare_threads` worker threads, so that preparing arrivals never holds up
+  the loop that keeps the device fed; a slice joins the rounds once it is prepared, in arrival order.
 - Rounds. Work is cut into tile pairs (independent units of up to 256 x 256 pairs). Each round gives
   every slice at least `min_units` of its remaining tile pairs, then hands out the rest of the
   round's pair budget shortest-remaining-first, and runs all of it as one batched launch (one
@@ -24,6 +26,7 @@ busy with all of them at once:
 `tests/test_serving_cpu.py` drives the same loop with a simulated executor.
 """
 import collections
+import concurrent.futures
 import threading
 import time
 from dataclasses import dataclass, field
@@ -110,9 +113,14 @@ class Server:
     """Continuous-batching loop over an executor (see the module documentation)."""
 
     def __init__(self, executor, max_slots=48, memory_reserve=1 << 30, round_pairs=1.5e9, min_units=1,
-                 depth=2, clock=time.perf_counter):
+                 depth=2, prepare_threads=1, clock=time.perf_counter):
         self.ex = executor
         self.depth = max(1, int(depth)) if hasattr(executor, "wait_oldest") else 1
+        self._prep = (concurrent.futures.ThreadPoolExecutor(int(prepare_threads), thread_name_prefix="sfb200-prep")
+                      if prepare_threads else None)
+        self._preparing = collections.deque()  # (ticket, future, bytes), in admission order
+        self._prep_bytes = 0
+        self.failed = None  # the exception that stopped the loop, if any
         self.max_slots = int(max_slots)
         self.memory_reserve = int(memory_reserve)
         self.round_pairs = float(round_pairs)
@@ -129,6 +137,9 @@ class Server:
     # ------------------------------------------------------------------ public
     def submit(self, request):
         t = Ticket(request, self.clock())
+        if self.failed is not None:  # the loop has stopped on an error
+            self._fail(t, self.failed)
+            return t
         with self._cv:
             self._pending.append(t)
             self._cv.notify()
@@ -146,37 +157,71 @@ class Server:
             self._cv.notify()
         if self._thread:
             self._thread.join()
+        if self._prep:
+            self._prep.shutdown(wait=True)
 
     def run_until_idle(self):
         """Run the loop on the calling thread until nothing is pending or active."""
         self._stop = True
         self._drain = True
-        self._loop()
+        self._loop(reraise=True)
 
     # ------------------------------------------------------------------ loop
+    def _activate(self, t, h):
+        t.t_admit = self.clock()
+        a = _Active(t, h, int(h.tile_pairs), 0, max(1.0, h.pairs / max(1, h.tile_pairs)))
+        if a.units == 0:
+            self._complete(a)
+        else:
+            self._active.append(a)
+
+    def _fail(self, t, e):  # invalid request: fail the ticket, keep serving
+        t.error = e
+        t.t_done = self.clock()
+        t._event.set()
+
+    def _harvest(self, block=False):
+        """Move prepared slices into the rounds (in admission order)."""
+        while self._preparing:
+            t, fut, need = self._preparing[0]
+            if not fut.done():
+                if not block:
+                    return
+                concurrent.futures.wait([fut], timeout=0.005)
+                if not fut.done():
+                    return
+            self._preparing.popleft()
+            self._prep_bytes -= need
+            try:
+                h = fut.result()
+            except BaseException as e:
+                self._fail(t, e)
+                continue
+            self._activate(t, h)
+            block = False
+
     def _admit(self):
+        self._harvest()
         while True:
             with self._cv:
-                if not self._pending or len(self._active) >= self.max_slots:
+                busy = len(self._active) + len(self._preparing)
+                if not self._pending or busy >= self.max_slots:
                     return
                 t = self._pending[0]
                 need = self.ex.estimate_bytes(t.request)
-                if self._active and self.ex.free_bytes() - need < self.memory_reserve:
+                if busy and self.ex.free_bytes() - self._prep_bytes - need < self.memory_reserve:
                     return  # wait for a slice to finish and free its memory
                 self._pending.popleft()
+            if self._prep is not None:
+                self._preparing.append((t, self._prep.submit(self.ex.create, t.request), need))
+                self._prep_bytes += need
+                continue
             try:
                 h = self.ex.create(t.request)
-            except BaseException as e:  # invalid request: fail the ticket, keep serving
-                t.error = e
-                t.t_done = self.clock()
-                t._event.set()
+            except BaseException as e:
+                self._fail(t, e)
                 continue
-            t.t_admit = self.clock()
-            a = _Active(t, h, int(h.tile_pairs), 0, max(1.0, h.pairs / max(1, h.tile_pairs)))
-            if a.units == 0:
-                self._complete(a)
-            else:
-                self._active.append(a)
+            self._activate(t, h)
 
     def _plan_round(self):
         """Tile-pair ranges of this round: min_units each, then shortest remaining first (over the
@@ -208,7 +253,44 @@ class Server:
         t.t_done = self.clock()
         t._event.set()
 
-    def _loop(self):
+    def _loop(self, reraise=False):
+        try:
+            self._run_loop()
+        except BaseException as e:
+            self._abort(e)  # every ticket now carries the error; the loop thread ends quietly
+            if reraise:
+                raise
+
+    def _abort(self, e):
+        """The loop failed (a device error): fail every ticket it holds instead of leaving it waiting."""
+        self.failed = e
+        try:
+            self.ex.wait_round()
+        except BaseException:
+            pass
+        tickets = [a.ticket for a in self._active]
+        for a in self._active:
+            try:
+                self.ex.destroy(a.handle)
+            except BaseException:
+                pass
+        self._active.clear()
+        for t, fut, _ in self._preparing:
+            tickets.append(t)
+            try:
+                self.ex.destroy(fut.result())
+            except BaseException:
+                pass
+        self._preparing.clear()
+        with self._cv:
+            tickets.extend(self._pending)
+            self._pending.clear()
+            self._stop = True
+        for t in tickets:
+            if not t.done():
+                self._fail(t, e)
+
+    def _run_loop(self):
         inflight = collections.deque()  # queued rounds, oldest first: lists of (active, begin, end)
         while True:
             self._admit()
@@ -238,6 +320,9 @@ class Server:
                 for a in finished:
                     self._active.remove(a)
                     self._complete(a)
+                continue
+            if self._preparing:
+                self._harvest(block=True)  # nothing to run until a prepared slice arrives
                 continue
             with self._cv:
                 if self._pending:

@@ -7,7 +7,8 @@ invariants the GPU path relies on: each tile pair of each request runs exactly o
 admission honours the slot count and the memory reserve; every admitted slice progresses in every
 round; short requests are not held behind long ones; a bad request fails alone; with pipelined
 rounds, no more than `depth` rounds are queued at once, rounds complete oldest first, and a slice is
-read only after every round that touched it has completed.
+read only after every round that touched it has completed. Each invariant holds with slices prepared
+on the loop thread and on a preparation thread (prepare_threads 0 and 1).
 """
 import collections
 import threading
@@ -42,6 +43,7 @@ class FakeExecutor:
         self.live = 0
         self.max_live = 0
         self.admissions = []  # (slices live before, free bytes after)
+        self.lock = threading.Lock()  # create runs on the preparation thread, destroy on the loop
 
     def estimate_bytes(self, req):
         return req.n * self.bpp
@@ -53,11 +55,12 @@ class FakeExecutor:
         if self.fail_n is not None and req.n == self.fail_n:
             raise ValueError("rejected")
         h = FakeHandle(req, self.estimate_bytes(req))
-        before = self.live
-        self.used += h.device_bytes
-        self.live += 1
-        self.max_live = max(self.max_live, self.live)
-        self.admissions.append((before, self.free_bytes()))
+        with self.lock:
+            before = self.live
+            self.used += h.device_bytes
+            self.live += 1
+            self.max_live = max(self.max_live, self.live)
+            self.admissions.append((before, self.free_bytes()))
         return h
 
     def run_round(self, work):
@@ -82,8 +85,9 @@ class FakeExecutor:
         return cover.astype(np.float64), np.array([h.req.n], dtype=np.uint64)
 
     def destroy(self, h):
-        self.used -= h.device_bytes
-        self.live -= 1
+        with self.lock:
+            self.used -= h.device_bytes
+            self.live -= 1
 
 
 def req(n, tag=None):
@@ -91,9 +95,10 @@ def req(n, tag=None):
     return Request((), x, x, [0.0, 1.0], tag=tag)
 
 
-def test_every_tile_pair_runs_exactly_once_in_order():
+@pytest.mark.parametrize("prep", [0, 1])
+def test_every_tile_pair_runs_exactly_once_in_order(prep):
     ex = FakeExecutor()
-    srv = Server(ex, max_slots=4, round_pairs=5e5, memory_reserve=0)
+    srv = Server(ex, max_slots=4, round_pairs=5e5, memory_reserve=0, prepare_threads=prep)
     sizes = [1, 2, 300, 1000, 5000, 20000, 700, 2, 256, 257]
     tickets = [srv.submit(req(n)) for n in sizes]
     srv.run_until_idle()
@@ -112,9 +117,10 @@ def test_every_tile_pair_runs_exactly_once_in_order():
     assert ex.live == 0 and ex.used == 0
 
 
-def test_slots_bound_concurrency():
+@pytest.mark.parametrize("prep", [0, 1])
+def test_slots_bound_concurrency(prep):
     ex = FakeExecutor()
-    srv = Server(ex, max_slots=3, round_pairs=1e5, memory_reserve=0)
+    srv = Server(ex, max_slots=3, round_pairs=1e5, memory_reserve=0, prepare_threads=prep)
     for n in [3000] * 10:
         srv.submit(req(n))
     srv.run_until_idle()
@@ -122,9 +128,11 @@ def test_slots_bound_concurrency():
     assert max(len(r) for r in ex.rounds) <= 3
 
 
-def test_memory_reserve_bounds_admission():
+@pytest.mark.parametrize("prep", [0, 1])
+def test_memory_reserve_bounds_admission(prep):
     ex = FakeExecutor(memory=2_000_000, bytes_per_point=100)
-    srv = Server(ex, max_slots=64, round_pairs=1e5, memory_reserve=500_000)
+    srv = Server(ex, max_slots=64, round_pairs=1e5, memory_reserve=500_000,
+                 prepare_threads=prep)
     ts = [srv.submit(req(5000)) for _ in range(8)]  # 500 kB each
     srv.run_until_idle()
     assert all(t.done() for t in ts)
@@ -134,17 +142,27 @@ def test_memory_reserve_bounds_admission():
     assert ex.max_live == 3
 
 
-def test_every_active_slice_progresses_each_round():
+@pytest.mark.parametrize("prep", [0, 1])
+def test_every_active_slice_progresses_each_round(prep):
     ex = FakeExecutor()
-    srv = Server(ex, max_slots=8, round_pairs=1.0, min_units=2, memory_reserve=0)  # budget ~ nothing extra
+    srv = Server(ex, max_slots=8, round_pairs=1.0, min_units=2, memory_reserve=0,  # budget ~ nothing extra
+                 prepare_threads=prep)
     for n in [4000, 6000, 8000]:
         srv.submit(req(n))
     srv.run_until_idle()
-    # while all three were active, each round advanced each of them by >= 2 units (or to its end)
-    first = ex.rounds[0]
-    assert len(first) == 3
-    for h, b, e in first:
-        assert e - b == min(2, h.tile_pairs)
+    # from the round a slice first joins until it is done, every round advances it by the minimum
+    # share (2 units, or what is left): no active slice is skipped
+    seen = {}
+    for k, rnd in enumerate(ex.rounds):
+        for h, b, e in rnd:
+            seen.setdefault(id(h), (h, k))
+            assert e - b == min(2, h.tile_pairs - b)
+    for h, k0 in seen.values():
+        k_last = max(k for k, rnd in enumerate(ex.rounds) if any(g is h for g, _, _ in rnd))
+        for k in range(k0, k_last + 1):
+            assert any(g is h for g, _, _ in ex.rounds[k]), "an active slice sat out a round"
+    if prep == 0:
+        assert len(ex.rounds[0]) == 3
 
 
 def test_short_request_overtakes_long_one():
@@ -158,9 +176,10 @@ def test_short_request_overtakes_long_one():
     assert small.t_done <= big.t_done
 
 
-def test_invalid_request_fails_alone():
+@pytest.mark.parametrize("prep", [0, 1])
+def test_invalid_request_fails_alone(prep):
     ex = FakeExecutor(fail_n=777)
-    srv = Server(ex, max_slots=4, round_pairs=1e6, memory_reserve=0)
+    srv = Server(ex, max_slots=4, round_pairs=1e6, memory_reserve=0, prepare_threads=prep)
     good = srv.submit(req(1000))
     bad = srv.submit(req(777))
     also = srv.submit(req(2000))
@@ -171,9 +190,10 @@ def test_invalid_request_fails_alone():
     assert also.wait(0)[1][0] == 2000
 
 
-def test_threaded_arrivals_complete():
+@pytest.mark.parametrize("prep", [0, 1])
+def test_threaded_arrivals_complete(prep):
     ex = FakeExecutor()
-    srv = Server(ex, max_slots=5, round_pairs=3e5, memory_reserve=0).start()
+    srv = Server(ex, max_slots=5, round_pairs=3e5, memory_reserve=0, prepare_threads=prep).start()
     rng = np.random.default_rng(4)
     sizes = rng.integers(2, 9000, 60)
     tickets = []
@@ -225,3 +245,27 @@ def test_executor_without_wait_oldest_runs_one_round_at_a_time():
     srv.run_until_idle()
     assert ex.max_inflight == 1
     assert all(np.all(t.wait(0)[0] == 1.0) for t in ts)
+
+
+class FailingExecutor(FakeExecutor):
+    """Raises from the third round on, as a device error would."""
+
+    def run_round(self, work):
+        if len(self.rounds) >= 2:
+            raise RuntimeError("device error")
+        super().run_round(work)
+
+
+@pytest.mark.parametrize("prep", [0, 1])
+def test_loop_failure_fails_every_ticket(prep):
+    ex = FailingExecutor()
+    srv = Server(ex, max_slots=2, round_pairs=1e5, memory_reserve=0, prepare_threads=prep).start()
+    tickets = [srv.submit(req(n)) for n in (6000, 7000, 8000, 9000)]
+    for t in tickets:
+        with pytest.raises(RuntimeError, match="device error"):
+            t.wait(5)
+    late = srv.submit(req(100))
+    with pytest.raises(RuntimeError, match="device error"):
+        late.wait(1)
+    srv.stop()
+    assert ex.live == 0
