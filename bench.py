@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--requests", type=int, default=2000, help="c4: number of requests")
     ap.add_argument("--rate", type=float, default=200.0, help="c4: Poisson arrival rate per second")
     ap.add_argument("--slots", type=int, default=256, help="c4: slices resident at once (admission slots)")
-    ap.add_argument("--round-pairs", type=float, default=1.5e9, help="c4: pair budget of one batched round")
+    ap.add_argument("--round-pairs", type=float, default=6e9, help="c4: pair budget of one batched round")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample length")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
