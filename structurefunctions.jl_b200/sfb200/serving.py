@@ -137,12 +137,13 @@ class Server:
     # ------------------------------------------------------------------ public
     def submit(self, request):
         t = Ticket(request, self.clock())
-        if self.failed is not None:  # the loop has stopped on an error
-            self._fail(t, self.failed)
-            return t
         with self._cv:
-            self._pending.append(t)
-            self._cv.notify()
+            failed = self.failed
+            if failed is None:
+                self._pending.append(t)
+                self._cv.notify()
+        if failed is not None:  # the loop has stopped on an error
+            self._fail(t, failed)
         return t
 
     def start(self):
@@ -263,7 +264,8 @@ class Server:
 
     def _abort(self, e):
         """The loop failed (a device error): fail every ticket it holds instead of leaving it waiting."""
-        self.failed = e
+        with self._cv:
+            self.failed = e  # from here on, submit fails new tickets itself
         try:
             self.ex.wait_round()
         except BaseException:
