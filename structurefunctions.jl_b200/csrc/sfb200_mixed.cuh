@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(256) k_flat1d_mx(const __grid_constant__ PairA
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256) k_flat1d_mx_batch(const __grid_constant__ BatchArgs b)
+__global__ void __launch_bounds__(256, OPS::n >= 4 ? 3 : 4) k_flat1d_mx_batch(const __grid_constant__ BatchArgs b)
 {
     batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { flat1d_mx_run<D, OPS, PRIV>(a, q0, q1, 1); });
 }
