@@ -280,3 +280,18 @@ def test_mixed_extreme_scales(xscale, uscale):
     vb = SF.LinearBinEdges(wj.value_bins.first_edge * uscale, wj.value_bins.last_edge * uscale, len(wj.value_bins))
     check(wj.ops, wj.x.astype(np.float64) * xscale, wj.u.astype(np.float64) * uscale,
           wj.distance_bins.edges * xscale, value_bins=vb, precision="mixed", tol=TOL_MIXED)
+
+
+@pytest.mark.parametrize("value_bins", [SF.LinearBinEdges(-1.0, 1.0, 9), SF.LinearBinEdges(-0.9, 1.1, 9)])
+def test_joint_values_near_zero(value_bins):
+    """Values a hundred times smaller than the half bin width, all in the value bins at or next to zero
+    (an edge at zero, or a bin straddling it). Every cell, down to the few-pair cells of the smallest
+    distances, must stay within 1e-6 of its sum |v|: the coarse fixed-point quantum alone bounds a
+    pair's error only by 2^-22 of the half width (3e-8 here, 2e-5 of such a value), so this exercises
+    the kernel's fine offsets near zero."""
+    rng = np.random.default_rng(17)
+    n = 1500
+    x = rng.random((2, n))
+    u = 1e-3 * rng.standard_normal((2, n))
+    edges = synthetic.log_edges(1e-3, math.sqrt(2.0), 12)
+    check((SF.ProjectedStructureFunctionType(1, 0),), x, u, edges, value_bins=value_bins)
