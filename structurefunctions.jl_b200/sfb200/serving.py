@@ -112,7 +112,7 @@ class _Active:
 class Server:
     """Continuous-batching loop over an executor (see the module documentation)."""
 
-    def __init__(self, executor, max_slots=48, memory_reserve=1 << 30, round_pairs=1.5e9, min_units=1,
+    def __init__(self, executor, max_slots=256, memory_reserve=1 << 30, round_pairs=6e9, min_units=1,
                  depth=2, prepare_threads=1, clock=time.perf_counter):
         self.ex = executor
         self.depth = max(1, int(depth)) if hasattr(executor, "wait_oldest") else 1
