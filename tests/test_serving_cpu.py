@@ -166,8 +166,10 @@ def test_every_active_slice_progresses_each_round(prep):
 
 
 def test_short_request_overtakes_long_one():
+    # the scheduling policy alone: slices prepared on the loop thread (with a preparation thread the
+    # simulated rounds, which take no time, could finish the long request before the short one is ready)
     ex = FakeExecutor()
-    srv = Server(ex, max_slots=8, round_pairs=2e6, memory_reserve=0)
+    srv = Server(ex, max_slots=8, round_pairs=2e6, memory_reserve=0, prepare_threads=0)
     big = srv.submit(req(60000))
     small = srv.submit(req(500))
     srv.run_until_idle()
