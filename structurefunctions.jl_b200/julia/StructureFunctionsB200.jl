@@ -23,7 +23,7 @@ using StructureFunctions: Calculations as SFC, StructureFunctionTypes as SFT,
 using ComputationalBackends: ComputationalBackends as CB
 using Distances: Distances as DI
 
-export B200Backend
+export B200Backend, B200Server, submit!, start!, stop!, fetch_result
 
 const LIB = Ref{String}("")
 libpath() = isempty(LIB[]) ? get(ENV, "SFB200_LIB", joinpath(@__DIR__, "..", "libsfb200.so")) : LIB[]
@@ -161,18 +161,26 @@ end
 
 # ---------------------------------------------------------------------- core call
 
-function run_pairs(b::B200Backend, sfs::Tuple, x::AbstractMatrix, u::AbstractMatrix, distance_bins,
-                   value_bins, metric, sums::Vector{Float64}, counts::Vector{UInt64}, flags::UInt32)
-    D = size(u, 1)
+# Plan description of a call; `keep` holds the tables the description points to (the library copies
+# them when the plan is created). xs, us: the inputs as contiguous column-major (W, N) / (D, N).
+function plan_desc(precision::Int32, sfs::Tuple, xs::Matrix, us::Matrix, distance_bins, value_bins, metric)
+    D = size(us, 1)
     geom, unit, radius = geometry_of(metric, D)
     keep = Any[]
-    xs = Matrix(x)   # contiguous column-major (W, N)
-    us = Matrix(u)
     ops = ntuple(k -> k <= length(sfs) ? c_op(sfs[k]) : NO_OP, 8)
     desc = CPlanDesc(geom, D, unit, radius, length(sfs), ops, distance_bins_of(keep, metric, distance_bins),
                      value_bins === nothing ? Int32(0) : Int32(1),
                      value_bins === nothing ? NO_BINS : value_bins_of(keep, value_bins),
-                     b.precision === :mixed ? Int32(1) : Int32(0), c_dtype(eltype(xs)), c_dtype(eltype(us)))
+                     precision, c_dtype(eltype(xs)), c_dtype(eltype(us)))
+    return desc, keep
+end
+
+function run_pairs(b::B200Backend, sfs::Tuple, x::AbstractMatrix, u::AbstractMatrix, distance_bins,
+                   value_bins, metric, sums::Vector{Float64}, counts::Vector{UInt64}, flags::UInt32)
+    xs = Matrix(x)   # contiguous column-major (W, N)
+    us = Matrix(u)
+    desc, keep = plan_desc(b.precision === :mixed ? Int32(1) : Int32(0), sfs, xs, us, distance_bins, value_bins,
+                           metric)
     ctx = context(b.device)
     plan = Ref{Ptr{Cvoid}}(C_NULL)
     GC.@preserve keep begin
@@ -253,5 +261,263 @@ SFC._dispatch_execution_backend(b::B200Backend, shape::SFC.AbstractFieldShape, a
     throw(ArgumentError("auxiliary-axis inputs are not implemented for B200Backend"))
 SFC._dispatch_execution_backend!(b::B200Backend, shape::SFC.AbstractFieldShape, args...; kwargs...) =
     throw(ArgumentError("in-place auxiliary-axis calculate_structure_function! is not implemented for B200Backend"))
+
+# ---------------------------------------------------------------------- serving (many requests)
+#
+# No counterpart in the reference, which computes one call at a time. A `B200Server` keeps requests
+# resident on the device as slices and runs their pairs together: a loop task admits requests in
+# arrival order while a slot is free and the device has room (sfb200_device_memory), gives every
+# active slice at least one tile pair per round and the rest of the round's pair budget
+# shortest-remaining-first, queues each round as one batched launch per kernel variant
+# (sfb200_batch_run; two rounds in flight, sfb200_batch_wait_oldest), and completes a request with its
+# own result container once all its tile pairs have run. The same loop as `sfb200.serving.Server` in
+# the Python mirror, which the test suite drives on the GPU.
+
+struct CSliceInfo
+    n_points::Int64
+    pairs::Int64
+    tile_pairs::Int64
+    device_bytes::Int64
+end
+
+struct B200Request
+    sf::Any
+    x::Matrix
+    u::Matrix
+    distance_bins::Any
+    value_bins::Any
+    metric::Any
+end
+
+mutable struct B200Ticket
+    request::B200Request
+    t_submit::Float64
+    t_done::Float64
+    result::Any
+    error::Any
+    done::Base.Event
+end
+
+mutable struct ActiveSlice
+    ticket::B200Ticket
+    slice::Ptr{Cvoid}
+    plan::Ptr{Cvoid}
+    n_sums::Int64
+    n_counts::Int64
+    units::Int64          # tile pairs in total
+    issued::Int64         # tile pairs queued so far (a prefix)
+    done::Int64           # tile pairs completed (a prefix)
+    pairs_per_unit::Float64
+end
+
+mutable struct B200Server
+    device::Int
+    max_slots::Int
+    memory_reserve::Int64
+    round_pairs::Float64
+    min_units::Int
+    pending::Vector{B200Ticket}
+    active::Vector{ActiveSlice}
+    plans::Dict{Any, Ptr{Cvoid}}
+    lock::ReentrantLock
+    stopping::Bool
+    task::Union{Nothing, Task}
+    rounds::Int
+end
+
+"""
+    B200Server(; device = 0, max_slots = 256, memory_reserve = 1 << 30, round_pairs = 6e9, min_units = 1)
+
+A request loop over one device (mixed precision). `start!` it, `submit!` requests (the arguments of
+`calculate_structure_function`), `fetch_result` a ticket, `stop!` it when done.
+"""
+B200Server(; device::Integer = 0, max_slots::Integer = 256, memory_reserve::Integer = 1 << 30,
+           round_pairs::Real = 6e9, min_units::Integer = 1) =
+    B200Server(Int(device), Int(max_slots), Int64(memory_reserve), Float64(round_pairs), Int(min_units),
+               B200Ticket[], ActiveSlice[], Dict{Any, Ptr{Cvoid}}(), ReentrantLock(), false, nothing, 0)
+
+function submit!(srv::B200Server, sf, x::AbstractMatrix, u::AbstractMatrix, distance_bins, value_bins = nothing;
+                 distance_metric::DI.PreMetric = DI.Euclidean())
+    t = B200Ticket(B200Request(sf, Matrix(x), Matrix(u), distance_bins, value_bins, distance_metric), time(),
+                   NaN, nothing, nothing, Base.Event())
+    lock(() -> push!(srv.pending, t), srv.lock)
+    return t
+end
+
+"""The request's result container (`StructureFunctionSumsAndCounts` or `...2DSumsAndCounts`)."""
+function fetch_result(t::B200Ticket)
+    wait(t.done)
+    t.error === nothing || throw(t.error)
+    return t.result
+end
+
+start!(srv::B200Server) = (srv.task = Threads.@spawn serve_loop(srv); srv)
+
+function stop!(srv::B200Server)
+    lock(() -> (srv.stopping = true), srv.lock)
+    srv.task === nothing || wait(srv.task)
+    for plan in values(srv.plans)
+        ccall((:sfb200_plan_destroy, libpath()), Cint, (Ptr{Cvoid},), plan)
+    end
+    empty!(srv.plans)
+    return nothing
+end
+
+function fail!(t::B200Ticket, err)
+    t.error = err
+    t.t_done = time()
+    notify(t.done)
+end
+
+function free_bytes(ctx)
+    f = Ref{Int64}(0)
+    total = Ref{Int64}(0)
+    check(ccall((:sfb200_device_memory, libpath()), Cint, (Ptr{Cvoid}, Ref{Int64}, Ref{Int64}), ctx, f, total), ctx)
+    return f[]
+end
+
+# device bytes of a slice: raw and packed points, ordering keys and the histogram (an estimate)
+estimate_bytes(r::B200Request) = Int64(size(r.x, 2)) * (8 * (size(r.x, 1) + 2 * size(r.u, 1)) + 136) + (1 << 20)
+
+function create_slice(srv::B200Server, ctx, t::B200Ticket)
+    r = t.request
+    key = (typeof(r.sf), r.sf, size(r.u, 1), r.metric, collect(r.distance_bins),
+           r.value_bins === nothing ? nothing : collect(r.value_bins), eltype(r.x), eltype(r.u))
+    plan = get!(srv.plans, key) do
+        desc, keep = plan_desc(Int32(1), (r.sf,), r.x, r.u, r.distance_bins, r.value_bins, r.metric)
+        p = Ref{Ptr{Cvoid}}(C_NULL)
+        GC.@preserve keep begin
+            check(ccall((:sfb200_plan_create, libpath()), Cint, (Ptr{Cvoid}, Ref{CPlanDesc}, Ref{Ptr{Cvoid}}),
+                        ctx, desc, p), ctx)
+        end
+        p[]
+    end
+    ns, nc = Ref{Int64}(0), Ref{Int64}(0)
+    check(ccall((:sfb200_plan_output_sizes, libpath()), Cint, (Ptr{Cvoid}, Ref{Int64}, Ref{Int64}), plan, ns, nc), ctx)
+    sl = Ref{Ptr{Cvoid}}(C_NULL)
+    GC.@preserve r begin
+        check(ccall((:sfb200_slice_create, libpath()), Cint,
+                    (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Int64, UInt32, Ptr{Cvoid}, Ref{Ptr{Cvoid}}),
+                    plan, r.x, r.u, size(r.x, 2), UInt32(0), C_NULL, sl), ctx)
+    end
+    info = Ref(CSliceInfo(0, 0, 0, 0))
+    check(ccall((:sfb200_slice_get_info, libpath()), Cint, (Ptr{Cvoid}, Ref{CSliceInfo}), sl[], info), ctx)
+    units = info[].tile_pairs
+    return ActiveSlice(t, sl[], plan, ns[], nc[], units, 0, 0, max(1.0, info[].pairs / max(1, units)))
+end
+
+function complete!(ctx, a::ActiveSlice)
+    t = a.ticket
+    r = t.request
+    try
+        sums = zeros(Float64, a.n_sums)
+        counts = zeros(UInt64, a.n_counts)
+        check(ccall((:sfb200_slice_read, libpath()), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{UInt64}, UInt32, Ptr{Cvoid}), a.slice, sums, counts, UInt32(0),
+                    C_NULL), ctx)
+        T = out_type(r.x, r.u)
+        if r.value_bins === nothing
+            t.result = SFO.StructureFunctionSumsAndCounts(r.sf, r.distance_bins, T.(sums), UInt32.(counts))
+        else
+            nd, nv = length(r.distance_bins) - 1, length(r.value_bins) - 1
+            t.result = SFO.StructureFunction2DSumsAndCounts(r.sf, r.distance_bins, r.value_bins,
+                reshape(T.(sums), nd, nv), reshape(UInt32.(counts), nd, nv))
+        end
+    catch err
+        t.error = err
+    finally
+        ccall((:sfb200_slice_destroy, libpath()), Cint, (Ptr{Cvoid},), a.slice)
+    end
+    t.t_done = time()
+    notify(t.done)
+end
+
+function admit!(srv::B200Server, ctx)
+    while true
+        t = lock(srv.lock) do
+            (isempty(srv.pending) || length(srv.active) >= srv.max_slots) && return nothing
+            head = srv.pending[1]
+            if !isempty(srv.active) && free_bytes(ctx) - estimate_bytes(head.request) < srv.memory_reserve
+                return nothing  # wait for a slice to finish and free its memory
+            end
+            popfirst!(srv.pending)
+        end
+        t === nothing && return nothing
+        try
+            a = create_slice(srv, ctx, t)
+            a.units == 0 ? complete!(ctx, a) : push!(srv.active, a)
+        catch err
+            fail!(t, err)
+        end
+    end
+end
+
+remaining(a::ActiveSlice) = a.units - a.issued
+
+function plan_round(srv::B200Server)
+    ready = filter(a -> remaining(a) > 0, srv.active)
+    give = Dict{ActiveSlice, Int64}(a => min(remaining(a), srv.min_units) for a in ready)
+    budget = srv.round_pairs - sum((give[a] * a.pairs_per_unit for a in ready); init = 0.0)
+    for a in sort(ready; by = a -> remaining(a) * a.pairs_per_unit)
+        budget <= 0 && break
+        extra = min(remaining(a) - give[a], floor(Int64, budget / a.pairs_per_unit) + 1)
+        if extra > 0
+            give[a] += extra
+            budget -= extra * a.pairs_per_unit
+        end
+    end
+    return [(a, a.issued, a.issued + give[a]) for a in ready if give[a] > 0]
+end
+
+function serve_loop(srv::B200Server)
+    ctx = context(srv.device)
+    inflight = Vector{Vector{Tuple{ActiveSlice, Int64, Int64}}}()
+    try
+        while true
+            admit!(srv, ctx)
+            if length(inflight) < 2 && any(a -> remaining(a) > 0, srv.active)
+                work = plan_round(srv)
+                slices = Ptr{Cvoid}[w[1].slice for w in work]
+                lo = Int64[w[2] for w in work]
+                hi = Int64[w[3] for w in work]
+                check(ccall((:sfb200_batch_run, libpath()), Cint,
+                            (Ptr{Cvoid}, Int32, Ptr{Ptr{Cvoid}}, Ptr{Int64}, Ptr{Int64}, Ptr{Cvoid}),
+                            ctx, length(work), slices, lo, hi, C_NULL), ctx)
+                for (a, _, e) in work
+                    a.issued = e
+                end
+                push!(inflight, work)
+                srv.rounds += 1
+                continue
+            end
+            if !isempty(inflight)
+                check(ccall((:sfb200_batch_wait_oldest, libpath()), Cint, (Ptr{Cvoid}, Ptr{Int64}), ctx, C_NULL), ctx)
+                for (a, _, e) in popfirst!(inflight)
+                    a.done = e
+                    if a.done >= a.units
+                        filter!(b -> b !== a, srv.active)
+                        complete!(ctx, a)
+                    end
+                end
+                continue
+            end
+            idle = lock(() -> (isempty(srv.pending), srv.stopping), srv.lock)
+            idle[1] && idle[2] && return nothing
+            sleep(0.001)
+        end
+    catch err
+        # a failed round fails every request the loop holds, instead of leaving it waiting
+        ccall((:sfb200_batch_wait, libpath()), Cint, (Ptr{Cvoid},), ctx)
+        for a in srv.active
+            ccall((:sfb200_slice_destroy, libpath()), Cint, (Ptr{Cvoid},), a.slice)
+            fail!(a.ticket, err)
+        end
+        empty!(srv.active)
+        for t in lock(() -> splice!(srv.pending, 1:length(srv.pending)), srv.lock)
+            fail!(t, err)
+        end
+        rethrow()
+    end
+end
 
 end # module
