@@ -287,8 +287,10 @@ SFB200_API int sfb200_device_memory(sfb200_ctx* ctx, int64_t* free_bytes, int64_
  * 1D plans of precision MIXED or FP64 only, at most 65536 points, at most 32768 sums (bins x
  * operators) and 4096 bins; larger calls return SFB200_ERR_UNSUPPORTED. Points are taken in the
  * caller's order. x, u, sums and counts are device pointers; flags may only hold
- * SFB200_RUN_ACCUMULATE. The first call on a device looks up the scratch array's device address (and
- * loads the kernels it uses), so make that first call before any stream capture. All calls on one
+ * SFB200_RUN_ACCUMULATE. The first call on a context looks up the scratch array's device address
+ * (and loads the kernels it uses), so make that first call before any stream capture; the context
+ * keeps the address, and a device reset (cudaDeviceReset) invalidates it together with every other
+ * context resource: destroy and re-create the context after one. All calls on one
  * device share the scratch: calls that overlap on the GPU (from several streams or threads) race on
  * it and must be serialised by the caller. */
 SFB200_API int sfb200_run_noalloc(sfb200_plan* plan, const void* x, const void* u, int64_t n, uint32_t flags,

@@ -55,6 +55,7 @@ struct sfb200_ctx {
     cudaEvent_t join[kLanes] = {};
     cudaStream_t prep_stream = nullptr;  // slice preparation, overlapping the running round
     cudaStream_t side_stream = nullptr;  // reads and frees of finished slices (not behind later rounds)
+    void* noalloc_ptr = nullptr;  // device address of the no-allocation scratch (looked up on first use)
 };
 
 // Device buffers of one run over n <= cap points: raw inputs, the packed SoA layout, the point
@@ -85,8 +86,8 @@ struct sfb200_plan {
     sfb200_ctx* ctx = nullptr;
     sfb200_plan_desc desc{};
     bool sphere = false, joint = false;
-    bool mixed = false;  // precision FP32: FP32-bulk kernels with the FP64 recheck
-    bool mx = false;     // precision MIXED: FP64 differences / numerators, FP32 normalisation + accumulation
+    bool fp32 = false;   // precision FP32: FP32-bulk kernels with the FP64 recheck
+    bool mixed = false;  // precision MIXED: FP64 differences / numerators, FP32 normalisation + accumulation
     bool df = false;  // FP32 records carry (hi, lo) pairs (an input is FP64, or the sphere basis)
     bool l_only = false;  // the joint value depends on du_L only (compensated in FP32)
     int D = 0, W = 0, nb = 0, nv = 0, nops = 0, nops_pad = 0, opl = 0, vorder = 1;
@@ -520,10 +521,10 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "unknown precision %d", d.precision);
     if ((d.x_dtype != SFB200_F64 && d.x_dtype != SFB200_F32) || (d.u_dtype != SFB200_F64 && d.u_dtype != SFB200_F32))
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "x_dtype/u_dtype must be F64 or F32");
-    p->mixed = d.precision == SFB200_PREC_FP32;
-    p->mx = d.precision == SFB200_PREC_MIXED;
+    p->fp32 = d.precision == SFB200_PREC_FP32;
+    p->mixed = d.precision == SFB200_PREC_MIXED;
     p->joint = d.joint != 0;
-    p->df = p->mixed && (p->sphere || d.x_dtype == SFB200_F64 || d.u_dtype == SFB200_F64);
+    p->df = p->fp32 && (p->sphere || d.x_dtype == SFB200_F64 || d.u_dtype == SFB200_F64);
     if (d.n_ops < 1 || d.n_ops > SFB200_MAX_OPS)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "n_ops must be in 1..%d", SFB200_MAX_OPS);
     if (p->joint && d.n_ops != 1)
@@ -587,7 +588,7 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
                                "distance_bins: Euclidean edges must be non-negative (their squares must stay sorted)");
     }
     // edge keys of the FP32 path (and the chord keys of the mixed sphere path)
-    if (p->mixed || (p->mx && p->sphere)) {
+    if (p->fp32 || (p->mixed && p->sphere)) {
         p->ck.resize(db.n_edges);
         for (int k = 0; k < db.n_edges; ++k) {
             double r = dlinear ? std::fma((double)k, db.step, db.first) : db.edges[k];
@@ -599,7 +600,7 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
                 p->ck[k] = p->exact_tab[k];
             }
         }
-        if (p->mixed && !geom_lut32(p->ck, p->lg32))
+        if (p->fp32 && !geom_lut32(p->ck, p->lg32))
             return set_err(ctx, SFB200_ERR_UNSUPPORTED,
                            "distance edges outside the FP32 range of the fp32 kernel; use precision=mixed or fp64");
         const double u32 = 0x1p-24, u64 = 0x1p-53;
@@ -629,7 +630,7 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         if (d.value.kind == SFB200_BINS_LINEAR) p->vlin = linear_of(d.value);
         else p->vedges.assign(d.value.edges, d.value.edges + d.value.n_edges);
     }
-    if (p->joint && (p->mixed || p->mx)) {
+    if (p->joint && (p->fp32 || p->mixed)) {
         // fixed-point scale of the value offsets from the bin centres: 2^k with (half width) 2^k < 2^30
         double hw = 0.0;
         if (d.value.kind == SFB200_BINS_LINEAR) {
@@ -676,25 +677,25 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
     cudaError_t e;
     if (!p->exact_tab.empty() && (e = upload(&p->d_exact, p->exact_tab.data(), p->exact_tab.size())) != cudaSuccess)
         return cuda_fail(ctx, e, "upload distance table");
-    if (p->mx && p->sphere) {
+    if (p->mixed && p->sphere) {
         std::vector<LutEntry64> lut;
         build_lut64(p->ck, p->lg64, lut, kChordWrel);
         p->lut64_bytes = (int)(lut.size() * sizeof(LutEntry64));
         if ((e = upload(&p->d_lut64, lut.data(), lut.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload table");
-    } else if (!dlinear && !p->mixed) {
+    } else if (!dlinear && !p->fp32) {
         std::vector<LutEntry64> lut;
         build_lut64(p->exact_tab, p->lg64, lut);
         p->lut64_bytes = (int)(lut.size() * sizeof(LutEntry64));
         if ((e = upload(&p->d_lut64, lut.data(), lut.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload table");
     }
-    if (p->mixed) {
+    if (p->fp32) {
         if ((e = upload(&p->d_ck, p->ck.data(), p->ck.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload keys");
         if ((e = cudaMalloc(&p->d_lut32, sizeof(LutEntry32) * p->lg32.ncell)) != cudaSuccess)
             return cuda_fail(ctx, e, "alloc table");
     }
     if (!p->vedges.empty() && (e = upload(&p->d_vedges, p->vedges.data(), p->vedges.size())) != cudaSuccess)
         return cuda_fail(ctx, e, "upload value edges");
-    if (p->joint && p->mixed) {
+    if (p->joint && p->fp32) {
         std::vector<double> rowlo(p->nb + 2, 0.0);
         for (int b = 1; b <= p->nb; ++b) rowlo[b] = std::max(p->ck[b - 1], 0.0);
         if ((e = upload(&p->d_rowlo, rowlo.data(), rowlo.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload rows");
@@ -711,13 +712,13 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
 
     // the kernel exists for this combination
     KernelChoice kc;
-    if (p->mx)
+    if (p->mixed)
         kc = p->joint ? pick_joint_mx(p->sphere, p->D, p->opl)
                       : (p->sphere ? pick_sphere1d_mx(p->D, p->opl, 0) : pick_flat1d_mx(p->D, p->opl, 0));
     else
-        kc = p->joint ? pick_joint(p->sphere, p->D, p->mixed, true, p->df, p->opl)
-                      : (p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, 0)
-                                   : pick_flat1d(p->D, p->mixed, p->df, p->opl, 0));
+        kc = p->joint ? pick_joint(p->sphere, p->D, p->fp32, true, p->df, p->opl)
+                      : (p->sphere ? pick_sphere1d(p->D, p->fp32, p->opl, 0)
+                                   : pick_flat1d(p->D, p->fp32, p->df, p->opl, 0));
     if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this operator on the joint mixed path");
     return SFB200_OK;
 }
@@ -809,11 +810,11 @@ static int workspace_layout(sfb200_plan* p, Workspace& w, long long cap, bool ou
     CK(alloc(&w.d_rawu, sizeof(double) * p->D * cap));
     CK(alloc((void**)&w.d_X64, sizeof(double) * nx64 * cap));
     CK(alloc((void**)&w.d_U64, sizeof(double) * p->D * cap));
-    if (p->mixed) {
+    if (p->fp32) {
         CK(alloc((void**)&w.d_XF, sizeof(float) * nxf * cap));
         if (!p->sphere) CK(alloc((void**)&w.d_UF, sizeof(float) * (p->df ? 2 : 1) * p->D * cap));
     }
-    if (p->mx && p->sphere) CK(alloc((void**)&w.d_XM, sizeof(double) * 10 * cap));
+    if (p->mixed && p->sphere) CK(alloc((void**)&w.d_XM, sizeof(double) * 10 * cap));
     CK(alloc((void**)&w.d_keys, sizeof(unsigned) * 2 * cap));
     CK(alloc((void**)&w.d_perm, sizeof(int) * 2 * cap));
     CK(alloc((void**)&w.d_box, sizeof(unsigned) * 6));
@@ -893,12 +894,12 @@ static void launch_pack(sfb200_plan* p, Workspace& w, const void* x, const void*
     const int tb = 256, nblk = (n + tb - 1) / tb;
     if (p->sphere)
         k_pack_sphere<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->desc.angle_unit, perm,
-                                                  w.d_X64, w.d_U64, p->mixed ? w.d_XF : nullptr,
-                                                  p->mx ? w.d_XM : nullptr, w.d_aux + 1);
+                                                  w.d_X64, w.d_U64, p->fp32 ? w.d_XF : nullptr,
+                                                  p->mixed ? w.d_XM : nullptr, w.d_aux + 1);
     else
         k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->df, perm, w.d_X64,
-                                                w.d_U64, p->mixed ? w.d_XF : nullptr,
-                                                p->mixed ? w.d_UF : nullptr, w.d_aux + 1);
+                                                w.d_U64, p->fp32 ? w.d_XF : nullptr,
+                                                p->fp32 ? w.d_UF : nullptr, w.d_aux + 1);
 }
 
 // Points below this count keep the caller's order: the sort costs more than the runs it lengthens.
@@ -979,7 +980,7 @@ static size_t hist_bytes(bool fp32, int NV, int priv, int NW, int NBP, int lc)
 static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_hist, int priv, int lc = 32)
 {
     const int NW = T / 32, NBP = p->nb + 2, NV = p->nops_pad;
-    if (p->mx) {
+    if (p->mixed) {
         const int rec = p->sphere ? 10 : 2 * p->D;  // doubles per j record
         if (p->joint)
             return (size_t)lut_bytes + (size_t)rec * T * 8 + ((size_t)p->nb * p->nv + (size_t)p->nb * p->nfine) * 8 +
@@ -988,14 +989,14 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
     }
     if (p->joint) {
         const long long ncell = (long long)p->nb * p->nv;
-        if (!p->mixed) {
+        if (!p->fp32) {
             const int nx = p->sphere ? 8 : p->D;
             return (size_t)(nx + p->D) * T * 8 + (smem_hist ? (size_t)ncell * 12 : 0);
         }
         const int nx = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 4 : 2) * p->D;
         return (size_t)lut_bytes + (size_t)nx * T * 4 + (size_t)ncell * 12 + (size_t)(p->nb + 2) * 4;
     }
-    if (!p->mixed) {
+    if (!p->fp32) {
         const int nx = p->sphere ? 8 : p->D;
         return (size_t)lut_bytes + (size_t)(nx + p->D) * T * 8 + hist_bytes(false, NV, priv, NW, NBP, lc);
     }
@@ -1058,7 +1059,7 @@ static int prepare_inputs(sfb200_plan* p, Workspace& w, const void* x, const voi
     else launch_pack<float, float>(p, w, xin, uin, (int)n, perm, s);
     ++*launches;
     CK(cudaGetLastError());
-    if (p->mixed) {
+    if (p->fp32) {
         k_build_lut32<<<(p->lg32.ncell + 127) / 128, 128, 0, s>>>(p->d_ck, (int)p->ck.size(), p->wp, p->lg32,
                                                                 w.d_aux + 1, p->d_lut32);
         ++*launches;
@@ -1106,8 +1107,8 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     sfb200_ctx* ctx = p->ctx;
     const bool dlinear = p->desc.distance.kind == SFB200_BINS_LINEAR;
     int lut_bytes = 0;
-    if (p->mixed) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
-    else if (p->mx) lut_bytes = p->lut64_bytes;  // exact table (flat) or chord table (sphere); 0 if linear
+    if (p->fp32) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
+    else if (p->mixed) lut_bytes = p->lut64_bytes;  // exact table (flat) or chord table (sphere); 0 if linear
     else if (!dlinear && !p->joint) lut_bytes = p->lut64_bytes;
     int T;
     bool smem_hist = true;
@@ -1121,32 +1122,32 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
         T = p->tile_ovr ? p->tile_ovr : (n >= 32768 ? 512 : (n >= 4096 ? 256 : 64));
         if (batch) T = kBatchTileJoint;
         smem = smem_bytes(p, T, lut_bytes, true, 0);
-        while (p->mx && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr) {
+        while (p->mixed && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr) {
             T /= 2;
             smem = smem_bytes(p, T, lut_bytes, true, 0);
         }
         if (smem > (size_t)dev_smem_max) {
-            if (p->mixed || p->mx)
+            if (p->fp32 || p->mixed)
                 return set_err(ctx, SFB200_ERR_UNSUPPORTED,
                                "joint histogram of %d x %d cells does not fit shared memory on the mixed path; use fp64",
                                p->nb, p->nv);
             smem_hist = false;
             smem = smem_bytes(p, T, lut_bytes, false, 0);
         }
-        kc = p->mx ? (batch ? pick_joint_mx_batch(p->sphere, p->D, p->opl) : pick_joint_mx(p->sphere, p->D, p->opl))
-                   : pick_joint(p->sphere, p->D, p->mixed, smem_hist, p->df, p->opl);
+        kc = p->mixed ? (batch ? pick_joint_mx_batch(p->sphere, p->D, p->opl) : pick_joint_mx(p->sphere, p->D, p->opl))
+                   : pick_joint(p->sphere, p->D, p->fp32, smem_hist, p->df, p->opl);
         // block cells hold at most 2^31 pairs between flushes (T^2 pairs per tile pair); the mixed
         // kernel's packed cells fewer than 2^20
-        flush_every = (int)std::max<long long>(1, (p->mx ? (1ll << 20) - 1 : (1ll << 31)) / ((long long)T * T));
+        flush_every = (int)std::max<long long>(1, (p->mixed ? (1ll << 20) - 1 : (1ll << 31)) / ((long long)T * T));
     } else {
         const int want = p->priv_ovr >= 0 ? p->priv_ovr : default_privatization(p);
-        if (p->mx && batch)
+        if (p->mixed && batch)
             kc = p->sphere ? pick_sphere1d_mx_batch(p->D, p->opl) : pick_flat1d_mx_batch(p->D, p->opl);
-        else if (p->mx)
+        else if (p->mixed)
             kc = p->sphere ? pick_sphere1d_mx(p->D, p->opl, want) : pick_flat1d_mx(p->D, p->opl, want);
         else
-            kc = p->sphere ? pick_sphere1d(p->D, p->mixed, p->opl, want)
-                           : pick_flat1d(p->D, p->mixed, p->df, p->opl, want);
+            kc = p->sphere ? pick_sphere1d(p->D, p->fp32, p->opl, want)
+                           : pick_flat1d(p->D, p->fp32, p->df, p->opl, want);
         if (batch) {
             T = kBatchTile1D;
         } else if (p->tile_ovr) {
@@ -1180,11 +1181,11 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
         if (kc.priv == 3) {
             // FP32 table cells are folded into FP64 before any of them holds more than ~4096
             // pair terms (NW warps x T steps per tile pair add into one column)
-            flush_every = (p->mixed || p->mx) ? std::max(1, 4096 / ((T / 32) * T)) : 64;
+            flush_every = (p->fp32 || p->mixed) ? std::max(1, 4096 / ((T / 32) * T)) : 64;
         } else if (kc.priv > 0) {
             // FP32 copies are folded into FP64 before any lane-bin cell can hold more than ~512 terms
             const int copies = kc.priv == 2 ? 1 : kc.priv;
-            flush_every = (p->mixed || p->mx) ? std::max(1, 512 * copies / (32 * T)) : 64;
+            flush_every = (p->fp32 || p->mixed) ? std::max(1, 512 * copies / (32 * T)) : 64;
         }
     }
     if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this plan");
@@ -1201,7 +1202,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     const long long ntp = tile_pairs(n, T);
     const long long grid = std::min<long long>(ntp, (long long)ctx->nsm * occ);
     // the warp-aggregated FP32 histogram counts in 32 bits per warp and bin without folding
-    if (!p->joint && kc.priv == 0 && (p->mixed || p->mx) && ((ntp + grid - 1) / grid) * 32ll * T >= (1ll << 32))
+    if (!p->joint && kc.priv == 0 && (p->fp32 || p->mixed) && ((ntp + grid - 1) / grid) * 32ll * T >= (1ll << 32))
         return set_err(ctx, SFB200_ERR_UNSUPPORTED,
                        "privatization 0 would overflow its 32-bit counters at %lld points; use another", n);
 
@@ -1214,8 +1215,8 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     a.XF = w.d_XF;
     a.UF = w.d_UF;
     a.XM = w.d_XM;
-    a.lut = p->mixed ? (const void*)p->d_lut32 : (const void*)p->d_lut64;
-    a.lg = p->mixed ? p->lg32 : p->lg64;
+    a.lut = p->fp32 ? (const void*)p->d_lut32 : (const void*)p->d_lut64;
+    a.lg = p->fp32 ? p->lg32 : p->lg64;
     a.chord_wrel = kChordWrel;
     a.chord_short = 0x1p-40;         // (near-)coincident: the reference frame is degenerate
     a.chord_anti = 4.0 - 0x1p-40;    // (near-)antipodal: likewise
@@ -1239,7 +1240,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     // the rounding of t itself (the rest is in the per-row absolute window)
     a.vrel = (float)((p->l_only ? (6.0 * p->vorder + 6.0) * 1.25 : 4.0) * 0x1p-24);
     // mixed: the FP32 value carries ~5 ulps per order of L / T (conversion, rsqrtf, scaling)
-    if (p->mx) a.vrel = (float)((5.0 * p->vorder + 3.0) * 1.25 * 0x1p-24);
+    if (p->mixed) a.vrel = (float)((5.0 * p->vorder + 3.0) * 1.25 * 0x1p-24);
     a.vq = p->vq;
     a.vq_inv = p->vq_inv;
     a.vqc = p->vqc;
@@ -1388,7 +1389,7 @@ extern "C" int sfb200_slice_create(sfb200_plan* p, const void* x, const void* u,
     if (!p || !out) return SFB200_ERR_INVALID_ARG;
     sfb200_ctx* ctx = p->ctx;
     *out = nullptr;
-    if (!p->mx) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "batched slices need a plan of precision MIXED");
+    if (!p->mixed) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "batched slices need a plan of precision MIXED");
     if (n < 0) return set_err(ctx, SFB200_ERR_INVALID_ARG, "negative point count");
     if (n > (1ll << 31) - 1024) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "more than 2^31 points");
     if (n > 0 && (!x || !u)) return set_err(ctx, SFB200_ERR_INVALID_ARG, "x/u pointer is NULL");
@@ -1738,23 +1739,23 @@ static constexpr long long kNoAllocWords =                         // 8-byte wor
 // 3.4 MiB, held by every device that loads the library: X64 (D x N), U64 (D x N), sums, counts, aux
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
 
-static std::mutex g_noalloc_mutex;
-static void* g_noalloc_ptr[64] = {};  // per device, looked up once with that device current
-
 // Device address of the scratch array on ctx's device (which the caller has made current). The
-// first call on a device looks it up; later calls reuse it. Host code only ever passes this address
-// to kernels: the array's name on the host is a host-side stand-in, not a device address.
+// first call on a context looks it up and the context keeps it: a context lives on one device, and a
+// device reset, which would move the array, invalidates the context with it. Host code only ever
+// passes this address to kernels: the array's name on the host is a host-side stand-in, not a device
+// address.
+static std::mutex g_noalloc_mutex;  // threads sharing a context look the address up once
+
 static int noalloc_scratch(sfb200_ctx* ctx, void** out)
 {
-    if (ctx->device < 0 || ctx->device >= 64) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "device ordinal above 63");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[ctx->device]) {
+    if (!ctx->noalloc_ptr) {
         void* ptr = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (e != cudaSuccess || !ptr) return cuda_fail(ctx, e, "scratch address");
-        g_noalloc_ptr[ctx->device] = ptr;
+        ctx->noalloc_ptr = ptr;
     }
-    *out = g_noalloc_ptr[ctx->device];
+    *out = ctx->noalloc_ptr;
     return SFB200_OK;
 }
 
@@ -1763,7 +1764,7 @@ extern "C" int sfb200_run_noalloc(sfb200_plan* p, const void* x, const void* u, 
 {
     if (!p) return SFB200_ERR_INVALID_ARG;
     sfb200_ctx* ctx = p->ctx;
-    if (p->sphere || p->joint || p->mixed)
+    if (p->sphere || p->joint || p->fp32)
         return set_err(ctx, SFB200_ERR_UNSUPPORTED, "sfb200_run_noalloc takes flat 1D plans of precision MIXED or FP64");
     if (flags & ~SFB200_RUN_ACCUMULATE)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "sfb200_run_noalloc: inputs and outputs are device pointers; "

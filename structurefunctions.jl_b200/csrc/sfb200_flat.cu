@@ -4,7 +4,7 @@
 
 namespace sfb {
 
-template <int D, int MODE, class OPS, int PRIV>  // MODE 0: FP64, 1: mixed FP32 inputs, 2: mixed FP64 inputs
+template <int D, int MODE, class OPS, int PRIV>  // MODE 0: FP64, 1: FP32-bulk on FP32 inputs, 2: FP32-bulk on FP64 inputs
 static KernelChoice flat_kernel()
 {
     if constexpr (MODE == 1) return {reinterpret_cast<const void*>(&k_flat1d_mixed<D, false, false, OPS, PRIV>), 256, PRIV};
@@ -45,9 +45,9 @@ static KernelChoice flat_by_list(int opl, int priv)
     return {nullptr, 0, 0};
 }
 
-KernelChoice pick_flat1d(int D, bool mixed, bool df, int opl, int priv)
+KernelChoice pick_flat1d(int D, bool fp32, bool df, int opl, int priv)
 {
-    const int mode = mixed ? (df ? 2 : 1) : 0;
+    const int mode = fp32 ? (df ? 2 : 1) : 0;
     if (D == 2)
         return mode == 0 ? flat_by_list<2, 0>(opl, priv)
                          : (mode == 1 ? flat_by_list<2, 1>(opl, priv) : flat_by_list<2, 2>(opl, priv));

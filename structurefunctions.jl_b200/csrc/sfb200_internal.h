@@ -29,12 +29,12 @@ struct KernelChoice {
     int priv;         // histogram privatization depth the kernel was built with (1D kernels)
 };
 
-// Kernel lookup: returns nullptr fn for an unsupported combination. `mixed` here selects the
+// Kernel lookup: returns nullptr fn for an unsupported combination. `fp32` selects the
 // FP32-bulk kernels (precision SFB200_PREC_FP32); `df`: their FP32 records carry (hi, lo) pairs
 // because an input is FP64.
-KernelChoice pick_flat1d(int D, bool mixed, bool df, int opl, int priv);
-KernelChoice pick_sphere1d(int D, bool mixed, int opl, int priv);
-KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, bool df, int opl);
+KernelChoice pick_flat1d(int D, bool fp32, bool df, int opl, int priv);
+KernelChoice pick_sphere1d(int D, bool fp32, int opl, int priv);
+KernelChoice pick_joint(bool sphere, int D, bool fp32, bool smem_hist, bool df, int opl);
 // Mixed-precision kernels (FP64 differences and numerators, FP32 normalisation and accumulation).
 KernelChoice pick_flat1d_mx(int D, int opl, int priv);
 KernelChoice pick_sphere1d_mx(int D, int opl, int priv);

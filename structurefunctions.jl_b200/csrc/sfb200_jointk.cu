@@ -23,9 +23,9 @@ static KernelChoice joint_mixed(int opl)
     return {nullptr, 0, 0};
 }
 
-KernelChoice pick_joint(bool sphere, int D, bool mixed, bool smem_hist, bool df, int opl)
+KernelChoice pick_joint(bool sphere, int D, bool fp32, bool smem_hist, bool df, int opl)
 {
-    if (!mixed) {
+    if (!fp32) {
         if (sphere) return D == 2 ? joint_fp64<true, 2>(smem_hist) : joint_fp64<true, 3>(smem_hist);
         return D == 2 ? joint_fp64<false, 2>(smem_hist) : joint_fp64<false, 3>(smem_hist);
     }

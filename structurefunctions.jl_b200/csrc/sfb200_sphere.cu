@@ -42,10 +42,10 @@ static KernelChoice sphere_by_list(int opl, int priv)
     return {nullptr, 0, 0};
 }
 
-KernelChoice pick_sphere1d(int D, bool mixed, int opl, int priv)
+KernelChoice pick_sphere1d(int D, bool fp32, int opl, int priv)
 {
-    if (D == 2) return mixed ? sphere_by_list<2, true>(opl, priv) : sphere_by_list<2, false>(opl, priv);
-    if (D == 3) return mixed ? sphere_by_list<3, true>(opl, priv) : sphere_by_list<3, false>(opl, priv);
+    if (D == 2) return fp32 ? sphere_by_list<2, true>(opl, priv) : sphere_by_list<2, false>(opl, priv);
+    if (D == 3) return fp32 ? sphere_by_list<3, true>(opl, priv) : sphere_by_list<3, false>(opl, priv);
     return {nullptr, 0, 0};
 }
 

@@ -88,6 +88,50 @@ def test_noalloc_matches_run_on_two_calls(precision, name, n):
         ctx.close()
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_noalloc_at_the_scratch_limit_allocates_nothing(precision):
+    """The largest call the scratch takes: 3D, 65536 points (the packed coordinates and velocities then
+    end exactly where the accumulators begin), the c1 workload's four operators. Against sfb200_run
+    and the oracle, and with the device's free memory unchanged by a call (after a first call has
+    loaded the kernels)."""
+    from full_oracle import oracle_for
+
+    w = synthetic.config("c1")
+    assert w.n == 65536 and w.u.shape[0] == 3
+    os_, oc, oa, _src = oracle_for("c1", w)
+    ctx = _lib.Context(0)
+    desc, keep = plan_description(w.ops, 3, w.distance_bins, None, w.metric, precision, w.x.dtype, w.u.dtype)
+    plan = _lib.Plan(ctx, desc, keep)
+    plan.set_option(_abi.OPT_POINT_ORDER, 0)
+    tol = TOL_MIXED if precision == "mixed" else TOL_FP64
+    nb = len(w.distance_bins) - 1
+    xd, ud = device_inputs(w)
+    lib = _lib.load()
+    try:
+        ref_s, ref_c = run_plain(plan, ctx, xd, ud, w.n)
+        run_noalloc(plan, ctx, xd, ud, w.n)  # loads the kernels of this plan
+        sums = torch.zeros(plan.n_sums, dtype=torch.float64, device="cuda")
+        counts = torch.zeros(plan.n_counts, dtype=torch.int64, device="cuda")
+        free0, free1, total = _abi.C.c_int64(), _abi.C.c_int64(), _abi.C.c_int64()
+        torch.cuda.synchronize()
+        _lib.check(lib.sfb200_device_memory(ctx.ptr, _abi.C.byref(free0), _abi.C.byref(total)), ctx.ptr)
+        _lib.check(lib.sfb200_run_noalloc(plan.ptr, xd.data_ptr(), ud.data_ptr(), w.n, 0, sums.data_ptr(),
+                                          counts.data_ptr(), ctx.stream), ctx.ptr, "run_noalloc")
+        torch.cuda.synchronize()
+        _lib.check(lib.sfb200_device_memory(ctx.ptr, _abi.C.byref(free1), _abi.C.byref(total)), ctx.ptr)
+        assert free1.value == free0.value
+        s, c = sums.cpu().numpy(), counts.cpu().numpy()
+        assert np.array_equal(c, ref_c)
+        assert int(c.sum()) == w.pairs
+        for k in range(len(w.ops)):
+            sl = slice(k * nb, (k + 1) * nb)
+            compare(s[sl], c, os_[sl], oc, oa[sl], tol)
+            compare(s[sl], c, ref_s[sl], ref_c, oa[sl], 2 * tol)
+    finally:
+        plan.close()
+        ctx.close()
+
+
 def test_noalloc_refuses_what_does_not_fit():
     ctx = _lib.Context(0)
     w = synthetic.config("c0", n=70000)  # above the fixed scratch of 65536 points
