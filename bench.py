@@ -9,8 +9,10 @@ One step = one full pass of the pair loop over the workload (all N(N-1)/2 pairs,
   e2e    : the same metric through the C ABI with host buffers: H2D of x,u (pinned) + kernels + D2H of
            sums/counts inside the timed region.
   fp64   : the plain FP64 kernel on the same workload, timed like `value`.
-Multi-GPU (torchrun): every rank runs the whole workload (replicas, weak scaling); the elapsed time
-is the max over ranks.
+Multi-GPU (--gpus N): one process per GPU (torchrun; `python bench.py --gpus N` launches it itself).
+The one workload's upper-triangle tile pairs are cut into N shards of equal pair counts, each rank
+runs its shard and one NCCL all-reduce adds the partial histograms inside the timed step (strong
+scaling: the whole job's pairs over the slowest rank's time, max over ranks).
 
 --impl reference: the reference's CPU path restated (ThreadedBackend: round-robin outer-index chunks,
 per-thread histograms), all host threads, on a bounded sample of the same workload.
@@ -646,8 +648,23 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def spawn_ranks(n):
+    """`--gpus N` without a launcher: run this script as N ranks under torch.distributed.run (one
+    process per GPU, rendezvous on 127.0.0.1) and return its exit status."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd, cwd=ROOT)
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     if args.warmup < 3:
         args.warmup = 3
     if args.profile:

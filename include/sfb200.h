@@ -211,15 +211,29 @@ typedef enum {
      * 16 or 32. */
     SFB200_OPT_HIST_COLUMNS = 2,
     /* Multi-GPU sharding of sfb200_run: value = (count << 32) | index; the run then covers only
-     * shard `index` of `count` equal contiguous ranges of the upper-triangle tile pairs (its outputs
+     * shard `index` of `count` contiguous ranges of the upper-triangle tile pairs holding equal numbers
+     * of pairs (sfb200_shard_bounds; its outputs
      * hold that shard's partial histogram; the caller adds the shards, e.g. with one all-reduce).
      * Default 1 << 32 (one shard: everything). The partition of the pair set into tile pairs is
      * the reference's (i < j) pair set exactly, so the shard sums add up to the full histogram. */
-    SFB200_OPT_SHARD = 3
+    SFB200_OPT_SHARD = 3,
+    /* J-tile order of the flat 1D kernels (precision FP64 and MIXED, 256-point tiles): -1 automatic
+     * (sorted), 0 storage order, 1 each off-diagonal J tile staged in the order of its distance from
+     * the I tile, so that each lane's run of equal bins is long. Counts are identical either way;
+     * only the summation order of the sums changes. */
+    SFB200_OPT_TILE_SORT = 4
 } sfb200_option;
 
 /* Set a plan option (autotuning; no counterpart in the reference). */
 SFB200_API int sfb200_plan_set_option(sfb200_plan* plan, int option, int64_t value);
+
+/* Tile pairs [*tp_lo, *tp_hi) of shard `index` of `count` for n points in tiles of `tile` points (the
+ * partition SFB200_OPT_SHARD uses; host arithmetic only, no device needed). Shard k begins at the
+ * first tile pair before which k / count of the N(N-1)/2 pairs lie, so every shard is within one
+ * tile pair of an equal share of the pairs. Replaces: the per-rank share of the outer index, _rank_share
+ * (ext/StructureFunctionsMPIExt.jl:24-26), with tile pairs as the unit. */
+SFB200_API int sfb200_shard_bounds(int64_t n, int32_t tile, int32_t index, int32_t count, int64_t* tp_lo,
+                                   int64_t* tp_hi);
 
 /* ------------------------------------------------------------------------------------ serving
  * Batched execution for many independent point sets (time slices, fields, requests) of uneven size.

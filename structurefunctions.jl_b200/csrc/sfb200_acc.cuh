@@ -31,13 +31,15 @@ namespace sfb {
 //             terms) and the table is folded into the block FP64 histogram every `flush_every` tile
 //             pairs. With the points in space-filling-curve order, the j of consecutive steps are
 //             neighbours, the pair distance changes little from step to step and most steps extend
-//             the run: the per-pair cost is a compare and one add + select per operator.
+//             the run: the per-pair cost is a compare and one add per operator. (The flat kernels also
+//             stage each J tile sorted by distance from the I tile, so that a lane's bins rise almost
+//             monotonically along its row and its runs last tens to hundreds of pairs.)
 template <typename R, int NV, int PRIV>
 struct BlockHist {
     static constexpr bool AGG = PRIV == 0;
     static constexpr bool AGG_RED = PRIV == 2;
     static constexpr bool RUN = PRIV == 3;
-    static constexpr int C = (PRIV == 0 || PRIV == 2 || PRIV == 3) ? 1 : PRIV;
+    static constexpr int C = (PRIV == 0 || PRIV == 2 || RUN) ? 1 : PRIV;
     using CountT = typename std::conditional<AGG && sizeof(R) == 8, unsigned long long, unsigned>::type;
 
     R* hv;          // values: AGG: [warp][o][bin] (+ lo plane for FP32); RUN: [o][bin][column];
@@ -138,12 +140,16 @@ struct BlockHist {
     __device__ __forceinline__ void add(int key, R (&v)[NV], int lane, int warp)
     {
         if constexpr (RUN) {
-            const bool brk = key != rkey;
-            if (brk) flush_run(lane);
+            if (key != rkey) {  // the run ends: add it to the table and open an empty one
+                flush_run(lane);
 #pragma unroll
-            for (int o = 0; o < NV; ++o) rs[o] = brk ? v[o] : rs[o] + v[o];
-            rc = brk ? 1u : rc + 1u;
-            rkey = key;
+                for (int o = 0; o < NV; ++o) rs[o] = R(0);
+                rc = 0u;
+                rkey = key;
+            }
+#pragma unroll
+            for (int o = 0; o < NV; ++o) rs[o] += v[o];
+            ++rc;
         } else if constexpr (AGG) {
             const unsigned peers = __match_any_sync(FULL, key);
             reduce_peers<NV>(peers, lane, v);

@@ -102,6 +102,8 @@ struct sfb200_plan {
     LutGeom lg64{};
     LutEntry64* d_lut64 = nullptr;
     int lut64_bytes = 0;
+    // flat byte table (FP64 and mixed 1D kernels): kByteCells bytes + kByteEdges padded edges
+    unsigned char* d_lut8 = nullptr;
     // FP32 table (mixed): edge keys, geometry, window parameters
     std::vector<double> ck;
     double* d_ck = nullptr;
@@ -123,6 +125,7 @@ struct sfb200_plan {
     int order_ovr = -1;   // -1 auto, 0 caller order, 1 Morton order
     int shard_index = 0, shard_count = 1;  // sfb200_run covers shard shard_index of shard_count
     int cols_ovr = 0;     // run-length histogram columns (0 auto)
+    int sort_ovr = -1;    // J-tile order of the flat 1D kernels: -1 auto (sorted), 0 storage order, 1 sorted
 };
 
 // ------------------------------------------------------------------------------- errors
@@ -177,6 +180,61 @@ static int cuda_fail(sfb200_ctx* ctx, cudaError_t e, const char* what)
     } while (0)
 
 extern "C" int sfb200_abi_version(void) { return SFB200_ABI_VERSION; }
+
+// Tile-pair shards balanced by pairs. The tile pairs of n points in tiles of T are numbered row by
+// row (ti <= tj); a diagonal tile pair holds s(s - 1) / 2 pairs and an off-diagonal one s_i s_j, with
+// s = T except for the last, partial tile. Shard k of c starts at the first tile pair p whose
+// preceding pairs reach k / c of all N(N - 1) / 2, so every shard is within one tile pair of an equal
+// share (equal tile-pair counts would leave the shard holding the most diagonal tiles short).
+static void shard_range(long long n, int T, long long index, long long count, long long* lo, long long* hi)
+{
+    const long long nt = (n + T - 1) / T;
+    const unsigned __int128 total = (unsigned __int128)n * (unsigned __int128)(n > 0 ? n - 1 : 0) / 2;
+    auto first_at = [&](long long k) -> long long {
+        if (k <= 0) return 0;
+        if (k >= count) return nt * (nt + 1) / 2;
+        const unsigned __int128 target = (total * (unsigned __int128)k + (unsigned __int128)(count - 1)) /
+                                         (unsigned __int128)count;  // ceil(total k / count)
+        unsigned __int128 cum = 0;
+        long long p = 0;
+        for (long long ti = 0; ti < nt; ++ti) {
+            const long long si = std::min<long long>(T, n - ti * T);
+            const long long sl = n - (nt - 1) * T;  // the last tile's size
+            const unsigned __int128 diag = (unsigned __int128)(si * (si - 1) / 2);
+            const unsigned __int128 full = (unsigned __int128)si * (unsigned __int128)T;
+            const long long noff = nt - 1 - ti;  // off-diagonal tile pairs of the row
+            const unsigned __int128 row = diag + (noff > 0 ? full * (unsigned __int128)(noff - 1) + (unsigned __int128)si * sl : 0);
+            if (cum + row < target) {
+                cum += row;
+                p += 1 + noff;
+                continue;
+            }
+            if (cum >= target) return p;
+            cum += diag;
+            ++p;
+            if (cum >= target) return p;
+            // off-diagonal tile pairs of `full` pairs each (the row's last one may be partial)
+            const unsigned __int128 need = target - cum;
+            long long k2 = (long long)((need + full - 1) / full);
+            if (k2 > noff) k2 = noff;
+            return p + k2;
+        }
+        return p;
+    };
+    *lo = first_at(index);
+    *hi = first_at(index + 1);
+}
+
+extern "C" int sfb200_shard_bounds(int64_t n, int32_t tile, int32_t index, int32_t count, int64_t* tp_lo,
+                                   int64_t* tp_hi)
+{
+    if (n < 0 || tile < 1 || count < 1 || index < 0 || index >= count || !tp_lo || !tp_hi) return SFB200_ERR_INVALID_ARG;
+    long long lo, hi;
+    shard_range(n, tile, index, count, &lo, &hi);
+    *tp_lo = lo;
+    *tp_hi = hi;
+    return SFB200_OK;
+}
 
 extern "C" const char* sfb200_last_error(const sfb200_ctx* ctx)
 {
@@ -362,6 +420,37 @@ static void build_lut64(const std::vector<double>& tab, LutGeom& g, std::vector<
     }
 }
 
+// Byte table of the flat FP64 / mixed 1D kernels over the squared-edge table `tab` (sorted): cell c
+// covers the keys whose high word, sign bit cleared, shifted right by 18 equals c, i.e. [lo_c, hi_c)
+// with lo_c = bits(c << 50). The cell's byte is the number of edges strictly below lo_c when the
+// cell holds at most one distinct edge, no repeated edge and only keys the FP32 arithmetic takes
+// (within [2^-100, 2^100]); otherwise kByteSlow. `out` receives the bytes followed by the edges padded
+// with +inf to kByteEdges doubles. Returns false when the table cannot hold the edges (> 254).
+static bool build_byte_table(const std::vector<double>& tab, std::vector<unsigned char>& out)
+{
+    const int ne = (int)tab.size();
+    if (ne > kByteEdges - 2) return false;
+    out.assign((size_t)kByteCells + sizeof(double) * kByteEdges, 0);
+    double* sqx = reinterpret_cast<double*>(out.data() + kByteCells);
+    for (int k = 0; k < kByteEdges; ++k) sqx[k] = k < ne ? tab[k] : INFINITY;
+    for (int c = 0; c < kByteCells; ++c) {
+        const double lo = bits_to_double((unsigned long long)c << 50);
+        const double hi = bits_to_double((unsigned long long)(c + 1) << 50);  // NaN/inf for the top cells
+        int below = 0, inside = 0;
+        bool repeat = false;
+        for (int k = 0; k < ne; ++k) {
+            if (tab[k] < lo) ++below;
+            else if (tab[k] < hi || !(hi == hi)) {
+                ++inside;
+                if (k > 0 && tab[k] == tab[k - 1]) repeat = true;
+            }
+        }
+        const bool fp32_ok = lo >= 0x1p-100 && hi <= 0x1p100;
+        out[c] = (inside > 1 || repeat || !fp32_ok) ? (unsigned char)kByteSlow : (unsigned char)below;
+    }
+    return true;
+}
+
 // Cell geometry over FP32 keys for the window table; fails if the edge keys leave FP32's range.
 static bool geom_lut32(const std::vector<double>& keys, LutGeom& g)
 {
@@ -479,7 +568,7 @@ static void free_plan_device(sfb200_plan* p)
 {
     free_workspace(p->ws, true);
     cudaFree(p->d_exact); cudaFree(p->d_vedges); cudaFree(p->d_lut64); cudaFree(p->d_ck);
-    cudaFree(p->d_lut32); cudaFree(p->d_rowlo); cudaFree(p->d_vwin);
+    cudaFree(p->d_lut32); cudaFree(p->d_rowlo); cudaFree(p->d_vwin); cudaFree(p->d_lut8);
 }
 
 extern "C" int sfb200_plan_destroy(sfb200_plan* p)
@@ -688,6 +777,11 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         p->lut64_bytes = (int)(lut.size() * sizeof(LutEntry64));
         if ((e = upload(&p->d_lut64, lut.data(), lut.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload table");
     }
+    if (!p->sphere && !p->joint && !dlinear && !p->fp32) {
+        std::vector<unsigned char> bt;
+        if (build_byte_table(p->exact_tab, bt) && (e = upload(&p->d_lut8, bt.data(), bt.size())) != cudaSuccess)
+            return cuda_fail(ctx, e, "upload byte table");
+    }
     if (p->fp32) {
         if ((e = upload(&p->d_ck, p->ck.data(), p->ck.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload keys");
         if ((e = cudaMalloc(&p->d_lut32, sizeof(LutEntry32) * p->lg32.ncell)) != cudaSuccess)
@@ -784,6 +878,10 @@ extern "C" int sfb200_plan_set_option(sfb200_plan* p, int option, int64_t value)
             return set_err(ctx, SFB200_ERR_INVALID_ARG, "shard: index (low 32 bits) must be below the count (high 32 bits)");
         p->shard_index = (int)(value & 0xffffffffll);
         p->shard_count = (int)(value >> 32);
+        return SFB200_OK;
+    case SFB200_OPT_TILE_SORT:
+        if (value < -1 || value > 1) return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile sort must be -1, 0 or 1");
+        p->sort_ovr = (int)value;
         return SFB200_OK;
     case SFB200_OPT_HIST_COLUMNS:
         if (value < 0 || value > 32 || (value & (value - 1)))
@@ -1107,7 +1205,10 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     sfb200_ctx* ctx = p->ctx;
     const bool dlinear = p->desc.distance.kind == SFB200_BINS_LINEAR;
     int lut_bytes = 0;
-    if (p->fp32) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
+    // flat 1D kernels of precision FP64 / MIXED bin with the byte table when the plan has one
+    const bool byte_lut = p->d_lut8 && !p->joint && !p->sphere && !p->fp32;
+    if (byte_lut) lut_bytes = kByteCells + (int)sizeof(double) * kByteEdges;
+    else if (p->fp32) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
     else if (p->mixed) lut_bytes = p->lut64_bytes;  // exact table (flat) or chord table (sphere); 0 if linear
     else if (!dlinear && !p->joint) lut_bytes = p->lut64_bytes;
     int T;
@@ -1221,6 +1322,10 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     a.chord_short = 0x1p-40;         // (near-)coincident: the reference frame is degenerate
     a.chord_anti = 4.0 - 0x1p-40;    // (near-)antipodal: likewise
     a.lut_bytes = lut_bytes;
+    a.lut8 = p->d_lut8;
+    a.byte_lut = byte_lut ? 1 : 0;
+    // flat 1D kernels (FP64 / MIXED) with 256-point tiles stage off-diagonal J tiles sorted by distance
+    a.sort_j = (!p->joint && !p->sphere && !p->fp32 && T == 256 && p->sort_ovr != 0) ? 1 : 0;
     a.edges = p->d_exact;
     a.n_edges = p->desc.distance.n_edges;
     a.dist_linear = dlinear;
@@ -1258,10 +1363,17 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     out->ntp = ntp;
     out->grid = (long long)ctx->nsm * occ;  // resident blocks; a single run launches min(grid, ntp)
     out->a = a;
-    // this plan's shard of the tile pairs (equal-size contiguous ranges; the batched form walks
-    // explicit item ranges instead)
-    out->a.tp_lo = batch ? 0 : ntp * p->shard_index / p->shard_count;
-    out->a.tp_hi = batch ? ntp : ntp * (p->shard_index + 1) / p->shard_count;
+    // this plan's shard of the tile pairs (contiguous ranges of equal pair counts; the batched form
+    // walks explicit item ranges instead)
+    if (batch) {
+        out->a.tp_lo = 0;
+        out->a.tp_hi = ntp;
+    } else {
+        long long lo, hi;
+        shard_range(n, T, p->shard_index, p->shard_count, &lo, &hi);
+        out->a.tp_lo = lo;
+        out->a.tp_hi = hi;
+    }
     return SFB200_OK;
 }
 

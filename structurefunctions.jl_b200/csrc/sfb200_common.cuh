@@ -76,6 +76,27 @@ __device__ __forceinline__ int lut_cell32(float key, const LutGeom& g)
     return c;
 }
 
+// Byte table (flat FP64 kernels): one byte per quarter octave of the key over the whole FP64
+// range, indexed by the key's high word with no clamping: cell = (hi & 0x7fffffff) >> 18 (11
+// exponent bits and the top 2 mantissa bits; 8192 cells). A cell holds b = the number of edges
+// strictly below the cell's lower end, and the cell contains at most one edge, sqx[b] (the padded
+// edge table: sqx[k] = edge k for k < n_edges, +inf above), so that
+//     bin(key) = #{k : edge_k < key} = b + (key > sqx[b]).
+// Cells with two or more edges, a repeated edge, or keys the FP32 arithmetic of the mixed kernels
+// must not see (outside [2^-100, 2^100], NaN, infinity) hold kByteSlow: the pair takes the exact
+// out-of-line route. The table lives in shared memory beside the 256-entry padded edge array.
+constexpr int kByteCells = 8192;
+constexpr int kByteEdges = 256;     // padded edge array entries (n_edges <= 254)
+constexpr unsigned kByteSlow = 255u;
+
+__device__ __forceinline__ int byte_bin(const unsigned char* lut8, const double* sqx, double key, bool& slow)
+{
+    const unsigned c = ((unsigned)__double2hiint(key) & 0x7fffffffu) >> 18;
+    const unsigned b = lut8[c];
+    slow = b == kByteSlow;
+    return (int)b + (key > sqx[b] ? 1 : 0);
+}
+
 // Exact count of table entries strictly below key (binary search; `tab` sorted, n entries).
 __device__ __forceinline__ int count_below(const double* __restrict__ tab, int n, double key)
 {

@@ -44,6 +44,9 @@ struct PairArgs {
     const double* edges; // exact edge table in key space: flat squared edges, sphere raw edges
     int n_edges;
     int dist_linear;   // 1: LinearBinEdges search on r (flat: sqrt(r^2))
+    const unsigned char* lut8;  // flat byte table (kByteCells bytes) + padded edges (kByteEdges doubles)
+    int byte_lut;      // 1: the flat kernels bin with the byte table (it replaces `lut` in shared memory)
+    int sort_j;        // 1: off-diagonal J tiles of 256 points are staged sorted by distance (flat 1D)
     LinearParams dlin;
     double radius;     // sphere
     double chord_wrel; // mixed sphere: relative half-width of the chord ambiguity band at an edge
@@ -109,6 +112,91 @@ __device__ __forceinline__ void batch_items(const BatchArgs& b, RUN run)
     }
 }
 
+// ---------------------------------------------------------------------------- J-tile staging
+// Stages the J tile in shared memory, in the order of each record's squared distance from a
+// reference point of the I tile. Every pair of the tile pair is still formed exactly once (a tile
+// pair is a full T x T block of pairs when ti != tj), so the result does not depend on the order;
+// what changes is the sequence of bins a lane walks: sorted by distance, a lane's bins rise almost
+// monotonically across the tile, and its run-length histogram runs last for tens to hundreds of
+// pairs instead of a few (each run ends in shared-memory atomics).
+//
+// Counting sort over 256 buckets taken from the float bits of the FP32 key (two octaves of the
+// squared distance at 128 buckets per octave, cyclically): a tile whose keys span less than two
+// octaves -- every tile far from the reference point -- comes out sorted up to one rotation and to
+// the order inside a bucket (0.5 % of the key); closer tiles come out partly sorted. Must be called
+// by all 256 threads of the block (it holds barriers); thread t < jn passes point j0 + t's record.
+template <int R>
+__device__ __forceinline__ void stage_sorted(const double (&rec)[R], bool has, float key, double* srec,
+                                             unsigned* s_cnt, unsigned* s_wtot)
+{
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    s_cnt[t] = 0u;
+    const unsigned bucket = (__float_as_uint(key) >> 16) & 255u;
+    __syncthreads();
+    unsigned rank = 0u;
+    if (has) rank = atomicAdd(&s_cnt[bucket], 1u);
+    __syncthreads();
+    const unsigned v = s_cnt[t];
+    unsigned incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_wtot[warp] = incl;
+    __syncthreads();
+    unsigned off = 0u;
+    for (int w = 0; w < warp; ++w) off += s_wtot[w];
+    s_cnt[t] = off + incl - v;  // first slot of bucket t
+    __syncthreads();
+    if (has) {
+        double2* dst = reinterpret_cast<double2*>(srec + (size_t)(s_cnt[bucket] + rank) * R);
+#pragma unroll
+        for (int q = 0; q < R / 2; ++q) dst[q] = make_double2(rec[2 * q], rec[2 * q + 1]);
+    }
+}
+
+// Flat J tile: record [x(D), u(D) us] of point j0 + t in slot t (storage order) or in distance order
+// from I-tile point `iref` (`sorted`, block-uniform; needs blockDim.x == 256).
+template <int D>
+__device__ __forceinline__ void stage_flat_j(const PairArgs& a, int j0, int jn, double us, bool sorted, int iref,
+                                             double* srec, unsigned* s_cnt, unsigned* s_wtot)
+{
+    const int t = threadIdx.x;
+    const int n = a.n;
+    const bool has = t < jn;
+    double rec[2 * D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        rec[d] = has ? a.X64[(size_t)d * n + j0 + t] : 0.0;
+        rec[D + d] = has ? a.U64[(size_t)d * n + j0 + t] * us : 0.0;
+    }
+    if (!sorted) {
+        if (has) {
+            double2* dst = reinterpret_cast<double2*>(srec + (size_t)t * 2 * D);
+#pragma unroll
+            for (int q = 0; q < D; ++q) dst[q] = make_double2(rec[2 * q], rec[2 * q + 1]);
+        }
+        return;
+    }
+    float key = 0.f;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const float c = (float)(rec[d] - a.X64[(size_t)d * n + iref]);
+        key = fmaf(c, c, key);
+    }
+    stage_sorted<2 * D>(rec, has, key, srec, s_cnt, s_wtot);
+}
+
+// Copies the kernel's bin table into shared memory (the byte table and its padded edges, or the
+// cell table of `lut`), 16 bytes per thread and step.
+__device__ __forceinline__ void load_bin_table(const PairArgs& a, unsigned char* dst)
+{
+    const int4* src = static_cast<const int4*>(a.byte_lut ? (const void*)a.lut8 : a.lut);
+    int4* d4 = reinterpret_cast<int4*>(dst);
+    for (int k = threadIdx.x; k < a.lut_bytes / 16; k += blockDim.x) d4[k] = src[k];
+}
+
 // Exact FP64 bin of a flat pair from r^2 (src/BinEdges.jl:515-517).
 __device__ __forceinline__ int flat_exact_bin(const PairArgs& a, double r2)
 {
@@ -158,15 +246,17 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
     using Needs = ListNeeds<OPS>;
     using Hist = BlockHist<double, NV, PRIV>;
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ unsigned s_cnt[256], s_wtot[8];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n = a.n;
-    LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
+    const LutEntry64* lut = reinterpret_cast<const LutEntry64*>(smem);
+    const unsigned char* lut8 = smem;
+    const double* sqx = reinterpret_cast<const double*>(smem + kByteCells);
     double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);  // T records x(D) u(D)
     Hist hist;
     hist.init(reinterpret_cast<unsigned char*>(srec + (size_t)2 * D * T), NW, a.nb + 2, a.hist_cols);
-    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
-        lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
+    load_bin_table(a, smem);
 
     int iter = 0;
     for (long long p = a.tp_lo + blockIdx.x; p < a.tp_hi; p += gridDim.x, ++iter) {
@@ -185,16 +275,10 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
         __syncthreads();
         const int j0 = tj * T;
         const int jn = min(T, n - j0);
-        if ((int)threadIdx.x < jn) {
-            double* rec = srec + threadIdx.x * 2 * D;
-#pragma unroll
-            for (int d = 0; d < D; ++d) {
-                rec[d] = a.X64[(size_t)d * n + j0 + threadIdx.x];
-                rec[D + d] = a.U64[(size_t)d * n + j0 + threadIdx.x];
-            }
-        }
-        __syncthreads();
         const bool diag = ti == tj;
+        stage_flat_j<D>(a, j0, jn, 1.0, a.sort_j && !diag && T == 256, ti * T + min(T / 2, n - 1 - ti * T), srec,
+                        s_cnt, s_wtot);
+        __syncthreads();
         auto pair = [&](int jj, int& key, double (&v)[NV]) {
             double dx[D], du[D];
 #pragma unroll
@@ -208,8 +292,15 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
             const double h2 = SFB_ADD(SFB_MUL(dx[0], dx[0]), SFB_MUL(dx[1], dx[1]));
             double r2 = h2;
             if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
-            if (a.dist_linear) key = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
-            else key = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+            if (a.byte_lut) {
+                bool slow;
+                key = byte_bin(lut8, sqx, r2, slow);
+                if (slow) key = count_below_ool(a.edges, a.n_edges, r2);
+            } else if (a.dist_linear) {
+                key = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
+            } else {
+                key = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+            }
 
             double L = 0.0, Tt = 0.0, Q = 0.0;
             const double rs = rsqrt(r2);

@@ -97,14 +97,16 @@ __device__ __forceinline__ float rsqrt_normal(float x)
 }
 
 // Per-pair FP32 primitives of a flat pair from FP64 differences (du already scaled by us).
-// Returns false when the pair must be evaluated in FP64 (squared distances outside FP32's range).
+// Returns false when the pair must be evaluated in FP64 because its horizontal squared distance (the
+// 3D transverse direction) leaves FP32's range; the caller checks r^2 itself (the byte table routes
+// such keys out of line already).
 template <int D, class OPS>
 __device__ __forceinline__ bool flat_primitives_mx(const double (&dx)[D], const double (&du)[D], double r2, double h2,
                                                    float& L, float& Tt, float& T2, float& Q)
 {
     using N = ListNeeds2<OPS>;
     const float r2f = f32(r2);
-    bool fine = f32_range_ok(r2f);
+    bool fine = true;
     const float rs = rsqrt_normal(r2f);
     L = 0.f;
     Tt = 0.f;
@@ -206,15 +208,17 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
     constexpr int NP = D;  // double2 per j record: x(D) u(D)
     using Hist = BlockHist<float, NV, PRIV>;
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ unsigned s_cnt[256], s_wtot[8];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n = a.n;
-    LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
+    const LutEntry64* lut = reinterpret_cast<const LutEntry64*>(smem);
+    const unsigned char* lut8 = smem;
+    const double* sqx = reinterpret_cast<const double*>(smem + kByteCells);
     double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);  // T records of 2D doubles
     Hist hist;
     hist.init(reinterpret_cast<unsigned char*>(srec + (size_t)2 * NP * T), NW, a.nb + 2, a.hist_cols);
-    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
-        lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
+    load_bin_table(a, smem);
     const int ku = pow2_exponent_above(a.g_stats[2]);
     const double us = ldexp(1.0, -ku);
     double unscale[NV];
@@ -237,17 +241,10 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
         __syncthreads();
         const int j0 = tj * T;
         const int jn = min(T, n - j0);
-        if ((int)threadIdx.x < jn) {
-            double* rec = srec + threadIdx.x * 2 * NP;
-            const int jg = j0 + threadIdx.x;
-#pragma unroll
-            for (int d = 0; d < D; ++d) {
-                rec[d] = a.X64[(size_t)d * n + jg];
-                rec[D + d] = a.U64[(size_t)d * n + jg] * us;
-            }
-        }
-        __syncthreads();
         const bool diag = ti == tj;
+        stage_flat_j<D>(a, j0, jn, us, a.sort_j && !diag && T == 256, ti * T + min(T / 2, n - 1 - ti * T), srec,
+                        s_cnt, s_wtot);
+        __syncthreads();
         // one pair: key (bin) and values
         auto pair = [&](int jj, int& key, float (&v)[NV]) {
             double rj[2 * NP];
@@ -262,12 +259,19 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
             const double h2 = SFB_ADD(SFB_MUL(dx[0], dx[0]), SFB_MUL(dx[1], dx[1]));
             double r2 = h2;
             if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
-            if (a.dist_linear) key = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
-            else key = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+            bool slow;
+            if (a.byte_lut) {
+                key = byte_bin(lut8, sqx, r2, slow);  // slow: several edges in the cell or r^2 outside FP32
+            } else {
+                if (a.dist_linear) key = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
+                else key = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+                slow = !f32_range_ok(f32(r2));
+            }
             float L, Tt, T2, Q;
             const bool fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q);
             eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
-            if (!fine) {
+            if (slow || !fine) {
+                if (slow && a.byte_lut) key = count_below_ool(a.edges, a.n_edges, r2);
                 const FlatValues<D, OPS> f = flat_values_fp64_ool<D, OPS>(
                     dx[0], dx[1], D == 3 ? dx[D - 1] : 0.0, du[0], du[1], D == 3 ? du[D - 1] : 0.0, r2, h2, &a.gen);
 #pragma unroll
@@ -298,7 +302,7 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
 }
 
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256) k_flat1d_mx(const __grid_constant__ PairArgs a)
+__global__ void __launch_bounds__(256, 3) k_flat1d_mx(const __grid_constant__ PairArgs a)
 {
     flat1d_mx_run<D, OPS, PRIV>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
@@ -741,7 +745,7 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                 else db = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
                 // flat bins are exact: a pair outside the distance range needs no value
                 if (db < 1 || db > nd) return r;
-                fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q);
+                fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q) && f32_range_ok(f32(r2));
             }
             float v[1];
             eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);

@@ -31,17 +31,26 @@ libpath() = isempty(LIB[]) ? get(ENV, "SFB200_LIB", joinpath(@__DIR__, "..", "li
 """
     B200Backend(; device = 0, precision = :mixed)
 
-Run the O(N^2) pair loop on a B200. `precision = :mixed` (FP32 pair arithmetic, FP64 recheck of
-pairs near a bin edge, FP64 merge) or `:fp64` (every pair in FP64). Not an `AbstractGPUBackend`, so
-no KernelAbstractions route captures it; `AutoBackend` never selects it.
+Run the O(N^2) pair loop on a B200. `precision`:
+- `:mixed` (default): FP64 point differences, squared distance (the bin, exactly the reference's)
+  and projection numerators; FP32 normalisation, operator powers and per-lane accumulation; FP64
+  merge. Sums within 1e-6 of each bin's sum of |value|.
+- `:fp64`: every pair in FP64 (the plain form).
+- `:fp32`: FP32 pair arithmetic from (hi, lo) records with an FP64 recheck of the pairs near a bin
+  edge; counts exact, sums within 2e-5 of each bin's sum of |value|.
+Plans (bin tables, operator mapping, device workspace) are cached per call shape, so repeated
+calls with the same operators, bins, metric and element types reuse them. Not an
+`AbstractGPUBackend`, so no KernelAbstractions route captures it; `AutoBackend` never selects it.
 """
 struct B200Backend <: CB.AbstractExecutionBackend
     device::Int
     precision::Symbol
 end
 B200Backend(; device::Integer = 0, precision::Symbol = :mixed) =
-    precision in (:mixed, :fp64) ? B200Backend(Int(device), precision) :
-    throw(ArgumentError("precision must be :mixed or :fp64"))
+    precision in (:mixed, :fp64, :fp32) ? B200Backend(Int(device), precision) :
+    throw(ArgumentError("precision must be :mixed, :fp64 or :fp32"))
+
+c_precision(p::Symbol) = p === :fp64 ? Int32(0) : p === :mixed ? Int32(1) : Int32(2)
 
 # ---------------------------------------------------------------------- C structs (sfb200.h)
 
@@ -175,26 +184,53 @@ function plan_desc(precision::Int32, sfs::Tuple, xs::Matrix, us::Matrix, distanc
     return desc, keep
 end
 
-function run_pairs(b::B200Backend, sfs::Tuple, x::AbstractMatrix, u::AbstractMatrix, distance_bins,
-                   value_bins, metric, sums::Vector{Float64}, counts::Vector{UInt64}, flags::UInt32)
-    xs = Matrix(x)   # contiguous column-major (W, N)
-    us = Matrix(u)
-    desc, keep = plan_desc(b.precision === :mixed ? Int32(1) : Int32(0), sfs, xs, us, distance_bins, value_bins,
-                           metric)
+# Plans cached per call shape: (device, precision, operator types, D, metric, bins, element types).
+# A plan owns its device workspace and serves one call at a time (the reference's workspace rule,
+# src/Calculations/workspace.jl:44), so calls on one backend from several tasks are serialised by
+# PLAN_LOCK around the run.
+const PLANS = Dict{Any, Ptr{Cvoid}}()
+const PLAN_LOCK = ReentrantLock()
+
+function cached_plan(b::B200Backend, sfs::Tuple, xs::Matrix, us::Matrix, distance_bins, value_bins, metric)
+    key = (b.device, b.precision, map(typeof, sfs), sfs, size(us, 1), metric, collect(distance_bins),
+           value_bins === nothing ? nothing : collect(value_bins), eltype(xs), eltype(us))
     ctx = context(b.device)
-    plan = Ref{Ptr{Cvoid}}(C_NULL)
-    GC.@preserve keep begin
-        check(ccall((:sfb200_plan_create, libpath()), Cint, (Ptr{Cvoid}, Ref{CPlanDesc}, Ref{Ptr{Cvoid}}),
-                    ctx, desc, plan), ctx)
+    plan = get!(PLANS, key) do
+        desc, keep = plan_desc(c_precision(b.precision), sfs, xs, us, distance_bins, value_bins, metric)
+        p = Ref{Ptr{Cvoid}}(C_NULL)
+        GC.@preserve keep begin
+            check(ccall((:sfb200_plan_create, libpath()), Cint, (Ptr{Cvoid}, Ref{CPlanDesc}, Ref{Ptr{Cvoid}}),
+                        ctx, desc, p), ctx)
+        end
+        p[]
     end
-    try
+    return plan, ctx
+end
+
+"""Destroy every cached plan (they are rebuilt on the next call)."""
+function clear_plans!()
+    lock(PLAN_LOCK) do
+        for p in values(PLANS)
+            ccall((:sfb200_plan_destroy, libpath()), Cint, (Ptr{Cvoid},), p)
+        end
+        empty!(PLANS)
+    end
+    return nothing
+end
+
+# Runs the pair loop into `sums` / `counts` (Float64 / UInt64, contiguous). flags: RUN_ACCUMULATE adds
+# into them (the mutating API), 0 overwrites them.
+function run_pairs(b::B200Backend, sfs::Tuple, x::AbstractMatrix, u::AbstractMatrix, distance_bins,
+                   value_bins, metric, sums::Array{Float64}, counts::Array{UInt64}, flags::UInt32)
+    xs = x isa Matrix ? x : Matrix(x)   # contiguous column-major (W, N)
+    us = u isa Matrix ? u : Matrix(u)
+    lock(PLAN_LOCK) do
+        plan, ctx = cached_plan(b, sfs, xs, us, distance_bins, value_bins, metric)
         GC.@preserve xs us sums counts begin
             check(ccall((:sfb200_run, libpath()), Cint,
                         (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Int64, UInt32, Ptr{Float64}, Ptr{UInt64}, Ptr{Cvoid}),
-                        plan[], xs, us, size(xs, 2), flags, sums, counts, C_NULL), ctx)
+                        plan, xs, us, size(xs, 2), flags, sums, counts, C_NULL), ctx)
         end
-    finally
-        ccall((:sfb200_plan_destroy, libpath()), Cint, (Ptr{Cvoid},), plan[])
     end
     return nothing
 end
@@ -229,18 +265,28 @@ function SFC._dispatch_execution_backend(
         reshape(out_type(x, u).(sums), nd, nv), reshape(CT.(counts), nd, nv))
 end
 
-# mutating: add into the caller's buffers (beside dispatch.jl:399-404)
+# mutating: add into the caller's buffers (beside dispatch.jl:399-404). Float64 sums and UInt64 counts
+# in contiguous arrays are accumulated into by the library itself (SFB200_RUN_ACCUMULATE); other
+# element types go through library-typed buffers and a conversion.
+function accumulate_into!(b, sfs, x, u, distance_bins, value_bins, metric, sums::AbstractArray, counts::AbstractArray)
+    if sums isa Array{Float64} && counts isa Array{UInt64}
+        run_pairs(b, sfs, x, u, distance_bins, value_bins, metric, sums, counts, RUN_ACCUMULATE)
+    else
+        s = zeros(Float64, length(sums))
+        c = zeros(UInt64, length(counts))
+        run_pairs(b, sfs, x, u, distance_bins, value_bins, metric, s, c, UInt32(0))
+        sums .+= reshape(s, size(sums))
+        counts .+= reshape(c, size(counts))
+    end
+    return nothing
+end
+
 function SFC._dispatch_execution_backend!(
     b::B200Backend, shape::SFC.PointField, sums::AbstractVector, counts::AbstractVector,
     sf::SFT.AbstractPairwiseStructureFunctionType, x, u, distance_bins;
     distance_metric::DI.PreMetric = DI.Euclidean(), kwargs...,
 )
-    s = zeros(Float64, length(sums))
-    c = zeros(UInt64, length(counts))
-    run_pairs(b, (sf,), x, u, distance_bins, nothing, distance_metric, s, c, UInt32(0))
-    sums .+= s
-    counts .+= c
-    return nothing
+    accumulate_into!(b, (sf,), x, u, distance_bins, nothing, distance_metric, sums, counts)
 end
 
 function SFC._dispatch_execution_backend!(
@@ -248,12 +294,7 @@ function SFC._dispatch_execution_backend!(
     sf::SFT.AbstractPairwiseStructureFunctionType, x, u, distance_bins, value_bins::AbstractVector;
     distance_metric::DI.PreMetric = DI.Euclidean(), kwargs...,
 )
-    s = zeros(Float64, length(sums_2d))
-    c = zeros(UInt64, length(counts_2d))
-    run_pairs(b, (sf,), x, u, distance_bins, value_bins, distance_metric, s, c, UInt32(0))
-    sums_2d .+= reshape(s, size(sums_2d))
-    counts_2d .+= reshape(c, size(counts_2d))
-    return nothing
+    accumulate_into!(b, (sf,), x, u, distance_bins, value_bins, distance_metric, sums_2d, counts_2d)
 end
 
 # auxiliary-axis shapes are not on this path (as the GPU in-place route, dispatch.jl:406-410)
@@ -287,6 +328,7 @@ struct B200Request
     distance_bins::Any
     value_bins::Any
     metric::Any
+    count_eltype::Type
 end
 
 mutable struct B200Ticket
@@ -321,6 +363,7 @@ mutable struct B200Server
     plans::Dict{Any, Ptr{Cvoid}}
     lock::ReentrantLock
     stopping::Bool
+    failed::Any           # the error that ended the loop (nothing while it runs)
     task::Union{Nothing, Task}
     rounds::Int
 end
@@ -334,13 +377,25 @@ A request loop over one device (mixed precision). `start!` it, `submit!` request
 B200Server(; device::Integer = 0, max_slots::Integer = 256, memory_reserve::Integer = 1 << 30,
            round_pairs::Real = 6e9, min_units::Integer = 1) =
     B200Server(Int(device), Int(max_slots), Int64(memory_reserve), Float64(round_pairs), Int(min_units),
-               B200Ticket[], ActiveSlice[], Dict{Any, Ptr{Cvoid}}(), ReentrantLock(), false, nothing, 0)
+               B200Ticket[], ActiveSlice[], Dict{Any, Ptr{Cvoid}}(), ReentrantLock(), false, nothing, nothing, 0)
 
+"""
+    submit!(srv, sf, x, u, distance_bins[, value_bins]; distance_metric, count_eltype = UInt32)
+
+Queue one request. The count guard of the public entry runs here (`_assert_counts_representable`,
+src/Calculations/serial.jl:111-120): counts of `count_eltype` must hold N(N-1)/2. A request submitted
+after the loop has failed fails at once with the loop's error.
+"""
 function submit!(srv::B200Server, sf, x::AbstractMatrix, u::AbstractMatrix, distance_bins, value_bins = nothing;
-                 distance_metric::DI.PreMetric = DI.Euclidean())
-    t = B200Ticket(B200Request(sf, Matrix(x), Matrix(u), distance_bins, value_bins, distance_metric), time(),
-                   NaN, nothing, nothing, Base.Event())
-    lock(() -> push!(srv.pending, t), srv.lock)
+                 distance_metric::DI.PreMetric = DI.Euclidean(), count_eltype::Type = UInt32)
+    SFC._assert_counts_representable(count_eltype, size(x, 2))
+    t = B200Ticket(B200Request(sf, Matrix(x), Matrix(u), distance_bins, value_bins, distance_metric, count_eltype),
+                   time(), NaN, nothing, nothing, Base.Event())
+    err = lock(srv.lock) do
+        srv.failed === nothing && push!(srv.pending, t)
+        srv.failed
+    end
+    err === nothing || fail!(t, err)
     return t
 end
 
@@ -355,11 +410,14 @@ start!(srv::B200Server) = (srv.task = Threads.@spawn serve_loop(srv); srv)
 
 function stop!(srv::B200Server)
     lock(() -> (srv.stopping = true), srv.lock)
-    srv.task === nothing || wait(srv.task)
-    for plan in values(srv.plans)
-        ccall((:sfb200_plan_destroy, libpath()), Cint, (Ptr{Cvoid},), plan)
+    try
+        srv.task === nothing || wait(srv.task)  # rethrows the loop's failure, if any
+    finally
+        for plan in values(srv.plans)
+            ccall((:sfb200_plan_destroy, libpath()), Cint, (Ptr{Cvoid},), plan)
+        end
+        empty!(srv.plans)
     end
-    empty!(srv.plans)
     return nothing
 end
 
@@ -401,7 +459,12 @@ function create_slice(srv::B200Server, ctx, t::B200Ticket)
                     plan, r.x, r.u, size(r.x, 2), UInt32(0), C_NULL, sl), ctx)
     end
     info = Ref(CSliceInfo(0, 0, 0, 0))
-    check(ccall((:sfb200_slice_get_info, libpath()), Cint, (Ptr{Cvoid}, Ref{CSliceInfo}), sl[], info), ctx)
+    try
+        check(ccall((:sfb200_slice_get_info, libpath()), Cint, (Ptr{Cvoid}, Ref{CSliceInfo}), sl[], info), ctx)
+    catch
+        ccall((:sfb200_slice_destroy, libpath()), Cint, (Ptr{Cvoid},), sl[])  # the slice exists: free it
+        rethrow()
+    end
     units = info[].tile_pairs
     return ActiveSlice(t, sl[], plan, ns[], nc[], units, 0, 0, max(1.0, info[].pairs / max(1, units)))
 end
@@ -416,12 +479,13 @@ function complete!(ctx, a::ActiveSlice)
                     (Ptr{Cvoid}, Ptr{Float64}, Ptr{UInt64}, UInt32, Ptr{Cvoid}), a.slice, sums, counts, UInt32(0),
                     C_NULL), ctx)
         T = out_type(r.x, r.u)
+        CT = r.count_eltype
         if r.value_bins === nothing
-            t.result = SFO.StructureFunctionSumsAndCounts(r.sf, r.distance_bins, T.(sums), UInt32.(counts))
+            t.result = SFO.StructureFunctionSumsAndCounts(r.sf, r.distance_bins, T.(sums), CT.(counts))
         else
             nd, nv = length(r.distance_bins) - 1, length(r.value_bins) - 1
             t.result = SFO.StructureFunction2DSumsAndCounts(r.sf, r.distance_bins, r.value_bins,
-                reshape(T.(sums), nd, nv), reshape(UInt32.(counts), nd, nv))
+                reshape(T.(sums), nd, nv), reshape(CT.(counts), nd, nv))
         end
     catch err
         t.error = err
@@ -513,7 +577,13 @@ function serve_loop(srv::B200Server)
             fail!(a.ticket, err)
         end
         empty!(srv.active)
-        for t in lock(() -> splice!(srv.pending, 1:length(srv.pending)), srv.lock)
+        # under the lock: mark the loop failed and take what is pending, so that a later submit!
+        # fails its ticket at once instead of queueing it for a loop that no longer runs
+        waiting = lock(srv.lock) do
+            srv.failed = err
+            splice!(srv.pending, 1:length(srv.pending))
+        end
+        for t in waiting
             fail!(t, err)
         end
         rethrow()

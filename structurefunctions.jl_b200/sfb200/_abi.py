@@ -116,6 +116,7 @@ EXPORTED_SYMBOLS = (
     "sfb200_plan_last_stats",
     "sfb200_plan_set_launch",
     "sfb200_plan_set_option",
+    "sfb200_shard_bounds",
     "sfb200_slice_create",
     "sfb200_slice_get_info",
     "sfb200_batch_run",
@@ -132,3 +133,4 @@ EXPORTED_SYMBOLS = (
 OPT_POINT_ORDER = 1
 OPT_HIST_COLUMNS = 2
 OPT_SHARD = 3
+OPT_TILE_SORT = 4

@@ -70,6 +70,9 @@ def load():
         lib.sfb200_batch_query.restype = C.c_int
         lib.sfb200_batch_wait_oldest.argtypes = [P, C.POINTER(C.c_int64)]
         lib.sfb200_batch_wait_oldest.restype = C.c_int
+        lib.sfb200_shard_bounds.argtypes = [C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int64),
+                                            C.POINTER(C.c_int64)]
+        lib.sfb200_shard_bounds.restype = C.c_int
         lib.sfb200_run_noalloc.argtypes = [P, P, P, C.c_int64, C.c_uint32, P, P, P]
         lib.sfb200_run_noalloc.restype = C.c_int
         if lib.sfb200_abi_version() != _abi.ABI_VERSION:
@@ -232,7 +235,7 @@ class Plan:
         check(load().sfb200_plan_set_launch(self.ptr, tile, privatization, blocks_per_sm), self.ctx.ptr)
 
     def set_option(self, option, value):
-        """sfb200_plan_set_option: `option` is _abi.OPT_POINT_ORDER or _abi.OPT_HIST_COLUMNS."""
+        """sfb200_plan_set_option: `option` is one of the _abi.OPT_* values."""
         check(load().sfb200_plan_set_option(self.ptr, int(option), int(value)), self.ctx.ptr)
 
     def close(self):

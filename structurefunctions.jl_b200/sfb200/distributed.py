@@ -2,8 +2,9 @@
 
 The pair set of one call is cut into the upper-triangle tile pairs of the kernels, which are
 independent units of work. Every rank holds all points (they are small), runs one contiguous shard of
-the tile pairs (sfb200_plan_set_option SFB200_OPT_SHARD) into a partial histogram, and a single
-all-reduce (NCCL over NVLink on GPUs, gloo on CPUs) adds the partial sums (FP64) and counts (int64).
+the tile pairs (sfb200_plan_set_option SFB200_OPT_SHARD; shards hold equal numbers of pairs, see
+sfb200_shard_bounds) into a partial histogram, and a single all-reduce (NCCL over NVLink on GPUs, gloo
+on CPUs) adds the partial sums (FP64) and counts (int64).
 This mirrors the reference's MPI rank sharding (ext/StructureFunctionsMPIExt.jl:24-26, one reduction
 of the per-rank histograms), with tile pairs in place of outer-loop indices.
 """
@@ -20,9 +21,24 @@ def shard_value(index, count):
     return (int(count) << 32) | int(index)
 
 
-def shard_bounds(ntp, index, count):
-    """Tile pairs [lo, hi) of shard `index` of `count` (the library's partition)."""
-    return ntp * index // count, ntp * (index + 1) // count
+def shard_bounds(n, tile, index, count):
+    """Tile pairs [lo, hi) of shard `index` of `count` for n points in tiles of `tile` points: the
+    library's partition (sfb200_shard_bounds, host arithmetic only), contiguous ranges of tile pairs
+    each within one tile pair of an equal share of the pairs."""
+    import ctypes as C
+
+    lo, hi = C.c_int64(), C.c_int64()
+    rc = _lib.load().sfb200_shard_bounds(int(n), int(tile), int(index), int(count), C.byref(lo), C.byref(hi))
+    if rc != 0:
+        raise ValueError("invalid shard request")
+    return lo.value, hi.value
+
+
+def tile_pair_pairs(n, tile, ti, tj):
+    """Pairs of tile pair (ti, tj): s_i s_j off the diagonal, s (s - 1) / 2 on it."""
+    si = min(tile, n - ti * tile)
+    sj = min(tile, n - tj * tile)
+    return si * (si - 1) // 2 if ti == tj else si * sj
 
 
 def allreduce_histogram(sums, counts, group=None):

@@ -42,3 +42,16 @@ def test_reference_arm_is_silent_on_other_ranks():
                   {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert p.returncode == 0, p.stderr[-2000:]
     assert not [l for l in p.stdout.splitlines() if l.strip().startswith("{")]
+
+
+def test_gpus_flag_launches_one_rank_per_gpu():
+    """`bench.py --gpus 2` without a launcher starts two ranks itself (torch.distributed.run with
+    RANK / LOCAL_RANK / WORLD_SIZE set); rank 0 alone prints the line, which names both ranks."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--impl", "reference",
+                        "--config", "c0", "--steps", "1", "--warmup", "3"], cwd=ROOT, env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [l for l in p.stdout.splitlines() if l.strip().startswith("{")]
+    assert len(lines) == 1
+    assert json.loads(lines[0])["n_gpus"] == 2

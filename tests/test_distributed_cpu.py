@@ -3,7 +3,9 @@
 Each rank of a 2-process gloo group computes its shard of the upper-triangle tile pairs with a NumPy
 restatement of the pair loop (FP64, L2SF, squared-edge bins), the shards are added with the package's
 all-reduce helper, and the sum must equal the unsharded computation: counts exactly, sums to
-rounding. The shard arithmetic itself (the library's partition) is checked for every small case.
+rounding. The shard arithmetic itself (the library's partition, sfb200_shard_bounds, which needs no
+GPU) is checked for every small case: the shards tile the tile pairs and hold equal pair counts to
+within one tile pair.
 """
 import math
 import os
@@ -12,7 +14,7 @@ import socket
 import numpy as np
 import pytest
 
-from sfb200.distributed import shard_bounds, shard_value
+from sfb200.distributed import shard_bounds, shard_value, tile_pair_pairs
 
 T = 32
 
@@ -48,13 +50,44 @@ def histogram_of_tile_pairs(x, u, sqedges, pairs):
 
 @pytest.mark.parametrize("count", [1, 2, 3, 7, 8])
 def test_shard_bounds_partition_the_tile_pairs(count):
-    for ntp in (0, 1, 5, 36, 1000, 8256):
-        bounds = [shard_bounds(ntp, k, count) for k in range(count)]
+    for n in (0, 1, 2, 31, 32, 33, 300, 1000, 8256):
+        nt = (n + T - 1) // T
+        tp = tile_pairs(n)
+        ntp = nt * (nt + 1) // 2
+        assert len(tp) == ntp
+        bounds = [shard_bounds(n, T, k, count) for k in range(count)]
         assert bounds[0][0] == 0 and bounds[-1][1] == ntp
         for (a0, a1), (b0, b1) in zip(bounds, bounds[1:]):
             assert a1 == b0 and a0 <= a1
-        sizes = [hi - lo for lo, hi in bounds]
-        assert max(sizes) - min(sizes) <= 1
+        # each shard within one tile pair of its exact share
+        work = [sum(tile_pair_pairs(n, T, *tp[p]) for p in range(lo, hi)) for lo, hi in bounds]
+        assert sum(work) == n * (n - 1) // 2
+        if n > T:
+            assert max(work) - min(work) <= 2 * T * T, (n, count, work)
+
+
+def test_shard_bounds_balance_pairs_at_the_benchmark_size():
+    """65536 points in 256-point tiles over 8 shards: equal tile-pair counts would differ by the
+    diagonal tiles' half-empty blocks; balanced by pairs each shard is within one tile pair of its
+    exact share (so two shards differ by less than two)."""
+    n, tile = 65536, 256
+    nt = n // tile
+    for count in (2, 4, 8):
+        work = []
+        for k in range(count):
+            lo, hi = shard_bounds(n, tile, k, count)
+            # rows are contiguous: count the pairs of [lo, hi) row by row
+            w, p = 0, 0
+            for ti in range(nt):
+                row = nt - ti
+                a, b = max(lo, p), min(hi, p + row)
+                if a < b:
+                    w += (b - a) * tile * tile - (tile * tile - tile * (tile - 1) // 2 if a == p else 0)
+                p += row
+            work.append(w)
+        assert sum(work) == n * (n - 1) // 2
+        share = n * (n - 1) // 2 / count
+        assert all(abs(w - share) <= tile * tile for w in work), (count, work)
 
 
 def test_shard_value_encoding():
@@ -87,7 +120,7 @@ def _rank_main(rank, world, port, out_dir):
         edges = np.exp(np.linspace(math.log(1e-2), math.log(math.sqrt(2.0)), 9))
         sq = edges * edges
         tp = tile_pairs(n)
-        lo, hi = shard_bounds(len(tp), rank, world)
+        lo, hi = shard_bounds(n, T, rank, world)
         s, c = histogram_of_tile_pairs(x, u, sq, tp[lo:hi])
         st = torch.from_numpy(s)
         ct = torch.from_numpy(c)
