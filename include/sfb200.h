@@ -189,6 +189,15 @@ SFB200_API int sfb200_plan_output_sizes(const sfb200_plan* plan, int64_t* n_sums
 SFB200_API int sfb200_run(sfb200_plan* plan, const void* x, const void* u, int64_t n, uint32_t flags,
                double* sums, uint64_t* counts, void* stream);
 
+/* Smallest and largest pair distance over all pairs i < j of the N points, for automatic binning:
+ * Euclidean sqrt(r^2) from the reference's squared distance; on the sphere the arc length R sigma
+ * (SphericalAngle: sigma) from the pair frame's angle 2 atan(|q - p|, |q + p|). u is packed with x
+ * (the plan's layout) but not used. flags may hold SFB200_RUN_DEVICE_INPUT. Synchronous.
+ * Replaces: the min/max scan of the reference's auto-binning, _minmax_matrix_for_autobins / minmax_i
+ * (src/Calculations/dispatch.jl:205-298). */
+SFB200_API int sfb200_distance_range(sfb200_plan* plan, const void* x, const void* u, int64_t n, uint32_t flags,
+                                     double* dmin, double* dmax, void* stream);
+
 /* Statistics of the last sfb200_run on this plan. */
 SFB200_API int sfb200_plan_last_stats(const sfb200_plan* plan, sfb200_stats* out);
 

@@ -48,6 +48,9 @@ def load():
         lib.oracle_atan2.argtypes = [C.c_double, C.c_double]
         lib.oracle_atan2.restype = C.c_double
         lib.oracle_threads_available.restype = C.c_int
+        lib.oracle_run_single_pass.argtypes = [P, P, P, C.c_int64, C.c_int64, C.c_int64, P, P, P]
+        lib.oracle_run_single_pass.restype = C.c_int
+        lib.oracle_single_pass_derive.argtypes = [P, P, C.c_int64]
         _lib = lib
     return _lib
 
@@ -85,6 +88,37 @@ def run(desc, x, u, threads=0, i0=0, istep=1, with_abs=False):
     if with_abs:
         return sums, counts, abss
     return sums, counts
+
+
+def run_single_pass(desc, x, u, i0=0, istep=1, derive=True):
+    """Six-invariant single pass (rows S2, L2, T2, S3, L3, L1T2) as (sums, counts, abs_sums), each
+    (6, nb) column-major like the reference's accumulator. `abs_sums` holds the per-bin sums of
+    |value| of the accumulated rows and, for the derived rows, |S2| + |L2| and |S3| + |L3| sums (the
+    scale of a difference). With derive=False (partial rows of a split run) the derived rows are left
+    for the caller to fill once the partial results are added."""
+    lib = load()
+    xa, ua = _colmajor64(x), _colmajor64(u)
+    n = xa.shape[1]
+    nb = desc.distance.n_edges - 1
+    sums = np.zeros((6, nb), order="F")
+    counts = np.zeros((6, nb), dtype=np.uint64, order="F")
+    abss = np.zeros((6, nb), order="F")
+    rc = lib.oracle_run_single_pass(C.addressof(desc), xa.ctypes.data, ua.ctypes.data, n, int(i0), int(istep),
+                                    sums.ctypes.data, counts.ctypes.data, abss.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("oracle failed")
+    if derive:
+        single_pass_derive(sums, counts, abss)
+    return sums, counts, abss
+
+
+def single_pass_derive(sums, counts, abss=None):
+    """Fill the derived rows (T2 = S2 - L2, L1T2 = S3 - L3, counts of row S2 everywhere) in place."""
+    nb = sums.shape[1]
+    load().oracle_single_pass_derive(sums.ctypes.data, counts.ctypes.data, nb)
+    if abss is not None:
+        abss[2] = abss[0] + abss[1]
+        abss[5] = abss[3] + abss[4]
 
 
 def threads_available():

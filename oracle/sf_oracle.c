@@ -25,6 +25,8 @@
  *   projections, n-hat             src/HelperFunctions.jl:450-468, 624-683
  *   spherical frame                src/HelperFunctions.jl:133-153, 186-200, 265-276, 324-348
  *   bin average                    src/Calculations/serial.jl:132-141
+ *   six-invariant single pass      src/Calculations/serial_single_pass.jl:238-270 (Euclidean SIMD loop),
+ *                                  321-350 (other metrics), 209-219 (derived rows T2, L1T2)
  *
  * Third-party arithmetic that is not in the reference tree: StaticArrays `dot`/`cross` (compat 1.9,
  * plain left-to-right products and sums, restated literally), StaticArrays `normalize` (restated as
@@ -465,6 +467,96 @@ OR_EXPORT int oracle_run_threaded(const sfb200_plan_desc* d, const double* x, co
         for (int64_t k = 0; k < nc; ++k) counts[k] += lc[(size_t)nc * t + k];
     }
     free(ls); free(lc); free(P);
+    return 0;
+}
+
+/* ---------------------------------------------------------------- six-invariant single pass */
+
+/* Rows of the single-pass accumulator (src/Calculations/batch_api.jl:98, serial_single_pass.jl:593-600):
+ * 0 S2 = |du|^2, 1 L2 = du_L^2, 2 T2 = S2 - L2 (derived), 3 S3 = du_L |du|^2, 4 L3 = du_L^3,
+ * 5 L1T2 = S3 - L3 (derived). Sums and counts are (6, nb) column-major: element (t, b) at t + 6 b. */
+#define SP_N 6
+
+static void sp_add(double* sums, uint64_t* counts, double* abss, int64_t b, double duL, double dn2)
+{
+    const double duL2 = duL * duL;
+    const double v[4] = {dn2, duL2, duL * dn2, duL * duL2};
+    const int row[4] = {0, 1, 3, 4};
+    for (int k = 0; k < 4; ++k) {
+        sums[row[k] + SP_N * b] += v[k];
+        if (abss) abss[row[k] + SP_N * b] += fabs(v[k]);
+    }
+    counts[SP_N * b] += 1;
+}
+
+/* _pf_sp_simd_pairs! (serial_single_pass.jl:238-270): du_L = dot(du, dx) * inv(sqrt(r2)),
+ * dn2 = dot(du, du); the bin from r2 by the squared plan. Other metrics: _sp1d_pairs!
+ * (serial_single_pass.jl:321-350), du_L = du . r_hat in the pair frame (r_hat = e1 on the sphere). */
+static void sp_rows(const plan_view* pv, const double* x, const double* u, const sph_point* P, int64_t N,
+                    int64_t i0, int64_t istep, double* sums, uint64_t* counts, double* abss)
+{
+    const sfb200_plan_desc* d = pv->d;
+    const int D = d->dim;
+    for (int64_t i = i0; i < N - 1; i += istep) {
+        const double* ui = u + (size_t)D * i;
+        for (int64_t j = i + 1; j < N; ++j) {
+            const double* uj = u + (size_t)D * j;
+            double du[3] = {0.0, 0.0, 0.0}, duL;
+            int64_t b;
+            if (d->geometry == SFB200_GEOM_FLAT) {
+                const double* xi = x + (size_t)D * i;
+                const double* xj = x + (size_t)D * j;
+                double dx[3] = {0.0, 0.0, 0.0};
+                for (int k = 0; k < D; ++k) dx[k] = xj[k] - xi[k];
+                const double r2 = dotn(dx, dx, D);
+                b = squared_bin(&d->distance, pv->sq, r2);
+                if (!(b >= 1 && b <= pv->nd)) continue;
+                for (int k = 0; k < D; ++k) du[k] = uj[k] - ui[k];
+                const double inv_r = 1.0 / sqrt(r2);
+                duL = dotn(du, dx, D) * inv_r;
+            } else {
+                double r, tA[2], tB[2];
+                const int ok = oracle_sphere_frame((const double*)&P[i], (const double*)&P[j], d->radius, &r, tA, tB);
+                b = oracle_digitize(&d->distance, r);
+                if (!(ok && b >= 1 && b <= pv->nd)) continue;
+                sphere_delta(D, tA, tB, ui, uj, du);
+                duL = du[0];  /* dot(du, e1) */
+            }
+            sp_add(sums, counts, abss, b - 1, duL, dotn(du, du, D));
+        }
+    }
+}
+
+/* _sp1d_derive_rows! (serial_single_pass.jl:209-219): T2 = S2 - L2, L1T2 = S3 - L3, counts of row 0
+ * copied to every row. Idempotent (assignments). */
+OR_EXPORT void oracle_single_pass_derive(double* sums, uint64_t* counts, int64_t nb)
+{
+    for (int64_t b = 0; b < nb; ++b) {
+        sums[2 + SP_N * b] = sums[0 + SP_N * b] - sums[1 + SP_N * b];
+        sums[5 + SP_N * b] = sums[3 + SP_N * b] - sums[4 + SP_N * b];
+        for (int t = 1; t < SP_N; ++t) counts[t + SP_N * b] = counts[SP_N * b];
+    }
+}
+
+/* The six-invariant single pass over rows i0, i0 + istep, ... accumulated into (6, nb) sums/counts
+ * (and, if abss is not NULL, the per-bin sums of |value| of the four accumulated rows). The derived
+ * rows are NOT filled here: a caller that splits the rows over workers adds the partial results first
+ * and then calls oracle_single_pass_derive once. `desc` supplies geometry, distance bins and
+ * dimension; its operators are ignored. */
+OR_EXPORT int oracle_run_single_pass(const sfb200_plan_desc* d, const double* x, const double* u, int64_t N,
+                                     int64_t i0, int64_t istep, double* sums, uint64_t* counts, double* abss)
+{
+    double sqbuf[4096];
+    if (d->distance.n_edges > 4096 || d->joint) return -1;
+    plan_view pv;
+    plan_view_init(&pv, d, sqbuf);
+    sph_point* P = NULL;
+    if (d->geometry == SFB200_GEOM_SPHERE) {
+        P = sphere_points(d, x, N);
+        if (!P) return -1;
+    }
+    sp_rows(&pv, x, u, P, N, i0, istep > 0 ? istep : 1, sums, counts, abss);
+    free(P);
     return 0;
 }
 

@@ -126,6 +126,7 @@ struct sfb200_plan {
     int shard_index = 0, shard_count = 1;  // sfb200_run covers shard shard_index of shard_count
     int cols_ovr = 0;     // run-length histogram columns (0 auto)
     int sort_ovr = -1;    // J-tile order of the flat 1D kernels: -1 auto (sorted), 0 storage order, 1 sorted
+    unsigned long long* d_range = nullptr;  // sfb200_distance_range: min / max key bits
 };
 
 // ------------------------------------------------------------------------------- errors
@@ -568,7 +569,7 @@ static void free_plan_device(sfb200_plan* p)
 {
     free_workspace(p->ws, true);
     cudaFree(p->d_exact); cudaFree(p->d_vedges); cudaFree(p->d_lut64); cudaFree(p->d_ck);
-    cudaFree(p->d_lut32); cudaFree(p->d_rowlo); cudaFree(p->d_vwin); cudaFree(p->d_lut8);
+    cudaFree(p->d_lut32); cudaFree(p->d_rowlo); cudaFree(p->d_vwin); cudaFree(p->d_lut8); cudaFree(p->d_range);
 }
 
 extern "C" int sfb200_plan_destroy(sfb200_plan* p)
@@ -646,6 +647,8 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
     else if (d.n_ops == 1 && codes[0] == OC_L1) p->opl = OPL_L1;
     else if (d.n_ops == 4 && codes[0] == OC_L2 && codes[1] == OC_T2 && codes[2] == OC_L3 && codes[3] == OC_T3)
         p->opl = OPL_QUAD;
+    else if (d.n_ops == 4 && codes[0] == OC_S2 && codes[1] == OC_L2 && codes[2] == OC_S3 && codes[3] == OC_L3)
+        p->opl = OPL_SP;
     p->nops_pad = d.n_ops;
     if (p->opl < 0) {
         if (d.n_ops == 1) p->opl = OPL_GEN1;
@@ -777,7 +780,7 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         p->lut64_bytes = (int)(lut.size() * sizeof(LutEntry64));
         if ((e = upload(&p->d_lut64, lut.data(), lut.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload table");
     }
-    if (!p->sphere && !p->joint && !dlinear && !p->fp32) {
+    if (!p->sphere && !dlinear && !p->fp32 && (!p->joint || p->mixed)) {
         std::vector<unsigned char> bt;
         if (build_byte_table(p->exact_tab, bt) && (e = upload(&p->d_lut8, bt.data(), bt.size())) != cudaSuccess)
             return cuda_fail(ctx, e, "upload byte table");
@@ -1080,9 +1083,11 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
     const int NW = T / 32, NBP = p->nb + 2, NV = p->nops_pad;
     if (p->mixed) {
         const int rec = p->sphere ? 10 : 2 * p->D;  // doubles per j record
-        if (p->joint)
-            return (size_t)lut_bytes + (size_t)rec * T * 8 + ((size_t)p->nb * p->nv + (size_t)p->nb * p->nfine) * 8 +
+        if (p->joint) {
+            const size_t ndp = (size_t)((p->nb + 31) & ~31);  // slots per value bin (swizzled rows)
+            return (size_t)lut_bytes + (size_t)rec * T * 8 + (ndp * p->nv + ndp * p->nfine) * 8 +
                    (size_t)p->nv * 12;  // + value-bin centres (FP64 and FP32)
+        }
         return (size_t)lut_bytes + (size_t)rec * T * 8 + hist_bytes(true, NV, priv, NW, NBP, lc);
     }
     if (p->joint) {
@@ -1205,8 +1210,9 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     sfb200_ctx* ctx = p->ctx;
     const bool dlinear = p->desc.distance.kind == SFB200_BINS_LINEAR;
     int lut_bytes = 0;
-    // flat 1D kernels of precision FP64 / MIXED bin with the byte table when the plan has one
-    const bool byte_lut = p->d_lut8 && !p->joint && !p->sphere && !p->fp32;
+    // flat kernels of precision FP64 / MIXED (1D) and MIXED (joint) bin with the byte table when the
+    // plan has one
+    const bool byte_lut = p->d_lut8 && !p->sphere && !p->fp32 && (!p->joint || p->mixed);
     if (byte_lut) lut_bytes = kByteCells + (int)sizeof(double) * kByteEdges;
     else if (p->fp32) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
     else if (p->mixed) lut_bytes = p->lut64_bytes;  // exact table (flat) or chord table (sphere); 0 if linear
@@ -1441,6 +1447,52 @@ extern "C" int sfb200_run(sfb200_plan* p, const void* x, const void* u, int64_t 
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) p->stats.kernel_ms = ms;
         p->stats_pending = false;
+    }
+    return SFB200_OK;
+}
+
+// Smallest and largest pair distance over all pairs i < j (the reference's auto-binning scan,
+// _minmax_matrix_for_autobins / minmax_i, src/Calculations/dispatch.jl:205-298), on the device.
+extern "C" int sfb200_distance_range(sfb200_plan* p, const void* x, const void* u, int64_t n, uint32_t flags,
+                                     double* dmin, double* dmax, void* stream)
+{
+    if (!p) return SFB200_ERR_INVALID_ARG;
+    sfb200_ctx* ctx = p->ctx;
+    if (!dmin || !dmax) return set_err(ctx, SFB200_ERR_INVALID_ARG, "dmin/dmax pointer is NULL");
+    if (n < 2) return set_err(ctx, SFB200_ERR_INVALID_ARG, "a distance range needs at least 2 points");
+    if (n > (1ll << 31) - 1024) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "more than 2^31 points");
+    if (!x || !u) return set_err(ctx, SFB200_ERR_INVALID_ARG, "x/u pointer is NULL");
+    if (flags & ~SFB200_RUN_DEVICE_INPUT)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "sfb200_distance_range takes only SFB200_RUN_DEVICE_INPUT");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    int launches = 0;
+    int rc = prepare_inputs(p, p->ws, x, u, n, flags, s, &launches);
+    if (rc) return rc;
+    if (!p->d_range) CK(cudaMalloc((void**)&p->d_range, 2 * sizeof(unsigned long long)));
+    static const unsigned long long init[2] = {0x7ff0000000000000ull, 0ull};  // +inf, +0
+    CK(cudaMemcpyAsync(p->d_range, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const int ntiles = (int)((n + 255) / 256);
+    const long long ntp = (long long)ntiles * (ntiles + 1) / 2;
+    const unsigned grid = (unsigned)std::min<long long>(ntp, (long long)ctx->nsm * 4);
+    if (p->sphere) k_key_range<3, true><<<grid, 256, 0, s>>>(p->ws.d_X64, (int)n, ntiles, ntp, p->d_range);
+    else if (p->D == 2) k_key_range<2, false><<<grid, 256, 0, s>>>(p->ws.d_X64, (int)n, ntiles, ntp, p->d_range);
+    else k_key_range<3, false><<<grid, 256, 0, s>>>(p->ws.d_X64, (int)n, ntiles, ntp, p->d_range);
+    CK(cudaGetLastError());
+    unsigned long long h[2];
+    CK(cudaMemcpyAsync(h, p->d_range, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const double kmin = bits_to_double(h[0]), kmax = bits_to_double(h[1]);
+    if (!p->sphere) {
+        *dmin = std::sqrt(kmin);  // sqrt is monotone and correctly rounded: min of the distances
+        *dmax = std::sqrt(kmax);
+    } else {
+        // arc length R sigma, sigma = 2 atan(|d|, |s|) with |s|^2 = 4 - |d|^2 (the pair frame's angle)
+        auto arc = [&](double c2) {
+            return p->desc.radius * 2.0 * std::atan2(std::sqrt(c2), std::sqrt(std::max(4.0 - c2, 0.0)));
+        };
+        *dmin = arc(kmin);
+        *dmax = arc(kmax);
     }
     return SFB200_OK;
 }

@@ -36,6 +36,7 @@ static KernelChoice flat_by_list(int opl, int priv)
     case OPL_L3: return flat_entry<D, MODE, OpList<OC_L3>, true>(priv);
     case OPL_L1: return flat_entry<D, MODE, OpList<OC_L1>, true>(priv);
     case OPL_QUAD: return flat_entry<D, MODE, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, true>(priv);
+    case OPL_SP: return flat_entry<D, MODE, OpList<OC_S2, OC_L2, OC_S3, OC_L3>, false>(priv);
     case OPL_GEN1: return flat_entry<D, MODE, OpList<OC_GEN>, false>(priv);
     case OPL_GEN2: return flat_entry<D, MODE, OpList<OC_GEN, OC_GEN>, false>(priv);
     case OPL_GEN4: return flat_entry<D, MODE, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv);

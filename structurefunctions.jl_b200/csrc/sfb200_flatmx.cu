@@ -32,6 +32,7 @@ static KernelChoice flatmx_by_list(int opl, int priv)
     case OPL_L3: return flatmx_entry<D, OpList<OC_L3>, true>(priv);
     case OPL_L1: return flatmx_entry<D, OpList<OC_L1>, true>(priv);
     case OPL_QUAD: return flatmx_entry<D, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, true>(priv);
+    case OPL_SP: return flatmx_entry<D, OpList<OC_S2, OC_L2, OC_S3, OC_L3>, false>(priv);
     case OPL_GEN1: return flatmx_entry<D, OpList<OC_GEN>, false>(priv);
     case OPL_GEN2: return flatmx_entry<D, OpList<OC_GEN, OC_GEN>, false>(priv);
     case OPL_GEN4: return flatmx_entry<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv);
@@ -57,6 +58,7 @@ static KernelChoice flat1d_mx_batch_by_list(int opl)
     case OPL_L3: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_L3>, 3>), 256, 3};
     case OPL_L1: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_L1>, 3>), 256, 3};
     case OPL_QUAD: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, 3>), 256, 3};
+    case OPL_SP: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_S2, OC_L2, OC_S3, OC_L3>, 3>), 256, 3};
     case OPL_GEN1: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_GEN>, 3>), 256, 3};
     case OPL_GEN2: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_GEN, OC_GEN>, 3>), 256, 3};
     case OPL_GEN4: return {reinterpret_cast<const void*>(&k_flat1d_mx_batch<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, 3>), 256, 3};

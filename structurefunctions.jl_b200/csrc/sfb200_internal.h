@@ -20,7 +20,8 @@ enum OpListId : int {
     OPL_GEN1 = 4,
     OPL_GEN2 = 5,
     OPL_GEN4 = 6,
-    OPL_GEN8 = 7
+    OPL_GEN8 = 7,
+    OPL_SP = 8         // {S2SF, L2SF, S3SF, L3SF}: the accumulated rows of the six-invariant single pass
 };
 
 struct KernelChoice {

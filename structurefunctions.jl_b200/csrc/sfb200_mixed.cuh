@@ -567,22 +567,32 @@ struct SplitWords {
     }
 };
 
+// Shared-memory slot of joint cell (distance bin d0, value bin v0), both 0-based, in rows of ndp
+// slots (nd rounded up to a multiple of 32) per value bin. The distance index is XOR-ed with the low 5
+// bits of the value bin: without it a slot's bank (slot mod 32) would be the distance bin's alone, and
+// the lanes of a warp, whose pairs crowd into the few most populated distance bins, would queue on the
+// same banks; with it, lanes of equal distance bin but different value bins take different banks. The
+// XOR permutes each row's aligned groups of 32 slots, so it is a bijection on [0, ndp).
+__device__ __forceinline__ int joint_slot(int d0, int v0, int ndp) { return v0 * ndp + (d0 ^ (v0 & 31)); }
+
 __device__ __forceinline__ void joint_flush_packed(const PairArgs& a, const SplitWords& hcell,
-                                                   const SplitWords& hfine, int ncell, const double* vcen)
+                                                   const SplitWords& hfine, int ndp, const double* vcen)
 {
     const int nd = a.nb;
-    for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
+    const int nslot = ndp * a.nv;
+    for (int k = threadIdx.x; k < nslot; k += blockDim.x) {
         if (!(hcell.lo[k] | hcell.hi[k])) continue;
         const unsigned long long w = hcell.take(k);
         const unsigned long long cnt = (w + (1ull << 43)) >> 44;
         const long long off = (long long)(w - (cnt << 44));
-        const int vb = k / nd + 1;
-        double s = (double)cnt * vcen[vb - 1] + (double)off * a.vqc_inv;
-        const int f = vb - a.vfine_lo;
-        if ((unsigned)f < (unsigned)a.nfine)
-            s += (double)(long long)hfine.take((k - (vb - 1) * nd) + nd * f) * a.vq_inv;
-        atomicAdd(&a.g_sums[k], s);
-        atomicAdd(&a.g_counts[k], cnt);
+        const int v0 = k / ndp;
+        const int d0 = (k - v0 * ndp) ^ (v0 & 31);  // slots of distance bins >= nd are never written
+        double s = (double)cnt * vcen[v0] + (double)off * a.vqc_inv;
+        const int f = v0 + 1 - a.vfine_lo;
+        if ((unsigned)f < (unsigned)a.nfine) s += (double)(long long)hfine.take(joint_slot(d0, f, ndp)) * a.vq_inv;
+        const int cell = d0 + nd * v0;
+        atomicAdd(&a.g_sums[cell], s);
+        atomicAdd(&a.g_counts[cell], cnt);
     }
     __syncthreads();
 }
@@ -646,19 +656,21 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     const int T = blockDim.x;
     const int n = a.n;
     const int nd = a.nb, nv = a.nv;
-    const int ncell = nd * nv;
-    LutEntry64* lut = reinterpret_cast<LutEntry64*>(smem);
+    const int ndp = (nd + 31) & ~31;  // slots per value bin (joint_slot)
+    const int ncell = ndp * nv;
+    const LutEntry64* lut = reinterpret_cast<const LutEntry64*>(smem);
+    const unsigned char* lut8 = smem;
+    const double* sqx = reinterpret_cast<const double*>(smem + kByteCells);
     double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);                                 // T * 2NP
     unsigned* words = reinterpret_cast<unsigned*>(srec + (size_t)2 * NP * T);
-    const int nfw = nd * a.nfine;
+    const int nfw = ndp * a.nfine;
     const SplitWords hcell{words, words + ncell};                                  // 2 x ncell
-    const SplitWords hfine{words + 2 * ncell, words + 2 * ncell + nfw};            // 2 x nd * nfine
+    const SplitWords hfine{words + 2 * ncell, words + 2 * ncell + nfw};            // 2 x ndp * nfine
     double* vcen = reinterpret_cast<double*>(words + 2 * (ncell + nfw));           // nv
     float* vc32 = reinterpret_cast<float*>(vcen + nv);                             // nv
     __shared__ unsigned long long s_recheck;
 
-    for (int k = threadIdx.x; k < a.lut_bytes / (int)sizeof(LutEntry64); k += T)
-        lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
+    load_bin_table(a, smem);
     for (int k = threadIdx.x; k < 2 * (ncell + nfw); k += T) words[k] = 0u;
     if (threadIdx.x == 0) s_recheck = 0ull;
     unsigned my_recheck = 0;
@@ -696,7 +708,7 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     for (long long p = p0; p < p1; p += ps, ++iter) {
         if (iter && iter % a.flush_every == 0) {
             __syncthreads();
-            joint_flush_packed(a, hcell, hfine, ncell, vcen);
+            joint_flush_packed(a, hcell, hfine, ndp, vcen);
         }
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
@@ -741,11 +753,16 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                 const double h2 = SFB_ADD(SFB_MUL(dx[0], dx[0]), SFB_MUL(dx[1], dx[1]));
                 double r2 = h2;
                 if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
-                if (a.dist_linear) db = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
-                else db = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+                if (a.byte_lut) {
+                    db = byte_bin(lut8, sqx, r2, slow);  // slow: the exact route decides the bin
+                } else {
+                    if (a.dist_linear) db = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
+                    else db = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+                    slow = !f32_range_ok(f32(r2));
+                }
                 // flat bins are exact: a pair outside the distance range needs no value
-                if (db < 1 || db > nd) return r;
-                fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q) && f32_range_ok(f32(r2));
+                if (!slow && (db < 1 || db > nd)) return r;
+                fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q);
             }
             float v[1];
             eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
@@ -781,10 +798,10 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                 ++my_recheck;
             }
             if (ok && db >= 1 && db <= nd && vb >= 1 && vb <= nv) {
-                r.cell = (db - 1) + nd * (vb - 1);
+                r.cell = joint_slot(db - 1, vb - 1, ndp);
                 const int f = vb - a.vfine_lo;
                 if ((unsigned)f < (unsigned)a.nfine) {  // near zero: the offset goes to the fine word
-                    r.fidx = (db - 1) + nd * f;
+                    r.fidx = joint_slot(db - 1, f, ndp);
                     r.fq = fq;
                 } else {
                     r.q = q;
@@ -810,7 +827,7 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     }
     if (my_recheck) atomicAdd(&s_recheck, (unsigned long long)my_recheck);
     __syncthreads();
-    joint_flush_packed(a, hcell, hfine, ncell, vcen);
+    joint_flush_packed(a, hcell, hfine, ndp, vcen);
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 

@@ -370,6 +370,60 @@ __global__ void k_value_windows(const double* __restrict__ row_key_lo, ValueWind
     }
 }
 
+// Smallest and largest pair key over all pairs i < j of the packed points: r^2 (flat; the reference's
+// left-to-right sum of squared differences) or the squared chord |q - p|^2 of the unit position
+// vectors (sphere). Tile pairs of 256 points as the pair kernels; each thread keeps its row's range,
+// each warp reduces, and lane 0 folds it into out[0] (min) / out[1] (max) with 64-bit integer
+// atomics on the keys' bit patterns (keys are >= 0, whose IEEE bits order like the values). NaN keys
+// are skipped (fmin / fmax), as the reference's `<` comparisons skip them. out must hold +inf / 0.
+template <int NC, bool SPHERE>
+__global__ void __launch_bounds__(256) k_key_range(const double* __restrict__ X64, int n, int ntiles, long long ntp,
+                                                   unsigned long long* out)
+{
+    __shared__ double sx[NC * 256];
+    const int t = threadIdx.x;
+    double mn = INFINITY, mx = 0.0;
+    for (long long p = blockIdx.x; p < ntp; p += gridDim.x) {
+        int ti, tj;
+        decode_tile_pair(p, ntiles, ti, tj);
+        const int i = ti * 256 + t;
+        const bool iv = i < n;
+        double xi[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) xi[c] = iv ? X64[(size_t)c * n + i] : 0.0;
+        __syncthreads();
+        const int j0 = tj * 256;
+        const int jn = min(256, n - j0);
+        if (t < jn) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) sx[c * 256 + t] = X64[(size_t)c * n + j0 + t];
+        }
+        __syncthreads();
+        if (iv) {
+            for (int jj = (ti == tj) ? t + 1 : 0; jj < jn; ++jj) {
+                double k = 0.0;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    const double d = __dsub_rn(sx[c * 256 + jj], xi[c]);
+                    k = (c == 0) ? __dmul_rn(d, d) : __dadd_rn(k, __dmul_rn(d, d));
+                }
+                mn = fmin(mn, k);
+                mx = fmax(mx, k);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((t & 31) == 0) {
+        atomicMin(&out[0], (unsigned long long)__double_as_longlong(mn));
+        atomicMax(&out[1], (unsigned long long)__double_as_longlong(mx));
+    }
+}
+
+
 // Device outputs: out = (accumulate ? out : 0) + accumulated histogram.
 __global__ void k_finalize(const double* __restrict__ s, const unsigned long long* __restrict__ c,
                            long long ns, long long nc, double* out_s, unsigned long long* out_c,

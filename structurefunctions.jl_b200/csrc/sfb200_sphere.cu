@@ -33,6 +33,7 @@ static KernelChoice sphere_by_list(int opl, int priv)
     case OPL_L3: return sphere_entry<D, MIXED, OpList<OC_L3>, true>(priv);
     case OPL_L1: return sphere_entry<D, MIXED, OpList<OC_L1>, true>(priv);
     case OPL_QUAD: return sphere_entry<D, MIXED, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, true>(priv);
+    case OPL_SP: return sphere_entry<D, MIXED, OpList<OC_S2, OC_L2, OC_S3, OC_L3>, false>(priv);
     case OPL_GEN1: return sphere_entry<D, MIXED, OpList<OC_GEN>, false>(priv);
     case OPL_GEN2: return sphere_entry<D, MIXED, OpList<OC_GEN, OC_GEN>, false>(priv);
     case OPL_GEN4: return sphere_entry<D, MIXED, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv);

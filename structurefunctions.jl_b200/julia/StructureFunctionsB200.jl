@@ -297,11 +297,111 @@ function SFC._dispatch_execution_backend!(
     accumulate_into!(b, (sf,), x, u, distance_bins, value_bins, distance_metric, sums_2d, counts_2d)
 end
 
-# auxiliary-axis shapes are not on this path (as the GPU in-place route, dispatch.jl:406-410)
-SFC._dispatch_execution_backend(b::B200Backend, shape::SFC.AbstractFieldShape, args...; kwargs...) =
-    throw(ArgumentError("auxiliary-axis inputs are not implemented for B200Backend"))
-SFC._dispatch_execution_backend!(b::B200Backend, shape::SFC.AbstractFieldShape, args...; kwargs...) =
-    throw(ArgumentError("in-place auxiliary-axis calculate_structure_function! is not implemented for B200Backend"))
+# ---------------------------------------------------------------------- six-invariant single pass
+#
+# calculate_structure_functions_single_pass[!] (src/Calculations/serial_single_pass.jl:408-421, 663-693)
+# route here through _dispatch_single_pass[!]. One fused pass accumulates S2, L2, S3, L3 (operator
+# list {S2, L2, S3, L3}); rows T2 = S2 - L2 and L1T2 = S3 - L3 and the shared count row are filled
+# by the reference's own _sp1d_derive_rows! (serial_single_pass.jl:209-219).
+
+const SP_ACCUMULATED = (SFT.SecondOrderStructureFunctionType(), SFT.LongitudinalSecondOrderStructureFunctionType(),
+                        SFT.ThirdOrderStructureFunctionType(), SFT.DiagonalConsistentThirdOrderStructureFunctionType())
+const SP_ROWS = (1, 2, 4, 5)
+
+# Adds the four accumulated rows of one pass into `sums` / `counts` ((6, n_bins)); derives the rest.
+function single_pass_into!(b::B200Backend, sums::AbstractMatrix, counts::AbstractMatrix, x, u, distance_bins,
+                           metric)
+    nb = length(distance_bins) - 1
+    size(sums) == (SFC.SINGLE_PASS_N, nb) ||
+        throw(DimensionMismatch("sums must have shape ($(SFC.SINGLE_PASS_N), n_bins); got $(size(sums))"))
+    size(counts) == size(sums) || throw(DimensionMismatch("counts must have shape $(size(sums))"))
+    s = zeros(Float64, 4 * nb)
+    c = zeros(UInt64, nb)
+    run_pairs(b, SP_ACCUMULATED, x, u, distance_bins, nothing, metric, s, c, UInt32(0))
+    for (k, row) in enumerate(SP_ROWS)
+        @views sums[row, :] .+= s[(k - 1) * nb + 1:k * nb]
+    end
+    @views counts[1, :] .+= c
+    SFC._sp1d_derive_rows!(sums, counts)
+    return sums, counts
+end
+
+function SFC._dispatch_single_pass(
+    b::B200Backend, ::SFC.PointField, x::AbstractMatrix{FT1}, u::AbstractMatrix{FT2}, distance_bins::AbstractVector;
+    count_eltype::Type{CT} = UInt32, distance_metric::DI.PreMetric = DI.Euclidean(), kwargs...,
+) where {FT1, FT2, CT}
+    OT = promote_type(float(FT1), float(FT2))
+    nb = length(distance_bins) - 1
+    sums = zeros(OT, SFC.SINGLE_PASS_N, nb)
+    counts = zeros(CT, SFC.SINGLE_PASS_N, nb)
+    single_pass_into!(b, sums, counts, x, u, distance_bins, distance_metric)
+    return (sums = sums, counts = counts)
+end
+
+function SFC._dispatch_single_pass!(
+    b::B200Backend, sums::AbstractMatrix, counts::AbstractMatrix, x::AbstractMatrix, u::AbstractMatrix,
+    distance_bins::AbstractVector; distance_metric::DI.PreMetric = DI.Euclidean(), kwargs...,
+)
+    return single_pass_into!(b, sums, counts, x, u, distance_bins, distance_metric)
+end
+
+# auxiliary-axis shapes (src/Calculations/shapes.jl:19-20): one pair pass per auxiliary slice, results
+# of shape (n_bins, aux...) / (n_dist, n_val, aux...) as the reference's batch drivers return them
+# (src/Calculations/batch.jl:209-217)
+aux_slices(x, u) = (ndims(x) == 2 ? (x, view(u, :, :, k)) : (view(x, :, :, k), view(u, :, :, k))
+                    for k in CartesianIndices(size(u)[3:end]))
+
+function SFC._dispatch_execution_backend(
+    b::B200Backend, shape::SFC.AbstractFieldShape, sf::SFT.AbstractPairwiseStructureFunctionType, x, u,
+    distance_bins, count_eltype::Type{CT} = UInt32; distance_metric::DI.PreMetric = DI.Euclidean(), kwargs...,
+) where {CT}
+    nb = length(distance_bins) - 1
+    aux = size(u)[3:end]
+    sums = zeros(out_type(x, u), nb, aux...)
+    counts = zeros(CT, nb, aux...)
+    s = zeros(Float64, nb)
+    c = zeros(UInt64, nb)
+    for (k, (xb, ub)) in zip(CartesianIndices(aux), aux_slices(x, u))
+        run_pairs(b, (sf,), xb, ub, distance_bins, nothing, distance_metric, s, c, UInt32(0))
+        @views sums[:, k] .= s
+        @views counts[:, k] .= c
+    end
+    return SFO.StructureFunctionSumsAndCounts(sf, distance_bins, sums, counts)
+end
+
+function SFC._dispatch_execution_backend(
+    b::B200Backend, shape::SFC.AbstractFieldShape, sf::SFT.AbstractPairwiseStructureFunctionType, x, u,
+    distance_bins, value_bins::AbstractVector; distance_metric::DI.PreMetric = DI.Euclidean(),
+    count_eltype::Type{CT} = UInt32, kwargs...,
+) where {CT}
+    nd, nv = length(distance_bins) - 1, length(value_bins) - 1
+    aux = size(u)[3:end]
+    sums = zeros(out_type(x, u), nd, nv, aux...)
+    counts = zeros(CT, nd, nv, aux...)
+    s = zeros(Float64, nd * nv)
+    c = zeros(UInt64, nd * nv)
+    for (k, (xb, ub)) in zip(CartesianIndices(aux), aux_slices(x, u))
+        run_pairs(b, (sf,), xb, ub, distance_bins, value_bins, distance_metric, s, c, UInt32(0))
+        @views sums[:, :, k] .= reshape(s, nd, nv)
+        @views counts[:, :, k] .= reshape(c, nd, nv)
+    end
+    return SFO.StructureFunction2DSumsAndCounts(sf, distance_bins, value_bins, sums, counts)
+end
+
+function SFC._dispatch_execution_backend!(
+    b::B200Backend, shape::SFC.AbstractFieldShape, sums, counts, sf::SFT.AbstractPairwiseStructureFunctionType,
+    x, u, distance_bins, value_bins::AbstractVector...; distance_metric::DI.PreMetric = DI.Euclidean(), kwargs...,
+)
+    for (k, (xb, ub)) in zip(CartesianIndices(size(u)[3:end]), aux_slices(x, u))
+        if isempty(value_bins)
+            accumulate_into!(b, (sf,), xb, ub, distance_bins, nothing, distance_metric, view(sums, :, k), view(counts, :, k))
+        else
+            accumulate_into!(b, (sf,), xb, ub, distance_bins, value_bins[1], distance_metric, view(sums, :, :, k),
+                             view(counts, :, :, k))
+        end
+    end
+    return nothing
+end
 
 # ---------------------------------------------------------------------- serving (many requests)
 #

@@ -117,6 +117,7 @@ EXPORTED_SYMBOLS = (
     "sfb200_plan_set_launch",
     "sfb200_plan_set_option",
     "sfb200_shard_bounds",
+    "sfb200_distance_range",
     "sfb200_slice_create",
     "sfb200_slice_get_info",
     "sfb200_batch_run",

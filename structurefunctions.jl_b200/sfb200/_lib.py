@@ -73,6 +73,9 @@ def load():
         lib.sfb200_shard_bounds.argtypes = [C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int64),
                                             C.POINTER(C.c_int64)]
         lib.sfb200_shard_bounds.restype = C.c_int
+        lib.sfb200_distance_range.argtypes = [P, P, P, C.c_int64, C.c_uint32, C.POINTER(C.c_double),
+                                              C.POINTER(C.c_double), P]
+        lib.sfb200_distance_range.restype = C.c_int
         lib.sfb200_run_noalloc.argtypes = [P, P, P, C.c_int64, C.c_uint32, P, P, P]
         lib.sfb200_run_noalloc.restype = C.c_int
         if lib.sfb200_abi_version() != _abi.ABI_VERSION:
@@ -225,6 +228,13 @@ class Plan:
     def run(self, x_ptr, u_ptr, n, flags, sums_ptr, counts_ptr, stream=None):
         check(load().sfb200_run(self.ptr, x_ptr, u_ptr, int(n), int(flags), sums_ptr, counts_ptr, stream),
               self.ctx.ptr, "run")
+
+    def distance_range(self, x_ptr, u_ptr, n, flags=0, stream=None):
+        """(min, max) pair distance over all pairs (sfb200_distance_range)."""
+        lo, hi = C.c_double(), C.c_double()
+        check(load().sfb200_distance_range(self.ptr, x_ptr, u_ptr, int(n), int(flags), C.byref(lo), C.byref(hi),
+                                           stream), self.ctx.ptr, "distance range")
+        return lo.value, hi.value
 
     def stats(self):
         st = _abi.Stats()

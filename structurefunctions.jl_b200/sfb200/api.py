@@ -18,7 +18,8 @@ import weakref
 import numpy as np
 
 from . import _abi, _lib, autotune
-from .bins import AbstractBinEdges, as_bin_edges
+from . import operators as ops_module
+from .bins import AbstractBinEdges, LinearBinEdges, LogBinEdges, as_bin_edges
 from .errors import ArgumentError, DimensionMismatch
 from .metrics import Euclidean, pair_geometry_for
 from .operators import AbstractDerivedStructureFunctionType, AbstractPairwiseStructureFunctionType
@@ -95,8 +96,27 @@ def default_backend():
 class PointField:
     """u is (D, N) (src/Calculations/shapes.jl:18)."""
 
+    aux = ()
+
     def __init__(self, D):
         self.D = D
+
+
+class SharedPositionField:
+    """x is (W, N), u is (D, N, auxiliary...): one geometry, several fields (src/Calculations/shapes.jl:19)."""
+
+    def __init__(self, D, aux):
+        self.D = D
+        self.aux = tuple(aux)
+
+
+class VaryingPositionField:
+    """x is (W, N, auxiliary...) and u is (D, N, auxiliary...) with the same auxiliary axes
+    (src/Calculations/shapes.jl:20)."""
+
+    def __init__(self, D, aux):
+        self.D = D
+        self.aux = tuple(aux)
 
 
 def _shape_of(a):
@@ -127,17 +147,15 @@ def validate_array_shape(x, u, distance_metric):
             f"x and u must share axis-2 point count N; got size(x,2)={xs[1]} and size(u,2)={us[1]}")
     if len(xs) == 2 and len(us) == 2:
         return PointField(D)
-    aux = ArgumentError("auxiliary-axis (batched) inputs are not implemented for B200Backend; "
-                        "pass (Dx, N)/(D, N) arrays")
-    if len(xs) == 2 and len(us) >= 3:  # SharedPositionField in the reference
-        raise aux
-    if len(xs) >= 3 and len(us) >= 3:  # VaryingPositionField in the reference
+    if len(xs) == 2 and len(us) >= 3:
+        return SharedPositionField(D, us[2:])
+    if len(xs) >= 3 and len(us) >= 3:
         if len(xs) != len(us):
             raise DimensionMismatch(
                 f"varying-position inputs must have the same rank; got ndims(x)={len(xs)} and ndims(u)={len(us)}")
         if xs[2:] != us[2:]:
             raise DimensionMismatch(f"varying-position inputs must share auxiliary axes; got {xs[2:]} and {us[2:]}")
-        raise aux
+        return VaryingPositionField(D, us[2:])
     raise DimensionMismatch(
         f"unsupported shape combination: x has shape {xs}, u has shape {us}; valid forms are (Dx,N)/(D,N), "
         "(Dx,N)/(D,N,auxiliary...), or matched (Dx,N,auxiliary...) arrays")
@@ -276,6 +294,69 @@ def _run(backend, ops, x, u, distance_bins, value_bins, distance_metric):
     return sums, counts, plan, xcode, ucode
 
 
+def _aux_slices(shape, x, u):
+    """The (x_b, u_b) point sets of an auxiliary-axis input, in column-major order of the auxiliary
+    axes (b runs fastest along the first auxiliary axis, as Julia's linear indexing)."""
+    B = int(np.prod(shape.aux))
+    shared = isinstance(shape, SharedPositionField)
+
+    def flat(a):
+        if _is_torch(a):
+            return a.permute(*range(a.dim() - 1, 1, -1), 0, 1).reshape(B, a.shape[0], a.shape[1]) \
+                if a.dim() > 3 else a.permute(2, 0, 1)
+        arr = np.asarray(a)
+        return np.reshape(arr, (arr.shape[0], arr.shape[1], B), order="F").transpose(2, 0, 1)
+
+    us = flat(u)
+    xs = None if shared else flat(x)
+    return [(x if shared else xs[b], us[b]) for b in range(B)]
+
+
+def _run_aux(backend, ops, shape, x, u, distance_bins, value_bins, distance_metric):
+    """The pair loop over every auxiliary-axis slice. Precision MIXED runs all slices as resident
+    slices in batched rounds (one persistent launch per kernel variant and round; sfb200_batch_run),
+    the other precisions one sfb200_run per slice. Returns per-slice (sums, counts) lists plus the
+    input codes."""
+    pieces = _aux_slices(shape, x, u)
+    out = []
+    if backend.precision == "mixed" and len(pieces) > 1:
+        xp0, _, xcode, xdev = _prepare(pieces[0][0])
+        up0, _, ucode, udev = _prepare(pieces[0][1])
+        dt = {_abi.F64: np.float64, _abi.F32: np.float32}
+        geom = pair_geometry_for(distance_metric, shape.D)
+        desc, keep = plan_description(ops, shape.D, distance_bins, value_bins, distance_metric, "mixed", dt[xcode],
+                                      dt[ucode])
+        key = (tuple(ops), as_bin_edges(distance_bins), value_bins is not None and as_bin_edges(value_bins), geom,
+               xcode, ucode)
+        plan = backend.plan(key, desc, keep)
+        ctx = backend.context
+        chunk = 256  # resident slices per round
+        for c0 in range(0, len(pieces), chunk):
+            slices, keepalive = [], []
+            try:
+                for xb, ub in pieces[c0:c0 + chunk]:
+                    xp, xk, _, _ = _prepare(xb)
+                    up, uk, _, _ = _prepare(ub)
+                    keepalive.append((xk, uk))
+                    slices.append(_lib.Slice(plan, xp, up, _shape_of(xb)[1], _abi.RUN_DEVICE_INPUT if xdev else 0))
+                _lib.batch_run(ctx, slices, [0] * len(slices), [sl.tile_pairs for sl in slices])
+                _lib.batch_wait(ctx)
+                for sl in slices:
+                    sb = np.zeros(plan.n_sums)
+                    cb = np.zeros(plan.n_counts, dtype=np.uint64)
+                    sl.read(sb.ctypes.data, cb.ctypes.data)
+                    out.append((sb, cb))
+            finally:
+                for sl in slices:
+                    sl.close()
+        return out, xcode, ucode
+    xcode = ucode = None
+    for xb, ub in pieces:
+        sb, cb, plan, xcode, ucode = _run(backend, ops, xb, ub, distance_bins, value_bins, distance_metric)
+        out.append((sb, cb))
+    return out, xcode, ucode
+
+
 def _split_args(args):
     """(value_bins?, count_eltype?) from the positional tail, as the reference's methods take them."""
     value_bins, count_eltype = None, np.uint32
@@ -299,20 +380,69 @@ def _is_dtype_like(v):
         return False
 
 
+def distance_range(x, u, distance_metric=None, backend=None):
+    """(min, max) distance over all pairs of the points, on the device (sfb200_distance_range): the
+    scan of the reference's auto-binning (_minmax_matrix_for_autobins / minmax_i,
+    src/Calculations/dispatch.jl:205-298), in the inputs' float type."""
+    distance_metric = Euclidean() if distance_metric is None else distance_metric
+    backend = default_backend() if backend is None else backend
+    shape = validate_array_shape(x, u, distance_metric)
+    geom = pair_geometry_for(distance_metric, shape.D)
+    xp, xkeep, xcode, xdev = _prepare(x)
+    up, ukeep, ucode, udev = _prepare(u)
+    if xdev != udev:
+        raise ArgumentError("x and u must both be host arrays or both be device tensors")
+    n = _shape_of(x)[1]
+    if n < 2:
+        raise ArgumentError("automatic binning needs at least 2 points")
+    dt = {_abi.F64: np.float64, _abi.F32: np.float32}
+    # a plan over placeholder edges: the scan needs only the geometry and the input layout
+    desc, keep = plan_description((ops_module.L2SF,), shape.D, [0.0, 1.0], None, distance_metric, backend.precision,
+                                  dt[xcode], dt[ucode])
+    plan = backend.plan(("distance_range", geom, xcode, ucode), desc, keep)
+    lo, hi = plan.distance_range(xp, up, n, _abi.RUN_DEVICE_INPUT if xdev else 0)
+    ft = np.float32 if xcode == _abi.F32 else np.float64  # float(eltype(x))
+    return ft(lo), ft(hi)
+
+
+def auto_distance_bins(min_distance, max_distance, n_bins, bin_spacing=None):
+    """_auto_distance_bins (src/Calculations/dispatch.jl:190-203): `n_bins` log-spaced (default) or
+    linear bins from prevfloat(min) to max, in the distances' float type."""
+    bin_spacing = LogBinEdges if bin_spacing is None else bin_spacing
+    ft = type(min_distance) if isinstance(min_distance, np.floating) else np.float64
+    lo = np.nextafter(ft(min_distance), ft(-np.inf))
+    hi = ft(max_distance)
+    if bin_spacing is LinearBinEdges:
+        return LinearBinEdges(float(lo), float(hi), int(n_bins) + 1)
+    if bin_spacing is LogBinEdges:
+        e = 10.0 ** np.linspace(np.log10(float(lo)), np.log10(float(hi)), int(n_bins) + 1)
+        e[0], e[-1] = lo, hi
+        return LogBinEdges(e)
+    raise ArgumentError(f"bin_spacing must be LinearBinEdges or LogBinEdges; got {bin_spacing}")
+
+
 def calculate_structure_function(structure_function_type, x, u, distance_bins, *args, backend=None,
                                  output_type=None, distance_metric=None, count_eltype=None, verbose=False,
-                                 show_progress=False):
-    """The reference's `calculate_structure_function` (src/Calculations/dispatch.jl:64-91, 108-136)."""
+                                 show_progress=False, bin_spacing=None):
+    """The reference's `calculate_structure_function` (src/Calculations/dispatch.jl:64-91, 108-136); with
+    an integer `distance_bins`, the auto-binning method (dispatch.jl:153-184): the pair-distance range
+    is scanned on the device and `distance_bins` log-spaced (or, with bin_spacing=LinearBinEdges,
+    linear) bins span it."""
     if isinstance(x, tuple) or isinstance(u, tuple):
         raise ArgumentError("tuple-of-component-vector inputs are not part of the stabilized public API; "
                             "pass arrays with shape (D, N) or (D, N, auxiliary...) instead")
+    if isinstance(distance_bins, (int, np.integer)) and not isinstance(distance_bins, bool):
+        lo, hi = distance_range(x, u, distance_metric, backend)
+        edges = auto_distance_bins(lo, hi, int(distance_bins), bin_spacing)
+        return calculate_structure_function(structure_function_type, x, u, edges, *args, backend=backend,
+                                            output_type=output_type, distance_metric=distance_metric,
+                                            count_eltype=count_eltype, verbose=verbose, show_progress=show_progress)
+    if bin_spacing is not None:
+        raise ArgumentError("bin_spacing only applies to an integer distance_bins (automatic binning)")
     ops, multi = _ops_of(structure_function_type)
     value_bins, ct = _split_args(args)
     if count_eltype is not None:
         ct = count_eltype
-    if isinstance(distance_bins, (int, np.integer)):
-        raise ArgumentError("automatic distance binning (distance_bins::Int) is not implemented for "
-                            "B200Backend; pass bin edges")
     distance_metric = Euclidean() if distance_metric is None else distance_metric
     backend = default_backend() if backend is None else backend
     if not isinstance(backend, B200Backend):
@@ -322,8 +452,11 @@ def calculate_structure_function(structure_function_type, x, u, distance_bins, *
         raise ArgumentError("a joint (distance x value) histogram takes exactly one operator")
     if output_type is None:
         output_type = StructureFunction2DSumsAndCounts if joint else StructureFunction
-    validate_array_shape(x, u, distance_metric)
+    shape = validate_array_shape(x, u, distance_metric)
     assert_counts_representable(ct, _shape_of(x)[1])
+    if shape.aux:
+        return _aux_result(backend, ops, multi, shape, x, u, distance_bins, value_bins, distance_metric, ct,
+                           output_type)
     sums, counts, plan, xcode, ucode = _run(backend, ops, x, u, distance_bins, value_bins, distance_metric)
     ot = _output_float_type(xcode, ucode)
     ct = np.dtype(ct)
@@ -343,6 +476,32 @@ def calculate_structure_function(structure_function_type, x, u, distance_bins, *
     for k, o in enumerate(ops):
         raw = StructureFunctionSumsAndCounts(o, distance_bins, sums[k * nb:(k + 1) * nb].astype(ot), c1.copy())
         results.append(_finalize(raw, output_type))
+    return tuple(results) if multi else results[0]
+
+
+def _aux_result(backend, ops, multi, shape, x, u, distance_bins, value_bins, distance_metric, ct, output_type):
+    """Auxiliary-axis results: sums and counts of shape (n_bins, aux...) for 1D histograms
+    (src/Calculations/batch.jl:209-217) and (n_dist, n_val, aux...) for joint ones."""
+    parts, xcode, ucode = _run_aux(backend, ops, shape, x, u, distance_bins, value_bins, distance_metric)
+    ot = _output_float_type(xcode, ucode)
+    ct = np.dtype(ct)
+    aux = shape.aux
+    if value_bins is not None:
+        nd, nv = len(distance_bins) - 1, len(value_bins) - 1
+        s = np.stack([p[0].reshape((nd, nv), order="F") for p in parts], axis=-1)
+        c = np.stack([p[1].reshape((nd, nv), order="F") for p in parts], axis=-1)
+        s = s.reshape((nd, nv) + aux, order="F").astype(ot)
+        c = c.reshape((nd, nv) + aux, order="F").astype(ct)
+        if output_type is not StructureFunction2DSumsAndCounts:
+            raise ArgumentError(f"Cannot produce a {getattr(output_type, '__name__', output_type)} from this "
+                                f"calculation (got a StructureFunction2DSumsAndCounts). Check the `output_type` keyword.")
+        return StructureFunction2DSumsAndCounts(ops[0], distance_bins, value_bins, s, c)
+    nb = len(distance_bins) - 1
+    c = np.stack([p[1] for p in parts], axis=-1).reshape((nb,) + aux, order="F").astype(ct)
+    results = []
+    for k, o in enumerate(ops):
+        s = np.stack([p[0][k * nb:(k + 1) * nb] for p in parts], axis=-1).reshape((nb,) + aux, order="F")
+        results.append(_finalize(StructureFunctionSumsAndCounts(o, distance_bins, s.astype(ot), c.copy()), output_type))
     return tuple(results) if multi else results[0]
 
 
@@ -369,9 +528,21 @@ def calculate_structure_function_inplace(sums, counts, structure_function_type, 
         raise ArgumentError("the mutating entry takes one operator")
     distance_metric = Euclidean() if distance_metric is None else distance_metric
     backend = default_backend() if backend is None else backend
-    validate_array_shape(x, u, distance_metric)
+    shape = validate_array_shape(x, u, distance_metric)
     counts_arr = np.asarray(counts)
     assert_counts_representable(counts_arr.dtype, _shape_of(x)[1])
+    if shape.aux:
+        # auxiliary axes (the reference's auxiliary_structure_function! / auxiliary_joint2d!,
+        # src/Calculations/dispatch.jl:380-386, 455-461): per-slice histograms added in place
+        raw = _aux_result(backend, ops, False, shape, x, u, distance_bins, value_bins, distance_metric,
+                          np.uint64, StructureFunction2DSumsAndCounts if value_bins is not None
+                          else StructureFunctionSumsAndCounts)
+        if sums.shape != raw.sums.shape or counts_arr.shape != raw.counts.shape:
+            raise DimensionMismatch(f"sums/counts must have shape {raw.sums.shape}; got {sums.shape} and "
+                                    f"{counts_arr.shape}")
+        sums += raw.sums.astype(sums.dtype)
+        counts += raw.counts.astype(counts_arr.dtype)
+        return None
     s, c, plan, _, _ = _run(backend, ops, x, u, distance_bins, value_bins, distance_metric)
     if value_bins is not None:
         nd, nv = len(distance_bins) - 1, len(value_bins) - 1

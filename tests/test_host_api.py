@@ -28,9 +28,15 @@ def test_dimension_mismatch_like_reference():
         SF.validate_array_shape(np.zeros((2, 8, 3)), np.zeros((2, 8, 4)), SF.Euclidean())
 
 
-def test_auxiliary_axes_and_unknown_metrics_raise_argument_error():
-    with pytest.raises(SF.ArgumentError):
-        SF.validate_array_shape(np.zeros((2, 8)), np.zeros((2, 8, 3)), SF.Euclidean())
+def test_auxiliary_axes_shapes_and_unknown_metrics():
+    # src/Calculations/shapes.jl:17-20, 67-105: shared positions (x (W,N), u (D,N,aux...)) and varying
+    # positions (matching auxiliary axes)
+    sh = SF.validate_array_shape(np.zeros((2, 8)), np.zeros((2, 8, 3, 2)), SF.Euclidean())
+    assert isinstance(sh, SF.api.SharedPositionField) and sh.aux == (3, 2) and sh.D == 2
+    vh = SF.validate_array_shape(np.zeros((3, 8, 4)), np.zeros((3, 8, 4)), SF.Euclidean())
+    assert isinstance(vh, SF.api.VaryingPositionField) and vh.aux == (4,)
+    with pytest.raises(SF.DimensionMismatch):
+        SF.validate_array_shape(np.zeros((2, 8, 4)), np.zeros((2, 8, 4, 1)), SF.Euclidean())
     with pytest.raises(SF.ArgumentError):
         SF.pair_geometry_for(SF.PreMetric(), 2)
 
