@@ -230,7 +230,15 @@ typedef enum {
      * (sorted), 0 storage order, 1 each off-diagonal J tile staged in the order of its distance from
      * the I tile, so that each lane's run of equal bins is long. Counts are identical either way;
      * only the summation order of the sums changes. */
-    SFB200_OPT_TILE_SORT = 4
+    SFB200_OPT_TILE_SORT = 4,
+    /* Formulation of the FP64 spherical 1D kernel (other plans ignore it): -1 automatic (chord), 1 the
+     * reference's own: the
+     * pair frame (geodesic frame, parallel transport, atan2) for every pair
+     * (src/HelperFunctions.jl:186-200, 265-276, 324-348), 2 the chord formulation of the mixed kernel
+     * in FP64 (bin on the squared chord against the chord images of the edges, the reference frame only
+     * for the pairs within 2^-40 of an edge image, coincident or antipodal; increments from the chord
+     * and the tangent velocities). Counts are identical; sums agree to FP64 rounding. */
+    SFB200_OPT_FORMULATION = 5
 } sfb200_option;
 
 /* Set a plan option (autotuning; no counterpart in the reference). */

@@ -127,6 +127,15 @@ struct sfb200_plan {
     int cols_ovr = 0;     // run-length histogram columns (0 auto)
     int sort_ovr = -1;    // J-tile order of the flat 1D kernels: -1 auto (sorted), 0 storage order, 1 sorted
     unsigned long long* d_range = nullptr;  // sfb200_distance_range: min / max key bits
+    // FP64 sphere (1D): the chord formulation (default) or the reference formulation (the pair frame
+    // for every pair); -1 automatic, 1 reference, 2 chord
+    int form_ovr = -1;
+    LutGeom lgc{};                    // chord-key table of the FP64 chord kernel
+    LutEntry64* d_lutc = nullptr;
+    int lutc_bytes = 0;
+    bool fp64_sphere_1d() const { return sphere && !joint && !fp32 && !mixed; }
+    bool chord64() const { return fp64_sphere_1d() && form_ovr != 1; }
+
 };
 
 // ------------------------------------------------------------------------------- errors
@@ -570,6 +579,7 @@ static void free_plan_device(sfb200_plan* p)
     free_workspace(p->ws, true);
     cudaFree(p->d_exact); cudaFree(p->d_vedges); cudaFree(p->d_lut64); cudaFree(p->d_ck);
     cudaFree(p->d_lut32); cudaFree(p->d_rowlo); cudaFree(p->d_vwin); cudaFree(p->d_lut8); cudaFree(p->d_range);
+    cudaFree(p->d_lutc);
 }
 
 extern "C" int sfb200_plan_destroy(sfb200_plan* p)
@@ -679,8 +689,8 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
                 return set_err(ctx, SFB200_ERR_INVALID_ARG,
                                "distance_bins: Euclidean edges must be non-negative (their squares must stay sorted)");
     }
-    // edge keys of the FP32 path (and the chord keys of the mixed sphere path)
-    if (p->fp32 || (p->mixed && p->sphere)) {
+    // edge keys of the FP32 path (and the chord keys of the mixed and FP64 chord sphere paths)
+    if (p->fp32 || (p->mixed && p->sphere) || p->fp64_sphere_1d()) {
         p->ck.resize(db.n_edges);
         for (int k = 0; k < db.n_edges; ++k) {
             double r = dlinear ? std::fma((double)k, db.step, db.first) : db.edges[k];
@@ -785,6 +795,12 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         if (build_byte_table(p->exact_tab, bt) && (e = upload(&p->d_lut8, bt.data(), bt.size())) != cudaSuccess)
             return cuda_fail(ctx, e, "upload byte table");
     }
+    if (p->fp64_sphere_1d()) {  // the chord kernel's table (the r-edge table above stays for the other)
+        std::vector<LutEntry64> lut;
+        build_lut64(p->ck, p->lgc, lut, kChordWrel);
+        p->lutc_bytes = (int)(lut.size() * sizeof(LutEntry64));
+        if ((e = upload(&p->d_lutc, lut.data(), lut.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload table");
+    }
     if (p->fp32) {
         if ((e = upload(&p->d_ck, p->ck.data(), p->ck.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload keys");
         if ((e = cudaMalloc(&p->d_lut32, sizeof(LutEntry32) * p->lg32.ncell)) != cudaSuccess)
@@ -882,6 +898,11 @@ extern "C" int sfb200_plan_set_option(sfb200_plan* p, int option, int64_t value)
         p->shard_index = (int)(value & 0xffffffffll);
         p->shard_count = (int)(value >> 32);
         return SFB200_OK;
+    case SFB200_OPT_FORMULATION:
+        if (value != -1 && value != 1 && value != 2)
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "formulation must be -1 (auto), 1 (reference) or 2 (chord)");
+        p->form_ovr = (int)value;
+        return SFB200_OK;
     case SFB200_OPT_TILE_SORT:
         if (value < -1 || value > 1) return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile sort must be -1, 0 or 1");
         p->sort_ovr = (int)value;
@@ -915,7 +936,7 @@ static int workspace_layout(sfb200_plan* p, Workspace& w, long long cap, bool ou
         CK(alloc((void**)&w.d_XF, sizeof(float) * nxf * cap));
         if (!p->sphere) CK(alloc((void**)&w.d_UF, sizeof(float) * (p->df ? 2 : 1) * p->D * cap));
     }
-    if (p->mixed && p->sphere) CK(alloc((void**)&w.d_XM, sizeof(double) * 10 * cap));
+    if ((p->mixed && p->sphere) || p->fp64_sphere_1d()) CK(alloc((void**)&w.d_XM, sizeof(double) * 10 * cap));
     CK(alloc((void**)&w.d_keys, sizeof(unsigned) * 2 * cap));
     CK(alloc((void**)&w.d_perm, sizeof(int) * 2 * cap));
     CK(alloc((void**)&w.d_box, sizeof(unsigned) * 6));
@@ -996,7 +1017,7 @@ static void launch_pack(sfb200_plan* p, Workspace& w, const void* x, const void*
     if (p->sphere)
         k_pack_sphere<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->desc.angle_unit, perm,
                                                   w.d_X64, w.d_U64, p->fp32 ? w.d_XF : nullptr,
-                                                  p->mixed ? w.d_XM : nullptr, w.d_aux + 1);
+                                                  w.d_XM, w.d_aux + 1);
     else
         k_pack_flat<TX, TU><<<nblk, tb, 0, s>>>((const TX*)x, (const TU*)u, n, p->D, p->df, perm, w.d_X64,
                                                 w.d_U64, p->fp32 ? w.d_XF : nullptr,
@@ -1099,6 +1120,8 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
         const int nx = p->sphere ? (p->D == 3 ? 20 : 18) : (p->df ? 4 : 2) * p->D;
         return (size_t)lut_bytes + (size_t)nx * T * 4 + (size_t)ncell * 12 + (size_t)(p->nb + 2) * 4;
     }
+    if (p->chord64())  // FP64 chord records p(3), U(3), W(3), up/pad
+        return (size_t)lut_bytes + (size_t)10 * T * 8 + hist_bytes(false, NV, priv, NW, NBP, lc);
     if (!p->fp32) {
         const int nx = p->sphere ? 8 : p->D;
         return (size_t)lut_bytes + (size_t)(nx + p->D) * T * 8 + hist_bytes(false, NV, priv, NW, NBP, lc);
@@ -1216,6 +1239,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     if (byte_lut) lut_bytes = kByteCells + (int)sizeof(double) * kByteEdges;
     else if (p->fp32) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
     else if (p->mixed) lut_bytes = p->lut64_bytes;  // exact table (flat) or chord table (sphere); 0 if linear
+    else if (p->chord64()) lut_bytes = p->lutc_bytes;
     else if (!dlinear && !p->joint) lut_bytes = p->lut64_bytes;
     int T;
     bool smem_hist = true;
@@ -1252,6 +1276,8 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
             kc = p->sphere ? pick_sphere1d_mx_batch(p->D, p->opl) : pick_flat1d_mx_batch(p->D, p->opl);
         else if (p->mixed)
             kc = p->sphere ? pick_sphere1d_mx(p->D, p->opl, want) : pick_flat1d_mx(p->D, p->opl, want);
+        else if (p->chord64())
+            kc = pick_sphere1d_chord64(p->D, p->opl, want);
         else
             kc = p->sphere ? pick_sphere1d(p->D, p->fp32, p->opl, want)
                            : pick_flat1d(p->D, p->fp32, p->df, p->opl, want);
@@ -1322,8 +1348,8 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     a.XF = w.d_XF;
     a.UF = w.d_UF;
     a.XM = w.d_XM;
-    a.lut = p->fp32 ? (const void*)p->d_lut32 : (const void*)p->d_lut64;
-    a.lg = p->fp32 ? p->lg32 : p->lg64;
+    a.lut = p->fp32 ? (const void*)p->d_lut32 : (p->chord64() ? (const void*)p->d_lutc : (const void*)p->d_lut64);
+    a.lg = p->fp32 ? p->lg32 : (p->chord64() ? p->lgc : p->lg64);
     a.chord_wrel = kChordWrel;
     a.chord_short = 0x1p-40;         // (near-)coincident: the reference frame is degenerate
     a.chord_anti = 4.0 - 0x1p-40;    // (near-)antipodal: likewise

@@ -332,19 +332,19 @@ __device__ __forceinline__ int sphere_chord_bin(const LutEntry64* lut, const Pai
 }
 
 // FP64 reference recomputation of a sphere pair: bin (nb + 1 when the frame is degenerate) and the
-// values scaled by us^order in FP32. Kept out of line (it is rare and large); inputs and the result
-// travel by value so that the caller's arrays stay in registers.
-template <int NV>
+// values scaled by us^order, in the kernel's value type R. Kept out of line (it is rare and large);
+// inputs and the result travel by value so that the caller's arrays stay in registers.
+template <int NV, typename R = float>
 struct ExactPair {
-    float v[NV];
+    R v[NV];
     int bin;
 };
 
-template <int D, class OPS>
-__device__ __forceinline__ ExactPair<OPS::n> sphere_pair_exact(const PairArgs& a, int i, int j, int ku)
+template <int D, class OPS, typename R = float>
+__device__ __forceinline__ ExactPair<OPS::n, R> sphere_pair_exact(const PairArgs& a, int i, int j, int ku)
 {
     constexpr int NV = OPS::n;
-    ExactPair<NV> res;
+    ExactPair<NV, R> res;
     double unscale[NV];
     op_unscale(OPS{}, a.gen, ku, unscale);
     SphPoint A, B;
@@ -364,12 +364,53 @@ __device__ __forceinline__ ExactPair<OPS::n> sphere_pair_exact(const PairArgs& a
     double v64[NV];
     eval_ops(OPS{}, du[0], du[1], Q64 - du[0] * du[0], Q64, D, a.gen, v64);
 #pragma unroll
-    for (int o = 0; o < NV; ++o) res.v[o] = f32(v64[o] / unscale[o]);
+    for (int o = 0; o < NV; ++o) res.v[o] = R(v64[o] / unscale[o]);
     return res;
 }
 
-// Per-pair FP32 primitives of a sphere pair from the FP64 records (fields: p 0-2, U 3-5, W 6-8,
-// up 9; velocities already scaled by us). Returns the chord^2.
+// Per-pair primitives of a sphere pair from the FP64 records (fields: p 0-2, U 3-5, W 6-8, up 9;
+// velocities already scaled by us), in FP32 (the mixed kernel) or FP64 (the FP64 chord kernel, R =
+// double: the same formulas with the normalisation and powers kept in FP64). Returns the chord^2.
+template <int D, class OPS>
+__device__ __forceinline__ double sphere_primitives_mx(const double* ra, const double* rb, double& L, double& Tt,
+                                                       double& T2, double& Q)
+{
+    using N = ListNeeds2<OPS>;
+    double d[3], sv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        d[c] = rb[c] - ra[c];
+        sv[c] = rb[c] + ra[c];
+    }
+    const double ch2 = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
+    const double ss = fma(sv[2], sv[2], fma(sv[1], sv[1], sv[0] * sv[0]));
+    // sin(sigma) = |d| |s| / 2; degenerate (coincident / antipodal) pairs are recomputed anyway
+    const double inv_s = rsqrt(0.25 * ch2 * ss);
+    L = 0.0;
+    Tt = 0.0;
+    T2 = 0.0;
+    Q = 0.0;
+    if constexpr (N::L || N::Q) {
+        double pl = d[0] * (rb[3] - ra[3]);
+        pl = fma(d[1], rb[4] - ra[4], pl);
+        pl = fma(d[2], rb[5] - ra[5], pl);
+        L = pl * inv_s;
+    }
+    if constexpr (N::T || N::T2 || N::Q) {
+        double pt = d[0] * (rb[6] - ra[6]);
+        pt = fma(d[1], rb[7] - ra[7], pt);
+        pt = fma(d[2], rb[8] - ra[8], pt);
+        Tt = pt * inv_s;
+        T2 = Tt * Tt;
+        if constexpr (D == 3) {
+            const double dw = rb[9] - ra[9];
+            T2 = fma(dw, dw, T2);
+        }
+    }
+    if constexpr (N::Q) Q = fma(L, L, T2);
+    return ch2;
+}
+
 template <int D, class OPS>
 __device__ __forceinline__ double sphere_primitives_mx(const double* ra, const double* rb, float& L, float& Tt,
                                                        float& T2, float& Q)
@@ -411,12 +452,12 @@ __device__ __forceinline__ double sphere_primitives_mx(const double* ra, const d
     return ch2;
 }
 
-template <int D, class OPS, int PRIV>
+template <int D, class OPS, int PRIV, typename R = float>
 __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0, long long p1, long long ps)
 {
     constexpr int NV = OPS::n;
     constexpr int NP = 5;  // double2 per record: p(3) U(3) W(3) up/pad(1)
-    using Hist = BlockHist<float, NV, PRIV>;
+    using Hist = BlockHist<R, NV, PRIV>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -430,7 +471,8 @@ __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0,
         lut[k] = static_cast<const LutEntry64*>(a.lut)[k];
     if (threadIdx.x == 0) s_recheck = 0ull;
     unsigned my_recheck = 0;
-    const int ku = pow2_exponent_above(a.g_stats[2]);
+    // FP32 values carry velocities scaled into FP32 range; the FP64 chord kernel needs no scaling
+    const int ku = sizeof(R) == 4 ? pow2_exponent_above(a.g_stats[2]) : 0;
     const double us = ldexp(1.0, -ku);
     double unscale[NV];
     op_unscale(OPS{}, a.gen, ku, unscale);
@@ -459,16 +501,16 @@ __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0,
         }
         __syncthreads();
         const bool diag = ti == tj;
-        auto pair = [&](int jj, int& key, float (&v)[NV]) {
+        auto pair = [&](int jj, int& key, R (&v)[NV]) {
             double rb[2 * NP];
             load_rec2<NP>(srec + jj * 2 * NP, rb);
-            float L, Tt, T2, Q;
+            R L, Tt, T2, Q;
             const double ch2 = sphere_primitives_mx<D, OPS>(ra, rb, L, Tt, T2, Q);
             bool slow;
             key = sphere_chord_bin(lut, a, ch2, slow);
             eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
             if (slow) {
-                const ExactPair<NV> ex = sphere_pair_exact<D, OPS>(a, i, j0 + jj, ku);
+                const ExactPair<NV, R> ex = sphere_pair_exact<D, OPS, R>(a, i, j0 + jj, ku);
                 key = ex.bin;
 #pragma unroll
                 for (int o = 0; o < NV; ++o) v[o] = ex.v[o];
@@ -480,7 +522,7 @@ __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0,
 #pragma unroll 2
                 for (int jj = diag ? (int)threadIdx.x + 1 : 0; jj < jn; ++jj) {
                     int key;
-                    float v[NV];
+                    R v[NV];
                     pair(jj, key, v);
                     hist.add(key, v, lane, warp);
                 }
@@ -489,12 +531,12 @@ __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0,
             for (int jj = 0; jj < jn; ++jj) {
                 const bool valid = iv && (!diag || jj > (int)threadIdx.x);
                 int key;
-                float v[NV];
+                R v[NV];
                 if (valid) pair(jj, key, v);
                 else {
                     key = a.nb + 1;
 #pragma unroll
-                    for (int o = 0; o < NV; ++o) v[o] = 0.f;
+                    for (int o = 0; o < NV; ++o) v[o] = R(0);
                 }
                 hist.add(key, v, lane, warp);
             }
@@ -509,6 +551,17 @@ template <int D, class OPS, int PRIV>
 __global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
 {
     sphere1d_mx_run<D, OPS, PRIV>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
+}
+
+// The plain FP64 form of the same chord formulation (precision FP64, the default formulation on the
+// sphere): FP64 chord bin with the same ambiguity band, FP64 normalisation, powers and accumulation.
+// It differs from the mixed kernel only in precision, so the two time the same algorithm; the
+// reference-formulation FP64 kernel (k_sphere1d_fp64: the reference's frame for every pair)
+// remains selectable with SFB200_OPT_FORMULATION.
+template <int D, class OPS, int PRIV>
+__global__ void __launch_bounds__(256, 2) k_sphere1d_chord64(const PairArgs a)
+{
+    sphere1d_mx_run<D, OPS, PRIV, double>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.

@@ -135,3 +135,4 @@ OPT_POINT_ORDER = 1
 OPT_HIST_COLUMNS = 2
 OPT_SHARD = 3
 OPT_TILE_SORT = 4
+OPT_FORMULATION = 5

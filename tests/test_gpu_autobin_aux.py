@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 import oracle_py
-from helpers import TOL_FP64, TOL_MIXED, compare
+from helpers import TOL_FP64, TOL_MIXED, compare, sphere_tol
 import sfb200 as SF
 from sfb200 import synthetic
 from sfb200.api import plan_description
@@ -129,7 +129,7 @@ def test_varying_positions_joint_and_sphere(precision, tol):
                                         output_type=SF.StructureFunctionSumsAndCounts, count_eltype=np.uint64)
     for b in range(2):
         rs, rc, ra = _slice_oracle((SF.L2SF,), xs[:, :, b], us[:, :, b], w.distance_bins.edges, metric=w.metric)
-        compare(r.sums[:, b], r.counts[:, b], rs, rc, ra, tol)
+        compare(r.sums[:, b], r.counts[:, b], rs, rc, ra, sphere_tol(precision, tol))
 
 
 def test_inplace_auxiliary_axes_accumulate():

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle_py
-from helpers import TOL_FP32, TOL_FP64, TOL_MIXED, compare
+from helpers import TOL_FP32, TOL_FP64, TOL_FP64_SPHERE, TOL_MIXED, compare, sphere_tol
 import sfb200 as SF
 from sfb200 import _abi, _lib, synthetic
 from sfb200.api import plan_description
@@ -118,7 +118,7 @@ def test_sphere_l2(precision, tol, D):
     if D == 3:
         u = np.vstack([w.u, np.random.default_rng(5).standard_normal((1, w.n)).astype(np.float32)])
     check((SF.L2SF, SF.T2SF, SF.S2SF) if D == 3 else w.ops, w.x, u, w.distance_bins.edges, metric=w.metric,
-          precision=precision, tol=tol)
+          precision=precision, tol=sphere_tol(precision, tol))
 
 
 @pytest.mark.parametrize("precision,tol", PRECISIONS)
@@ -129,7 +129,8 @@ def test_sphere_radians_and_odd_ops(precision, tol):
     x = np.stack([lon, lat])
     u = rng.standard_normal((2, 900))
     bins = np.linspace(0.0, math.pi, 13)
-    check((SF.L3SF, SF.T3SF, SF.L2T1SF), x, u, bins, metric=SF.SphericalAngle(), precision=precision, tol=tol)
+    check((SF.L3SF, SF.T3SF, SF.L2T1SF), x, u, bins, metric=SF.SphericalAngle(), precision=precision,
+          tol=sphere_tol(precision, tol))
 
 
 @pytest.mark.parametrize("precision,tol", PRECISIONS)
@@ -170,7 +171,7 @@ def test_privatization_modes(precision, tol, priv, tile):
     gs, gc, st = run_gpu(ws.ops, ws.x, ws.u, ws.distance_bins.edges, metric=ws.metric, precision=precision,
                          tile=tile, priv=priv)
     rs, rc, ra = run_oracle(ws.ops, ws.x, ws.u, ws.distance_bins.edges, metric=ws.metric)
-    compare(gs, gc, rs, rc, ra, tol)
+    compare(gs, gc, rs, rc, ra, sphere_tol(precision, tol))
 
 
 @pytest.mark.parametrize("precision,tol", PRECISIONS)
@@ -190,7 +191,7 @@ def test_point_order_and_table_columns(precision, tol, order, cols):
         gs, gc, st = run_gpu(w.ops, w.x, w.u, w.distance_bins.edges, metric=w.metric, precision=precision,
                              priv=3, options=opts)
         rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges, metric=w.metric)
-        compare(gs, gc, rs, rc, ra, tol)
+        compare(gs, gc, rs, rc, ra, sphere_tol(precision, tol) if name == "c2" else tol)
 
 
 @pytest.mark.parametrize("precision,tol", PRECISIONS)
@@ -218,7 +219,7 @@ def test_tile_pair_shards_add_up(precision, tol, count):
             tot_s = gs if tot_s is None else tot_s + gs
             tot_c = gc if tot_c is None else tot_c + gc
         rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges, metric=w.metric, value_bins=w.value_bins)
-        compare(tot_s, tot_c, rs, rc, ra, tol)
+        compare(tot_s, tot_c, rs, rc, ra, sphere_tol(precision, tol) if name == "c2" else tol)
 
 
 def test_autotuned_backend_gives_the_oracle_histogram():
@@ -295,3 +296,38 @@ def test_joint_values_near_zero(value_bins):
     u = 1e-3 * rng.standard_normal((2, n))
     edges = synthetic.log_edges(1e-3, math.sqrt(2.0), 12)
     check((SF.ProjectedStructureFunctionType(1, 0),), x, u, edges, value_bins=value_bins)
+
+
+@pytest.mark.parametrize("form", [1, 2])
+def test_fp64_sphere_formulations(form):
+    """Precision FP64 on the sphere in both formulations (SFB200_OPT_FORMULATION): 1 the reference's own
+    (the pair frame for every pair), 2 the mixed kernel's chord algorithm in FP64 (the chord bin with
+    its ambiguity band, increments from the chord and the tangent velocities). Both give the oracle's
+    histogram to FP64 rounding."""
+    opts = {_abi.OPT_FORMULATION: form}
+    TOL = TOL_FP64 if form == 1 else TOL_FP64_SPHERE
+    w = synthetic.config("c2", n=1500)
+    gs, gc, st = run_gpu(w.ops, w.x, w.u, w.distance_bins.edges, metric=w.metric, precision="fp64", options=opts)
+    rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges, metric=w.metric)
+    compare(gs, gc, rs, rc, ra, TOL)
+    rng = np.random.default_rng(31)
+    u = rng.standard_normal((3, 1200))
+    lon = rng.uniform(-180, 180, 1200)
+    xs = np.stack([lon, np.degrees(np.arcsin(rng.uniform(-1, 1, 1200)))])
+    ops = (SF.L2SF, SF.T2SF, SF.L3SF, SF.T3SF)
+    bins = np.linspace(0.0, 20000.0, 17)
+    gs, gc, st = run_gpu(ops, xs, u, bins, metric=SF.Haversine(6371.0), precision="fp64", options=opts)
+    rs, rc, ra = run_oracle(ops, xs, u, bins, metric=SF.Haversine(6371.0))
+    nb = len(bins) - 1
+    for k in range(len(ops)):
+        compare(gs[k * nb:(k + 1) * nb], gc, rs[k * nb:(k + 1) * nb], rc, ra[k * nb:(k + 1) * nb], TOL)
+    # radians, odd operators and the single-pass list
+    x = np.stack([rng.uniform(-math.pi, math.pi, 900), np.arcsin(rng.uniform(-1, 1, 900))])
+    for ops in ((SF.L3SF, SF.T3SF, SF.L2T1SF), (SF.S2SF, SF.L2SF, SF.S3SF, SF.L3SF)):
+        uu = rng.standard_normal((2, 900))
+        b = np.linspace(0.0, math.pi, 13)
+        gs, gc, st = run_gpu(ops, x, uu, b, metric=SF.SphericalAngle(), precision="fp64", options=opts)
+        rs, rc, ra = run_oracle(ops, x, uu, b, metric=SF.SphericalAngle())
+        nb = len(b) - 1
+        for k in range(len(ops)):
+            compare(gs[k * nb:(k + 1) * nb], gc, rs[k * nb:(k + 1) * nb], rc, ra[k * nb:(k + 1) * nb], TOL)

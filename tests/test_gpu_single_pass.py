@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import oracle_py
-from helpers import TOL_FP32, TOL_FP64, TOL_MIXED
+from helpers import TOL_FP32, TOL_FP64, TOL_MIXED, sphere_tol
 import sfb200 as SF
 from sfb200 import synthetic
 from sfb200.api import plan_description
@@ -65,7 +65,7 @@ def test_single_pass_sphere(precision, tol):
     # Float64 copies of the Float32 inputs (exact): the results then come back as Float64, so the
     # FP64 tolerance is not hidden by a Float32 output type
     check(w.x.astype(np.float64), w.u.astype(np.float64), w.distance_bins.edges, metric=w.metric,
-          precision=precision, tol=tol)
+          precision=precision, tol=sphere_tol(precision, tol))
 
 
 def test_reference_three_point_case():

@@ -135,3 +135,58 @@ def test_queued_rounds_on_one_slice_complete_in_order():
         assert ex.free_bytes() >= free_before + h.device_bytes - (2 << 20)
     finally:
         ex.close()
+
+
+def test_arrivals_during_rounds_same_alone_and_in_the_mix():
+    """Continuous batching proper: a large request is submitted first and, while its rounds are on the
+    device (small rounds, two in flight), a feeder thread submits the others one by one; they are
+    admitted and join rounds that still hold the first. Each result equals the request run alone
+    (counts identical, sums within the mixed tolerance)."""
+    import threading
+    import time
+
+    rng = np.random.default_rng(34)
+    big_x = rng.random((2, 40000))
+    big = Request((SF.L2SF,), big_x, synthetic.planar_field(big_x, 32, 64.0, rng, 0.01),
+                  synthetic.log_edges(1e-3, math.sqrt(2.0), 32), tag="big")
+    reqs = [big] + make_requests(seed=33, count=20)
+    ex = GpuExecutor(0)
+    try:
+        srv = Server(ex, max_slots=32, round_pairs=3e6, depth=2).start()
+        tickets = [srv.submit(big)]
+
+        def feeder():
+            for r in reqs[1:]:
+                tickets.append(srv.submit(r))
+                time.sleep(0.0005)
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        th.join()
+        srv.stop()
+        # the first request (8e8 pairs in rounds of 3e6) was still running when later ones were admitted,
+        # and rounds held several slices at once
+        first = tickets[0]
+        assert first.rounds > 20
+        assert sum(t.t_admit < first.t_done for t in tickets[1:]) >= 1
+        assert max(n for n, _ in srv.round_log) > 1
+        for r, t in zip(reqs, tickets):
+            mix_s, mix_c = t.wait(120)
+            desc, keep = plan_description(r.ops, r.u.shape[0], r.distance_bins, r.value_bins, r.metric, "mixed",
+                                          r.x.dtype, r.u.dtype)
+            plan = _lib.Plan(ex.ctx, desc, keep)
+            s = np.zeros(plan.n_sums)
+            c = np.zeros(plan.n_counts, dtype=np.uint64)
+            xa, ua = np.asfortranarray(r.x), np.asfortranarray(r.u)
+            plan.run(xa.ctypes.data, ua.ctypes.data, r.n, 0, s.ctypes.data, c.ctypes.data)
+            plan.close()
+            assert np.array_equal(mix_c, c), f"request {r.tag}: counts differ between the mix and alone"
+            if r.tag != "big":  # the oracle of the small ones (the big one: alone = mix suffices)
+                rs, rc, ra = oracle_of(r)
+                compare(mix_s, mix_c, rs, rc, ra, TOL_MIXED)
+                scale = np.maximum(ra, 1e-300)
+            else:
+                scale = np.maximum(np.abs(s), 1e-300)
+            assert float(np.max(np.abs(mix_s - s) / scale)) <= 2 * TOL_MIXED
+    finally:
+        ex.close()
