@@ -35,6 +35,11 @@ for _p in (os.path.join(ROOT, "structurefunctions.jl_b200"), os.path.join(ROOT, 
 import numpy as np  # noqa: E402
 
 METRIC = "pair-evals/s mixed-precision vs FP64 kernel on B200; p50/p99 slice latency"
+
+# DRAM bytes per point of one launch of the mixed pair kernel, from ncu captures of the same kernel
+# (dram__bytes_read.sum + dram__bytes_write.sum): c1 k_flat1d_mx at N = 16384, 851,200 bytes; c3
+# k_joint_mx at N = 32768, 1,255,424 bytes. The read is the packed points once (L2-resident after).
+DRAM_BYTES_PER_POINT = {"c1": 851200 / 16384, "c3": 1255424 / 32768}
 UNIT = "pair-evals/s"
 
 
@@ -226,16 +231,27 @@ def run_ours(args):
     mixed, msums, mcounts = make("mixed")
     fp64, fsums, fcounts = make("fp64")
     fp32, hsums, hcounts = make("fp32")
+    # the sphere's FP64 kernel in the reference's own formulation (the pair frame for every pair); the
+    # default FP64 kernel runs the mixed kernel's chord algorithm in FP64 (the like-for-like comparison)
+    fp64r = None
+    if w.metric.__class__.__name__ != "Euclidean" and w.value_bins is None:
+        fp64r, rsums, rcounts = make("fp64")
+        fp64r.set_option(_abi.OPT_FORMULATION, 1)
 
     clocks.start()
     t_mixed, kms_mixed, launches_mixed, st_mixed = device_steps(mixed, msums, mcounts, args.steps, args.warmup)
     t_fp64, kms_fp64, launches_fp64, st_fp64 = device_steps(fp64, fsums, fcounts, args.steps, args.warmup)
     t_fp32, kms_fp32, launches_fp32, st_fp32 = device_steps(fp32, hsums, hcounts, args.steps, args.warmup)
+    t_fp64r = kms_fp64r = None
+    if fp64r is not None:
+        t_fp64r, kms_fp64r, _, _ = device_steps(fp64r, rsums, rcounts, args.steps, args.warmup)
     clk = clocks.stop()
 
     # counts of the kernels must agree (bit-exact binning in all); sums: per-bin deviation of the
     # mixed and FP32-bulk kernels from the FP64 kernel at the full size (relative to |FP64 sum|)
     same_counts = bool(torch.equal(mcounts, fcounts)) and bool(torch.equal(hcounts, fcounts))
+    if fp64r is not None:
+        same_counts = same_counts and bool(torch.equal(rcounts, fcounts))
 
     def max_rel_dev(a, b):
         # per operator: max over bins of |a - b| / |b| (sign-definite operators: the tolerance figure;
@@ -299,6 +315,8 @@ def run_ours(args):
     e2e_total = max_over_ranks(e2e_total * 1e3)
 
     t_fp32 = max_over_ranks(t_fp32)
+    if fp64r is not None:
+        t_fp64r = max_over_ranks(t_fp64r)
     ms_mixed = t_mixed / args.steps
     ms_fp64 = t_fp64 / args.steps
     ms_fp32 = t_fp32 / args.steps
@@ -317,13 +335,10 @@ def run_ours(args):
     # per launch: this rank's share of the pairs
     achieved = flops * (pairs / world) / (kmed_mixed * 1e-3) / 1e12
     achieved64 = flops * (pairs / world) / (kmed_fp64 * 1e-3) / 1e12
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", f"{args.config}_mixed_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get("bytes_per_launch")
-        except Exception:
-            traffic = None
+    # DRAM bytes of one launch of the mixed kernel: measured with ncu (dram__bytes_read.sum +
+    # dram__bytes_write.sum) on a smaller case of the same kernel and scaled by N (the traffic is the
+    # compulsory read of the packed points, linear in N, not in pairs)
+    traffic = DRAM_BYTES_PER_POINT[args.config] * n if args.config in DRAM_BYTES_PER_POINT else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -357,12 +372,20 @@ def run_ours(args):
                 "blocks": st_mixed["blocks"],
             },
             "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms_fp64, "kernel_ms": kmed_fp64,
-                     "roofline_frac_fp64": (achieved64 / peak64) if peak64 else None},
+                     "roofline_frac_fp64": (achieved64 / peak64) if peak64 else None,
+                     "formulation": "the mixed kernel's algorithm with every step in FP64"},
             "fp32": {"value": fp32_value, "unit": UNIT, "ms_per_step": ms_fp32, "kernel_ms": kmed_fp32,
                      "rechecked_pairs_per_step": st_fp32["rechecked"],
                      "max_rel_dev_vs_fp64_per_operator": dev_fp32,
                      "note": "FP32-bulk kernel: FP32 differences, FP64 recheck of bin membership only"},
             "mixed_over_fp64": value / fp64_value,
+            **({"fp64_reference_formulation": {
+                "value": pairs / (t_fp64r / args.steps * 1e-3), "unit": UNIT, "ms_per_step": t_fp64r / args.steps,
+                "kernel_ms": sorted(kms_fp64r)[len(kms_fp64r) // 2],
+                "note": "FP64 kernel in the reference's formulation: the pair frame (geodesic frame, parallel "
+                        "transport, atan2) for every pair"},
+                "mixed_over_fp64_reference_formulation": value / (pairs / (t_fp64r / args.steps * 1e-3))}
+               if fp64r is not None else {}),
             "counts_equal_all_precisions": same_counts,
             "mixed_max_rel_dev_vs_fp64_per_operator": dev_mixed,
             "rechecked_pairs_per_step": st_mixed["rechecked"],
@@ -392,6 +415,8 @@ def run_ours(args):
     mixed.close()
     fp64.close()
     fp32.close()
+    if fp64r is not None:
+        fp64r.close()
     ctx.close()
     if dist:
         dist.destroy_process_group()

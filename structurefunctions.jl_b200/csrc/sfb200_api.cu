@@ -1099,9 +1099,18 @@ static size_t hist_bytes(bool fp32, int NV, int priv, int NW, int NBP, int lc)
     return (b + 15) & ~(size_t)15;
 }
 
-static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_hist, int priv, int lc = 32)
+// Whether a launch of this plan with tiles of T points sorts its J tiles (sfb200_plan_set_option
+// SFB200_OPT_TILE_SORT): flat 1D kernels of precision FP64 / MIXED, single runs, 256-point tiles.
+static bool sorts_tiles(const sfb200_plan* p, int T, bool batch)
+{
+    return !p->joint && !p->sphere && !p->fp32 && T == 256 && p->sort_ovr != 0 && !batch;
+}
+
+static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_hist, int priv, int lc = 32,
+                         bool batch = false)
 {
     const int NW = T / 32, NBP = p->nb + 2, NV = p->nops_pad;
+    lut_bytes += sorts_tiles(p, T, batch) ? kSortScratchBytes : 0;  // the sort's counters beside the records
     if (p->mixed) {
         const int rec = p->sphere ? 10 : 2 * p->D;  // doubles per j record
         if (p->joint) {
@@ -1234,8 +1243,12 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     const bool dlinear = p->desc.distance.kind == SFB200_BINS_LINEAR;
     int lut_bytes = 0;
     // flat kernels of precision FP64 / MIXED (1D) and MIXED (joint) bin with the byte table when the
-    // plan has one
-    const bool byte_lut = p->d_lut8 && !p->sphere && !p->fp32 && (!p->joint || p->mixed);
+    // plan has one and a block has enough pairs to repay copying its 10 KB into shared memory (about
+    // four 256 x 256 tile pairs; never in batched rounds, whose blocks set up per work item); the
+    // cell table of a few hundred bytes otherwise
+    const long long pairs_per_block = n * (n - 1) / 2 / std::max(1, ctx->nsm * 4);
+    const bool byte_lut = p->d_lut8 && !p->sphere && !p->fp32 && (!p->joint || p->mixed) && !batch &&
+                          pairs_per_block >= (1ll << 18);
     if (byte_lut) lut_bytes = kByteCells + (int)sizeof(double) * kByteEdges;
     else if (p->fp32) lut_bytes = p->lg32.ncell * (int)sizeof(LutEntry32);
     else if (p->mixed) lut_bytes = p->lut64_bytes;  // exact table (flat) or chord table (sphere); 0 if linear
@@ -1299,14 +1312,14 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
             if (!p->cols_ovr) {
                 int smem_sm = 0;
                 CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
-                while (hist_cols > 1 && smem_bytes(p, T, lut_bytes, true, 3, hist_cols) + 1024 > (size_t)smem_sm / 3)
+                while (hist_cols > 1 && smem_bytes(p, T, lut_bytes, true, 3, hist_cols, batch) + 1024 > (size_t)smem_sm / 3)
                     hist_cols /= 2;
             }
         }
-        smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols);
+        smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols, batch);
         while (smem > (size_t)dev_smem_max && T > 32) {
             T /= 2;
-            smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols);
+            smem = smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols, batch);
         }
         if (smem > (size_t)dev_smem_max)
             return set_err(ctx, SFB200_ERR_UNSUPPORTED, "%d bins x %d operators do not fit shared memory",
@@ -1357,7 +1370,8 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     a.lut8 = p->d_lut8;
     a.byte_lut = byte_lut ? 1 : 0;
     // flat 1D kernels (FP64 / MIXED) with 256-point tiles stage off-diagonal J tiles sorted by distance
-    a.sort_j = (!p->joint && !p->sphere && !p->fp32 && T == 256 && p->sort_ovr != 0) ? 1 : 0;
+    // (single runs; the batched rounds keep the storage order, their slices are mostly small)
+    a.sort_j = sorts_tiles(p, T, batch) ? 1 : 0;
     a.edges = p->d_exact;
     a.n_edges = p->desc.distance.n_edges;
     a.dist_linear = dlinear;

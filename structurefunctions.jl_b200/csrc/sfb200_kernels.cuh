@@ -156,6 +156,10 @@ __device__ __forceinline__ void stage_sorted(const double (&rec)[R], bool has, f
     }
 }
 
+// Shared-memory scratch of the tile sort: 256 bucket counters and 8 warp totals (a multiple of 16
+// bytes, so that what follows stays aligned). Reserved only in launches that sort.
+constexpr int kSortScratchBytes = (256 + 8) * 4;
+
 // Flat J tile: record [x(D), u(D) us] of point j0 + t in slot t (storage order) or in distance order
 // from I-tile point `iref` (`sorted`, block-uniform; needs blockDim.x == 256).
 template <int D>
@@ -246,7 +250,6 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
     using Needs = ListNeeds<OPS>;
     using Hist = BlockHist<double, NV, PRIV>;
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ unsigned s_cnt[256], s_wtot[8];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n = a.n;
@@ -254,8 +257,11 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
     const unsigned char* lut8 = smem;
     const double* sqx = reinterpret_cast<const double*>(smem + kByteCells);
     double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);  // T records x(D) u(D)
+    // the tile sort's counters (only when this launch sorts), then the histogram
+    unsigned* s_cnt = reinterpret_cast<unsigned*>(srec + (size_t)2 * D * T);
+    unsigned* s_wtot = s_cnt + 256;
     Hist hist;
-    hist.init(reinterpret_cast<unsigned char*>(srec + (size_t)2 * D * T), NW, a.nb + 2, a.hist_cols);
+    hist.init(reinterpret_cast<unsigned char*>(s_cnt) + (a.sort_j ? kSortScratchBytes : 0), NW, a.nb + 2, a.hist_cols);
     load_bin_table(a, smem);
 
     int iter = 0;

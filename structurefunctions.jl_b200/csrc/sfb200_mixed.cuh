@@ -201,14 +201,15 @@ __device__ __noinline__ FlatValues<D, OPS> flat_values_fp64_ool(double dx0, doub
 // range of j (j > i on a diagonal tile) and no pair is masked; the other histogram modes step the
 // warp in lockstep with out-of-range pairs sent to the dropped row.
 // ================================================================================================
-template <int D, class OPS, int PRIV>
+// SINGLE: the single-run kernel (J-tile sorting and the byte table compiled in); the batched kernel
+// leaves both out, so that its tighter register budget (four blocks per SM) holds without spills.
+template <int D, class OPS, int PRIV, bool SINGLE = true>
 __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, long long p1, long long ps)
 {
     constexpr int NV = OPS::n;
     constexpr int NP = D;  // double2 per j record: x(D) u(D)
     using Hist = BlockHist<float, NV, PRIV>;
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ unsigned s_cnt[256], s_wtot[8];
     const int T = blockDim.x, NW = T >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n = a.n;
@@ -216,8 +217,11 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
     const unsigned char* lut8 = smem;
     const double* sqx = reinterpret_cast<const double*>(smem + kByteCells);
     double* srec = reinterpret_cast<double*>(smem + a.lut_bytes);  // T records of 2D doubles
+    // the tile sort's counters (only when this launch sorts), then the histogram
+    unsigned* s_cnt = reinterpret_cast<unsigned*>(srec + (size_t)2 * NP * T);
+    unsigned* s_wtot = s_cnt + 256;
     Hist hist;
-    hist.init(reinterpret_cast<unsigned char*>(srec + (size_t)2 * NP * T), NW, a.nb + 2, a.hist_cols);
+    hist.init(reinterpret_cast<unsigned char*>(s_cnt) + (a.sort_j ? kSortScratchBytes : 0), NW, a.nb + 2, a.hist_cols);
     load_bin_table(a, smem);
     const int ku = pow2_exponent_above(a.g_stats[2]);
     const double us = ldexp(1.0, -ku);
@@ -242,8 +246,8 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
         const int j0 = tj * T;
         const int jn = min(T, n - j0);
         const bool diag = ti == tj;
-        stage_flat_j<D>(a, j0, jn, us, a.sort_j && !diag && T == 256, ti * T + min(T / 2, n - 1 - ti * T), srec,
-                        s_cnt, s_wtot);
+        stage_flat_j<D>(a, j0, jn, us, SINGLE && a.sort_j && !diag && T == 256, ti * T + min(T / 2, n - 1 - ti * T),
+                        srec, s_cnt, s_wtot);
         __syncthreads();
         // one pair: key (bin) and values
         auto pair = [&](int jj, int& key, float (&v)[NV]) {
@@ -260,7 +264,7 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
             double r2 = h2;
             if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
             bool slow;
-            if (a.byte_lut) {
+            if (SINGLE && a.byte_lut) {
                 key = byte_bin(lut8, sqx, r2, slow);  // slow: several edges in the cell or r^2 outside FP32
             } else {
                 if (a.dist_linear) key = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
@@ -271,7 +275,7 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
             const bool fine = flat_primitives_mx<D, OPS>(dx, du, r2, h2, L, Tt, T2, Q);
             eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
             if (slow || !fine) {
-                if (slow && a.byte_lut) key = count_below_ool(a.edges, a.n_edges, r2);
+                if (SINGLE && slow && a.byte_lut) key = count_below_ool(a.edges, a.n_edges, r2);
                 const FlatValues<D, OPS> f = flat_values_fp64_ool<D, OPS>(
                     dx[0], dx[1], D == 3 ? dx[D - 1] : 0.0, du[0], du[1], D == 3 ? du[D - 1] : 0.0, r2, h2, &a.gen);
 #pragma unroll
@@ -302,7 +306,7 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
 }
 
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256, 3) k_flat1d_mx(const __grid_constant__ PairArgs a)
+__global__ void __launch_bounds__(256, OPS::n >= 4 ? 3 : 4) k_flat1d_mx(const __grid_constant__ PairArgs a)
 {
     flat1d_mx_run<D, OPS, PRIV>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
@@ -311,7 +315,7 @@ __global__ void __launch_bounds__(256, 3) k_flat1d_mx(const __grid_constant__ Pa
 template <int D, class OPS, int PRIV>
 __global__ void __launch_bounds__(256, OPS::n >= 4 ? 3 : 4) k_flat1d_mx_batch(const __grid_constant__ BatchArgs b)
 {
-    batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { flat1d_mx_run<D, OPS, PRIV>(a, q0, q1, 1); });
+    batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { flat1d_mx_run<D, OPS, PRIV, false>(a, q0, q1, 1); });
 }
 
 // ================================================================================================
