@@ -34,11 +34,17 @@ namespace sfb {
 //             the run: the per-pair cost is a compare and one add per operator. (The flat kernels also
 //             stage each J tile sorted by distance from the I tile, so that a lane's bins rise almost
 //             monotonically along its row and its runs last tens to hundreds of pairs.)
+//   PRIV = 6  run-length with two open runs per lane (the same table as PRIV = 3): a lane keeps the
+//             two bins it met most recently open at once, so that a row whose bin alternates between
+//             two neighbours near a bin edge (the lanes of a warp differ in their i point, so the
+//             distance order of a J tile is only approximately each lane's own) extends its runs
+//             instead of ending one at every alternation; a third bin ends the least recently used.
 template <typename R, int NV, int PRIV>
 struct BlockHist {
     static constexpr bool AGG = PRIV == 0;
     static constexpr bool AGG_RED = PRIV == 2;
-    static constexpr bool RUN = PRIV == 3;
+    static constexpr bool RUN2 = PRIV == 6;
+    static constexpr bool RUN = PRIV == 3 || RUN2;
     static constexpr int C = (PRIV == 0 || PRIV == 2 || RUN) ? 1 : PRIV;
     using CountT = typename std::conditional<AGG && sizeof(R) == 8, unsigned long long, unsigned>::type;
 
@@ -50,10 +56,14 @@ struct BlockHist {
     unsigned long long* scnt;  // !AGG: block counts [bin]
     int NBP, NW;
     int LC;         // RUN: table columns (power of two <= 32)
-    // RUN: the lane's open run
+    // RUN: the lane's open run (RUN2: and its second open run, and which of the two was used last)
     int rkey;
     unsigned rc;
     R rs[NV];
+    int rkey2;
+    unsigned rc2;
+    R rs2[NV];
+    bool last2;
 
     // Bytes of shared memory this accumulator needs (mirrored on the host by hist_bytes()); `lc` is
     // the RUN table's column count.
@@ -115,6 +125,23 @@ struct BlockHist {
         rc = 0u;
 #pragma unroll
         for (int o = 0; o < NV; ++o) rs[o] = R(0);
+        if constexpr (RUN2) {
+            rkey2 = NBP - 1;
+            rc2 = 0u;
+#pragma unroll
+            for (int o = 0; o < NV; ++o) rs2[o] = R(0);
+            last2 = false;
+        }
+    }
+
+    // RUN: add a finished run (bin k, values s, count c) into the lane's table column.
+    __device__ __forceinline__ void flush_one(int lane, int k, const R (&sv)[NV], unsigned c)
+    {
+        const int at = k * LC + (lane & (LC - 1));
+        const int plane = NBP * LC;
+#pragma unroll
+        for (int o = 0; o < NV; ++o) atomicAdd(hv + (at + o * plane), sv[o]);
+        atomicAdd(hc + at, c);
     }
 
     // RUN: add the lane's open run into its table column.
@@ -132,6 +159,9 @@ struct BlockHist {
     {
         if constexpr (RUN) {
             if (rc) flush_run(lane);
+            if constexpr (RUN2) {
+                if (rc2) flush_one(lane, rkey2, rs2, rc2);
+            }
             open_empty();
         }
     }
@@ -139,7 +169,38 @@ struct BlockHist {
     // One pair step of the warp: every lane adds its values v under bin `key` (all lanes call).
     __device__ __forceinline__ void add(int key, R (&v)[NV], int lane, int warp)
     {
-        if constexpr (RUN) {
+        if constexpr (RUN2) {
+            bool in1 = key == rkey;
+            if (!in1 && key != rkey2) {  // a third bin: end the least recently used run
+                in1 = last2;
+                R sv[NV];
+#pragma unroll
+                for (int o = 0; o < NV; ++o) sv[o] = in1 ? rs[o] : rs2[o];
+                const unsigned c = in1 ? rc : rc2;
+                if (c) flush_one(lane, in1 ? rkey : rkey2, sv, c);
+                if (in1) {
+                    rkey = key;
+                    rc = 0u;
+#pragma unroll
+                    for (int o = 0; o < NV; ++o) rs[o] = R(0);
+                } else {
+                    rkey2 = key;
+                    rc2 = 0u;
+#pragma unroll
+                    for (int o = 0; o < NV; ++o) rs2[o] = R(0);
+                }
+            }
+            if (in1) {
+#pragma unroll
+                for (int o = 0; o < NV; ++o) rs[o] += v[o];
+                ++rc;
+            } else {
+#pragma unroll
+                for (int o = 0; o < NV; ++o) rs2[o] += v[o];
+                ++rc2;
+            }
+            last2 = !in1;
+        } else if constexpr (RUN) {
             if (key != rkey) {  // the run ends: add it to the table and open an empty one
                 flush_run(lane);
 #pragma unroll

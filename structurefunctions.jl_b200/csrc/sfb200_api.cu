@@ -873,8 +873,9 @@ extern "C" int sfb200_plan_set_launch(sfb200_plan* p, int tile, int privatizatio
     if (tile != 0 && tile != 32 && tile != 64 && tile != 128 && tile != 256 && tile != 512)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile must be 0, 32, 64, 128, 256 or 512");
     if (privatization != -1 && privatization != 0 && privatization != 1 && privatization != 2 &&
-        privatization != 3 && privatization != 4 && privatization != 8 && privatization != 32)
-        return set_err(ctx, SFB200_ERR_INVALID_ARG, "privatization must be -1 (auto), 0, 1, 2, 3, 4, 8 or 32");
+        privatization != 3 && privatization != 4 && privatization != 6 && privatization != 8 &&
+        privatization != 32)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "privatization must be -1 (auto), 0, 1, 2, 3, 4, 6, 8 or 32");
     if (blocks_per_sm < 0 || blocks_per_sm > 32)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "blocks_per_sm must be in 0..32");
     p->tile_ovr = tile;
@@ -1090,7 +1091,7 @@ static size_t hist_bytes(bool fp32, int NV, int priv, int NW, int NBP, int lc)
     size_t b;
     if (priv == 0) {
         b = (size_t)NW * NV * NBP * rs * (fp32 ? 2 : 1) + (size_t)NW * NBP * (fp32 ? 4 : 8);
-    } else if (priv == 3) {
+    } else if (priv == 3 || priv == 6) {
         b = (size_t)NV * NBP * 8 + (size_t)NBP * 8 + (size_t)NV * NBP * lc * rs + (size_t)NBP * lc * 4;
     } else {
         const int C = priv == 2 ? 1 : priv;  // 2: warp-aggregated with leader atomics, one copy
@@ -1140,17 +1141,24 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
     return (size_t)lut_bytes + (((size_t)nx * T * 4 + 15) & ~(size_t)15) + hist_bytes(true, NV, priv, NW, NBP, lc);
 }
 
-// Default histogram mode (overridable per plan): the run-length table.
-static int default_privatization(const sfb200_plan* p)
-{
-    (void)p;
-    return 3;
-}
-
 static long long tile_pairs(long long n, int T)
 {
     const long long nt = (n + T - 1) / T;
     return nt * (nt + 1) / 2;
+}
+
+// Default histogram mode (overridable per plan): two open runs per lane (6) for the flat FP64 and
+// MIXED kernels of single runs with 256-point tiles from 32768 points and a specialised operator list
+// (the generic lists of two and eight operators spill registers in that mode), the run-length table
+// (3) otherwise. Measured on B200 (c1 shape, 3D, four operators, 64 bins): two open runs 9.63 / 11.71 ms
+// (mixed / FP64) against 10.21 / 13.33 ms at 65536 points, 2.55 / 3.11 against 2.66 / 3.55 ms at
+// 32768, but 0.89 against 0.84 ms (mixed) at 16384 and 20-28 % slower with 64-point tiles (c0), where
+// rows are short and the second run's registers cost more than the flushes they save.
+static int default_privatization(const sfb200_plan* p, long long n, int T)
+{
+    const bool generic = p->opl == OPL_GEN1 || p->opl == OPL_GEN2 || p->opl == OPL_GEN4 || p->opl == OPL_GEN8;
+    if (!p->sphere && !p->fp32 && !generic && T == 256 && n >= 32768) return 6;
+    return 3;
 }
 
 // Copies (if on the host), orders and packs the points of one run into `w`, zeroes its histogram,
@@ -1284,16 +1292,6 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
         // kernel's packed cells fewer than 2^20
         flush_every = (int)std::max<long long>(1, (p->mixed ? (1ll << 20) - 1 : (1ll << 31)) / ((long long)T * T));
     } else {
-        const int want = p->priv_ovr >= 0 ? p->priv_ovr : default_privatization(p);
-        if (p->mixed && batch)
-            kc = p->sphere ? pick_sphere1d_mx_batch(p->D, p->opl) : pick_flat1d_mx_batch(p->D, p->opl);
-        else if (p->mixed)
-            kc = p->sphere ? pick_sphere1d_mx(p->D, p->opl, want) : pick_flat1d_mx(p->D, p->opl, want);
-        else if (p->chord64())
-            kc = pick_sphere1d_chord64(p->D, p->opl, want);
-        else
-            kc = p->sphere ? pick_sphere1d(p->D, p->fp32, p->opl, want)
-                           : pick_flat1d(p->D, p->fp32, p->df, p->opl, want);
         if (batch) {
             T = kBatchTile1D;
         } else if (p->tile_ovr) {
@@ -1304,15 +1302,26 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
                 if (tile_pairs(n, cand) >= 4ll * ctx->nsm) { T = cand; break; }
             }
         }
+        int want = p->priv_ovr >= 0 ? p->priv_ovr : default_privatization(p, n, T);
+        if (want == 6 && (p->sphere || p->fp32)) want = 3;  // two open runs: flat FP64 / MIXED kernels only
+        if (p->mixed && batch)
+            kc = p->sphere ? pick_sphere1d_mx_batch(p->D, p->opl) : pick_flat1d_mx_batch(p->D, p->opl);
+        else if (p->mixed)
+            kc = p->sphere ? pick_sphere1d_mx(p->D, p->opl, want) : pick_flat1d_mx(p->D, p->opl, want);
+        else if (p->chord64())
+            kc = pick_sphere1d_chord64(p->D, p->opl, want);
+        else
+            kc = p->sphere ? pick_sphere1d(p->D, p->fp32, p->opl, want)
+                           : pick_flat1d(p->D, p->fp32, p->df, p->opl, want);
         if (T > kc.max_threads) T = kc.max_threads;
-        if (kc.priv == 3) {
+        if (kc.priv == 3 || kc.priv == 6) {
             // run-length table: the most columns (<= 32) that leave room for 3 blocks per SM,
             // at least one column
             hist_cols = p->cols_ovr ? p->cols_ovr : 32;
             if (!p->cols_ovr) {
                 int smem_sm = 0;
                 CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
-                while (hist_cols > 1 && smem_bytes(p, T, lut_bytes, true, 3, hist_cols, batch) + 1024 > (size_t)smem_sm / 3)
+                while (hist_cols > 1 && smem_bytes(p, T, lut_bytes, true, kc.priv, hist_cols, batch) + 1024 > (size_t)smem_sm / 3)
                     hist_cols /= 2;
             }
         }
@@ -1324,7 +1333,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
         if (smem > (size_t)dev_smem_max)
             return set_err(ctx, SFB200_ERR_UNSUPPORTED, "%d bins x %d operators do not fit shared memory",
                            p->nb, p->nops);
-        if (kc.priv == 3) {
+        if (kc.priv == 3 || kc.priv == 6) {
             // FP32 table cells are folded into FP64 before any of them holds more than ~4096
             // pair terms (NW warps x T steps per tile pair add into one column)
             flush_every = (p->fp32 || p->mixed) ? std::max(1, 4096 / ((T / 32) * T)) : 64;

@@ -20,6 +20,7 @@ static KernelChoice flat_entry(int priv)
     switch (priv) {
     case 32: return flat_kernel<D, MODE, OPS, 32>();
     case 3: return flat_kernel<D, MODE, OPS, 3>();
+    case 6: if constexpr (MODE == 0) return flat_kernel<D, MODE, OPS, 6>(); break;
     case 8: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 8>(); break;
     case 4: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 4>(); break;
     case 1: if constexpr (ALL) return flat_kernel<D, MODE, OPS, 1>(); break;

@@ -15,6 +15,7 @@ static KernelChoice flatmx_entry(int priv)
 {
     switch (priv) {
     case 3: return flatmx_kernel<D, OPS, 3>();
+    case 6: return flatmx_kernel<D, OPS, 6>();
     case 32: return flatmx_kernel<D, OPS, 32>();
     case 2: if constexpr (ALL) return flatmx_kernel<D, OPS, 2>(); break;
     case 8: if constexpr (ALL) return flatmx_kernel<D, OPS, 8>(); break;

@@ -329,7 +329,8 @@ __global__ void __launch_bounds__(256) k_flat1d_fp64(const PairArgs a)
         };
         if constexpr (Hist::RUN) {
             if (iv) {
-#pragma unroll 2
+                constexpr int UNR = PRIV == 6 ? 1 : 2;  // two open runs: one pair per iteration
+#pragma unroll (UNR)
                 for (int jj = diag ? (int)threadIdx.x + 1 : 0; jj < jn; ++jj) {
                     int key;
                     double v[NV];

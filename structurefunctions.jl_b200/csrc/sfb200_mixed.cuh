@@ -225,8 +225,6 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
     load_bin_table(a, smem);
     const int ku = pow2_exponent_above(a.g_stats[2]);
     const double us = ldexp(1.0, -ku);
-    double unscale[NV];
-    op_unscale(OPS{}, a.gen, ku, unscale);
 
     int iter = 0;
     for (long long p = p0; p < p1; p += ps, ++iter) {
@@ -284,7 +282,10 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
         };
         if constexpr (Hist::RUN) {
             if (iv) {
-#pragma unroll 2
+                // two open runs (PRIV 6): one pair per iteration, so that their extra registers fit
+                // the three-block bound without spills
+                constexpr int UNR = PRIV == 6 ? 1 : 2;
+#pragma unroll (UNR)
                 for (int jj = diag ? (int)threadIdx.x + 1 : 0; jj < jn; ++jj) {
                     int key;
                     float v[NV];
@@ -302,6 +303,8 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
             }
         }
     }
+    double unscale[NV];  // formed after the pair loop: no registers held across it
+    op_unscale(OPS{}, a.gen, pow2_exponent_above(a.g_stats[2]), unscale);
     hist.merge(a.g_sums, a.g_counts, a.nops, a.nb, unscale);
 }
 

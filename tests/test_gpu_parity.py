@@ -156,13 +156,14 @@ def test_joint_sphere(precision, tol):
 
 
 @pytest.mark.parametrize("precision,tol", PRECISIONS)
-@pytest.mark.parametrize("priv", [0, 1, 2, 3, 4, 8, 32])
+@pytest.mark.parametrize("priv", [0, 1, 2, 3, 4, 6, 8, 32])
 @pytest.mark.parametrize("tile", [32, 64, 256])
 def test_privatization_modes(precision, tol, priv, tile):
     """Every histogram privatization depth and tile size gives the oracle's histogram."""
     w = synthetic.config("c1", n=1500)
     gs, gc, st = run_gpu(w.ops, w.x, w.u, w.distance_bins.edges, precision=precision, tile=tile, priv=priv)
-    assert st["privatization"] == priv and st["tile"] <= tile
+    # two open runs (6) exist in the flat FP64 and MIXED kernels; FP32-bulk plans take the run table
+    assert st["privatization"] == (3 if priv == 6 and precision == "fp32" else priv) and st["tile"] <= tile
     rs, rc, ra = run_oracle(w.ops, w.x, w.u, w.distance_bins.edges)
     nb = len(w.distance_bins) - 1
     for k in range(len(w.ops)):
