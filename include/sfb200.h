@@ -80,7 +80,13 @@ typedef enum {
     SFB200_OP_S3 = 2,        /* ThirdOrderStructureFunctionType: du_L |du|^2 */
     SFB200_OP_FULLVEC = 3,   /* FullVectorStructureFunctionType{NF}: |du|^NF */
     SFB200_OP_T2C = 4,       /* TransverseComponentSecondOrderStructureFunctionType: |du_t|^2/(D-1) */
-    SFB200_OP_L1T2C = 5      /* LongitudinalTransverseComponentThirdOrderStructureFunctionType */
+    SFB200_OP_L1T2C = 5,     /* LongitudinalTransverseComponentThirdOrderStructureFunctionType */
+    SFB200_OP_SP2D = 6       /* one of the six invariants of the two-dimensional single pass, nl = its row
+                                (0 S2, 1 L2, 2 T2, 3 S3, 4 L3, 5 L1T2), with that pass's own formulas: flat
+                                du_L = (du . dx) * inv(sqrt(r2)), sphere du_L = du . r_hat, |du|^2 = du . du,
+                                S2 = |du|^2, L2 = du_L^2, T2 = |du|^2 - L2, S3 = du_L |du|^2, L3 = du_L L2,
+                                L1T2 = du_L T2 (src/Calculations/serial_single_pass.jl:886-905 flat,
+                                :838-843 other metrics) */
 } sfb200_op_kind;
 
 typedef struct {

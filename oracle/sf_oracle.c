@@ -160,10 +160,29 @@ static double transverse_norm2(const double* du, const double* r, int D)
     return s - dl * dl;
 }
 
-/* The operator functor sf(du, r_hat) (src/StructureFunctionTypes.jl:58-151). */
+/* Row t of the two-dimensional single pass from du_L and |du|^2: (dn2, duL2, dn2 - duL2, duL dn2,
+ * duL duL2, duL (dn2 - duL2)) (src/Calculations/serial_single_pass.jl:840-843, 901-905). */
+static double sp2d_row(int t, double duL, double dn2)
+{
+    const double duL2 = duL * duL;
+    switch (t) {
+    case 0: return dn2;
+    case 1: return duL2;
+    case 2: return dn2 - duL2;
+    case 3: return duL * dn2;
+    case 4: return duL * duL2;
+    case 5: return duL * (dn2 - duL2);
+    }
+    return NAN;
+}
+
+/* The operator functor sf(du, r_hat) (src/StructureFunctionTypes.jl:58-151). The single-pass rows
+ * take du_L = du . r_hat and |du|^2 = du . du (src/Calculations/serial_single_pass.jl:839-841). */
 static double sf_functor(const sfb200_operator* op, int D, const double* du, const double* r)
 {
     switch (op->kind) {
+    case SFB200_OP_SP2D:
+        return sp2d_row(op->nl, dotn(du, r, D), dotn(du, du, D));
     case SFB200_OP_PROJECTED: {
         double ex = 1.0;
         if (op->nl != 0) ex = ex * lit_pow(dotn(du, r, D), op->nl);
@@ -196,6 +215,10 @@ static double sf_functor(const sfb200_operator* op, int D, const double* du, con
 /* _sf_raw(sf, du, dx, r2) (src/StructureFunctionTypes.jl:227-245). */
 static double sf_raw(const sfb200_operator* op, int D, const double* du, const double* dx, double r2)
 {
+    if (op->kind == SFB200_OP_SP2D) { /* flat single pass (src/Calculations/serial_single_pass.jl:889-893) */
+        const double inv_r = 1.0 / sqrt(r2);
+        return sp2d_row(op->nl, dotn(du, dx, D) * inv_r, dotn(du, du, D));
+    }
     if (op->kind == SFB200_OP_S2) return norm2(du, D);
     if (op->kind == SFB200_OP_PROJECTED && op->nl == 2 && op->nt == 0) {
         const double p = dotn(du, dx, D);

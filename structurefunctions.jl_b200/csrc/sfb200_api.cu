@@ -341,6 +341,7 @@ static int op_order(const sfb200_operator& o)
     case SFB200_OP_S2: case SFB200_OP_T2C: return 2;
     case SFB200_OP_S3: case SFB200_OP_L1T2C: return 3;
     case SFB200_OP_FULLVEC: return o.nf;
+    case SFB200_OP_SP2D: return o.nl < 3 ? 2 : 3;
     }
     return 1;
 }
@@ -631,8 +632,10 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "a joint histogram takes exactly one operator");
     for (int k = 0; k < d.n_ops; ++k) {
         const sfb200_operator& o = d.ops[k];
-        if (o.kind < SFB200_OP_PROJECTED || o.kind > SFB200_OP_L1T2C)
+        if (o.kind < SFB200_OP_PROJECTED || o.kind > SFB200_OP_SP2D)
             return set_err(ctx, SFB200_ERR_UNSUPPORTED, "unknown operator kind %d", o.kind);
+        if (o.kind == SFB200_OP_SP2D && o.nl > 5)
+            return set_err(ctx, SFB200_ERR_INVALID_ARG, "single-pass row must be in 0..5");
         if (o.nl < 0 || o.nt < 0 || o.nf < 0 || o.nl > 16 || o.nt > 16 || o.nf > 16)
             return set_err(ctx, SFB200_ERR_INVALID_ARG, "operator powers must be in 0..16");
     }
@@ -1116,7 +1119,8 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
         const int rec = p->sphere ? 10 : 2 * p->D;  // doubles per j record
         if (p->joint) {
             const size_t ndp = (size_t)((p->nb + 31) & ~31);  // slots per value bin (swizzled rows)
-            return (size_t)lut_bytes + (size_t)rec * T * 8 + (ndp * p->nv + ndp * p->nfine) * 8 +
+            // cells (split words), fine words (split) and FP64 cells of the bins near zero, centres
+            return (size_t)lut_bytes + (size_t)rec * T * 8 + (ndp * p->nv + 2 * ndp * p->nfine) * 8 +
                    (size_t)p->nv * 12;  // + value-bin centres (FP64 and FP32)
         }
         return (size_t)lut_bytes + (size_t)rec * T * 8 + hist_bytes(true, NV, priv, NW, NBP, lc);

@@ -66,11 +66,30 @@ __device__ __forceinline__ double x_transverse_norm2(const double* du, const dou
     return SFB_SUB(x_norm2<D>(du), SFB_MUL(dl, dl));
 }
 
-// sf(du, r_hat), src/StructureFunctionTypes.jl:58-151.
+// Row t of the two-dimensional single pass from du_L and |du|^2, in the reference's order
+// (src/Calculations/serial_single_pass.jl:840-843, 901-905).
+__device__ __forceinline__ double x_sp2d_row(int t, double duL, double dn2)
+{
+    const double duL2 = SFB_MUL(duL, duL);
+    switch (t) {
+    case 0: return dn2;
+    case 1: return duL2;
+    case 2: return SFB_SUB(dn2, duL2);
+    case 3: return SFB_MUL(duL, dn2);
+    case 4: return SFB_MUL(duL, duL2);
+    case 5: return SFB_MUL(duL, SFB_SUB(dn2, duL2));
+    }
+    return __longlong_as_double(0x7ff8000000000000ll);
+}
+
+// sf(du, r_hat), src/StructureFunctionTypes.jl:58-151; for the single-pass rows du_L = du . r_hat and
+// |du|^2 = du . du (src/Calculations/serial_single_pass.jl:839-841, the path of every metric but the
+// flat one).
 template <int D>
 __device__ double x_functor(const sfb200_operator& op, const double* du, const double* r)
 {
     switch (op.kind) {
+    case SFB200_OP_SP2D: return x_sp2d_row(op.nl, x_dot<D>(du, r), x_dot<D>(du, du));
     case SFB200_OP_PROJECTED: {
         double ex = 1.0;
         if (op.nl != 0) ex = SFB_MUL(ex, x_lit_pow(x_dot<D>(du, r), op.nl));
@@ -101,6 +120,10 @@ __device__ double x_functor(const sfb200_operator& op, const double* du, const d
 template <int D>
 __device__ double x_sf_raw(const sfb200_operator& op, const double* du, const double* dx, double r2)
 {
+    if (op.kind == SFB200_OP_SP2D) {  // flat single pass: du_L = (du . dx) * inv(sqrt(r2)) (:889-893)
+        const double inv_r = SFB_DIV(1.0, SFB_SQRT(r2));
+        return x_sp2d_row(op.nl, SFB_MUL(x_dot<D>(du, dx), inv_r), x_dot<D>(du, du));
+    }
     if (op.kind == SFB200_OP_S2) return x_norm2<D>(du);
     if (op.kind == SFB200_OP_PROJECTED && op.nl == 2 && op.nt == 0) {
         const double p = x_dot<D>(du, dx);

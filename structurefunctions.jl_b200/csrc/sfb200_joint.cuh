@@ -12,7 +12,9 @@
 // offset from its value-bin centre, in 64-bit fixed point: a cell's values lie within half a bin
 // width h of c_vbin, so with the power-of-two scale S = 2^k, h S < 2^30, every offset is one integer
 // of at most 2^30 and a block's cell sum stays exact (the quantum 1/S is below 2^-30 h). The merge
-// rebuilds sum = count * c_vbin + residual / S in FP64. Pairs whose value (or distance) lies within
+// rebuilds sum = count * c_vbin + residual / S in FP64. In the value bins near zero (within two half
+// widths), where a value can be tiny next to that quantum, the same 64-bit word holds an FP64 sum of
+// the offsets instead (shared FP64 atomic add). Pairs whose value (or distance) lies within
 // the FP32 error bound of an edge are recomputed in FP64 with the reference arithmetic.
 //
 // Both kernels move their block histogram to the global one every `flush_every` tile pairs, so a
@@ -168,15 +170,24 @@ __device__ __forceinline__ float dot2(const float* x, const float* y)
     return __fadd_rn(p, e);
 }
 
-// Add the block's cells (count, fixed-point offset sum) into the global FP64 histogram and clear
-// them (all threads, after a barrier).
+// Whether value bin vb (1-based) keeps its offsets as an FP64 sum (the bins near zero, where a value
+// can be tiny next to a quantum tied to the bin width) rather than in fixed point.
+__device__ __forceinline__ bool fine_value_bin(const PairArgs& a, int vb)
+{
+    return (unsigned)(vb - a.vfine_lo) < (unsigned)a.nfine;
+}
+
+// Add the block's cells (count, offset sum: fixed point, or FP64 in the fine bins) into the global FP64
+// histogram and clear them (all threads, after a barrier).
 __device__ __forceinline__ void joint_flush_mixed(const PairArgs& a, unsigned long long* hres, unsigned* hc,
                                                   int ncell)
 {
     for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
         if (hc[k]) {
             const int vb = k / a.nb + 1;
-            const double s = (double)hc[k] * value_center(a, vb) + (double)(long long)hres[k] * a.vq_inv;
+            const double off = fine_value_bin(a, vb) ? __longlong_as_double((long long)hres[k])
+                                                     : (double)(long long)hres[k] * a.vq_inv;
+            const double s = (double)hc[k] * value_center(a, vb) + off;
             atomicAdd(&a.g_sums[k], s);
             atomicAdd(&a.g_counts[k], (unsigned long long)hc[k]);
             hres[k] = 0ull;
@@ -351,7 +362,8 @@ __global__ void __launch_bounds__(512) k_joint_mixed(const PairArgs a)
                 const int cell = (db - 1) + nd * (vb - 1);
                 const double c = value_center(a, vb);
                 const double off = (slow ? v64 : (double)val) - c;
-                atomicAdd(&hres[cell], (unsigned long long)__double2ll_rn(off * a.vq));
+                if (fine_value_bin(a, vb)) atomicAdd(reinterpret_cast<double*>(&hres[cell]), off);
+                else atomicAdd(&hres[cell], (unsigned long long)__double2ll_rn(off * a.vq));
                 atomicAdd(&hc[cell], 1u);
             }
         }

@@ -65,6 +65,7 @@ __device__ __forceinline__ int op_order_of(const sfb200_operator& g)
         case SFB200_OP_S2: case SFB200_OP_T2C: return 2;
         case SFB200_OP_S3: case SFB200_OP_L1T2C: return 3;
         case SFB200_OP_FULLVEC: return g.nf;
+        case SFB200_OP_SP2D: return g.nl < 3 ? 2 : 3;
         }
         return 0;
     }
@@ -591,8 +592,12 @@ __global__ void __launch_bounds__(256, 3) k_sphere1d_mx_batch(const BatchArgs b)
 // (quantum 2^-21 of the largest half bin width or finer; the packed word decodes exactly while the
 // cell holds fewer than 2^20 pairs and the offset sum stays below 2^43 in magnitude, so blocks flush
 // at least every 2^20 - 1 pairs). That quantum is far below the 1e-6 tolerance for every value bin
-// whose values stay at least a half width away from zero; the bins closer to zero (where a value
-// can be tiny next to the quantum) keep their offsets in a separate 64-bit word at 2^-30.
+// whose values stay at least a half width away from zero; the bins closer to zero keep their offsets
+// in a separate 64-bit word at 2^-30 of the largest half width. There a value can still be tiny next
+// to that quantum (S2 or L3 of close pairs on a linear axis around zero, the low bins of a log axis):
+// a pair whose |value| is below 2^-8 of the largest half width takes the exact FP64 route and adds its
+// FP64 offset into a third, FP64 cell (a shared 64-bit compare-and-swap add, for those pairs only), so
+// that every fixed-point offset carries at most 2^-23 of its own value.
 //
 // Offsets are taken from C_b, the value-bin centre rounded to FP32 in the scaled units of the FP32
 // value (per block in shared memory, with its exact FP64 image for the flush). In every coarse bin
@@ -636,7 +641,8 @@ struct SplitWords {
 __device__ __forceinline__ int joint_slot(int d0, int v0, int ndp) { return v0 * ndp + (d0 ^ (v0 & 31)); }
 
 __device__ __forceinline__ void joint_flush_packed(const PairArgs& a, const SplitWords& hcell,
-                                                   const SplitWords& hfine, int ndp, const double* vcen)
+                                                   const SplitWords& hfine, double* htiny, int ndp,
+                                                   const double* vcen)
 {
     const int nd = a.nb;
     const int nslot = ndp * a.nv;
@@ -649,7 +655,11 @@ __device__ __forceinline__ void joint_flush_packed(const PairArgs& a, const Spli
         const int d0 = (k - v0 * ndp) ^ (v0 & 31);  // slots of distance bins >= nd are never written
         double s = (double)cnt * vcen[v0] + (double)off * a.vqc_inv;
         const int f = v0 + 1 - a.vfine_lo;
-        if ((unsigned)f < (unsigned)a.nfine) s += (double)(long long)hfine.take(joint_slot(d0, f, ndp)) * a.vq_inv;
+        if ((unsigned)f < (unsigned)a.nfine) {
+            const int fs = joint_slot(d0, f, ndp);
+            s += (double)(long long)hfine.take(fs) * a.vq_inv + htiny[fs];
+            htiny[fs] = 0.0;
+        }
         const int cell = d0 + nd * v0;
         atomicAdd(&a.g_sums[cell], s);
         atomicAdd(&a.g_counts[cell], cnt);
@@ -660,9 +670,10 @@ __device__ __forceinline__ void joint_flush_packed(const PairArgs& a, const Spli
 // Exact FP64 route of one joint pair (i, j) (the reference formula for the distance bin, the value
 // and the value bin), kept out of line: the pair loop only branches to it for the rare pairs that
 // need it. `a` points to the kernel's parameters in place (grid constants); q, fq are the coarse and
-// fine fixed-point offsets from the value-bin centre.
+// fine fixed-point offsets from the value-bin centre, fo the offset in FP64 and v the value.
 struct JointExact {
     int db, vb, q, fq;
+    double fo, v;
     bool ok;
 };
 
@@ -671,7 +682,7 @@ __device__ __noinline__ JointExact joint_exact_pair(const PairArgs* ap, int i, i
 {
     const PairArgs& a = *ap;
     const int n = a.n;
-    JointExact r{0, 0, 0, 0, true};
+    JointExact r{0, 0, 0, 0, 0.0, 0.0, true};
     double du64[D], v64;
     if constexpr (!SPHERE) {
         double dx64[D];
@@ -703,6 +714,8 @@ __device__ __noinline__ JointExact joint_exact_pair(const PairArgs* ap, int i, i
         const double off = v64 - vcen[r.vb - 1];  // exact: both within a bin of each other
         r.q = __double2int_rn(off * a.vqc);
         r.fq = __double2int_rn(off * a.vq);
+        r.fo = off;
+        r.v = v64;
     }
     return r;
 }
@@ -726,12 +739,13 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     const int nfw = ndp * a.nfine;
     const SplitWords hcell{words, words + ncell};                                  // 2 x ncell
     const SplitWords hfine{words + 2 * ncell, words + 2 * ncell + nfw};            // 2 x ndp * nfine
-    double* vcen = reinterpret_cast<double*>(words + 2 * (ncell + nfw));           // nv
+    double* htiny = reinterpret_cast<double*>(words + 2 * (ncell + nfw));          // ndp * nfine (FP64)
+    double* vcen = htiny + nfw;                                                    // nv
     float* vc32 = reinterpret_cast<float*>(vcen + nv);                             // nv
     __shared__ unsigned long long s_recheck;
 
     load_bin_table(a, smem);
-    for (int k = threadIdx.x; k < 2 * (ncell + nfw); k += T) words[k] = 0u;
+    for (int k = threadIdx.x; k < 2 * ncell + 4 * nfw; k += T) words[k] = 0u;
     if (threadIdx.x == 0) s_recheck = 0ull;
     unsigned my_recheck = 0;
     const int ku = pow2_exponent_above(a.g_stats[2]);
@@ -747,6 +761,9 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     // centre and the fixed-point scale to be normal FP32 numbers
     const float vqcs = (float)(a.vqc * unscale[0]);
     const float vqfs = (float)(a.vq * unscale[0]);
+    // below this |value| (2^-8 of the largest half width) a pair of a bin near zero takes the FP64 route
+    const double tiny64 = ldexp(a.vq_inv, 22);
+    const float tiny32 = (float)(tiny64 / unscale[0]);
     bool cok = vfast && vqcs != 0.f && f32_zero_or_normal(vqcs) && vqfs != 0.f && f32_zero_or_normal(vqfs);
     for (int k = threadIdx.x; k < nv; k += T) {
         const double c64 = value_center(a, k + 1);
@@ -768,7 +785,7 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     for (long long p = p0; p < p1; p += ps, ++iter) {
         if (iter && iter % a.flush_every == 0) {
             __syncthreads();
-            joint_flush_packed(a, hcell, hfine, ndp, vcen);
+            joint_flush_packed(a, hcell, hfine, htiny, ndp, vcen);
         }
         int ti, tj;
         decode_tile_pair(p, a.ntiles, ti, tj);
@@ -835,7 +852,8 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                 const float fr = t - fl;
                 const float wt = (fabsf(t) + fabsf(vnegf)) * a.vrel;
                 vb = (int)fminf(fmaxf(fl, -1.f), tmax) + 1;  // 0 below the range, nv + 1 above
-                slow = slow || !fine || !(fr > wt && fr < 1.f - wt);
+                const bool tiny = (unsigned)(vb - a.vfine_lo) < (unsigned)a.nfine && fabsf(val) < tiny32;
+                slow = slow || !fine || tiny || !(fr > wt && fr < 1.f - wt);
                 // offset from the bin centre as the exact FP32 sum s + e (TwoSum; e = 0 in the coarse
                 // bins, where the subtraction is exact), then both fixed-point images
                 const float c = vc32[min(max(vb, 1), nv) - 1];
@@ -856,6 +874,13 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                 fq = x.fq;
                 ok = x.ok;
                 ++my_recheck;
+                const int f = vb - a.vfine_lo;
+                if (ok && db >= 1 && db <= nd && (unsigned)f < (unsigned)a.nfine && fabs(x.v) < tiny64) {
+                    // a tiny value near zero: its exact FP64 offset now, only the count in the cell
+                    atomicAdd(&htiny[joint_slot(db - 1, f, ndp)], x.fo);
+                    r.cell = joint_slot(db - 1, vb - 1, ndp);
+                    return r;
+                }
             }
             if (ok && db >= 1 && db <= nd && vb >= 1 && vb <= nv) {
                 r.cell = joint_slot(db - 1, vb - 1, ndp);
@@ -887,7 +912,7 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     }
     if (my_recheck) atomicAdd(&s_recheck, (unsigned long long)my_recheck);
     __syncthreads();
-    joint_flush_packed(a, hcell, hfine, ndp, vcen);
+    joint_flush_packed(a, hcell, hfine, htiny, ndp, vcen);
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 

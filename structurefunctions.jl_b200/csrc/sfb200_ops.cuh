@@ -82,6 +82,15 @@ __device__ __forceinline__ R gen_value(const sfb200_operator& o, R L, R T, R T2,
     case SFB200_OP_FULLVEC: return o.nf == 2 ? Q : ipow(sqrt(Q), o.nf);
     case SFB200_OP_T2C: return T2 / R(D - 1);
     case SFB200_OP_L1T2C: return L * (T2 / R(D - 1));
+    case SFB200_OP_SP2D:  // rows S2, L2, T2, S3, L3, L1T2 of the two-dimensional single pass
+        switch (o.nl) {
+        case 0: return Q;
+        case 1: return L * L;
+        case 2: return T2;
+        case 3: return L * Q;
+        case 4: return L * L * L;
+        case 5: return L * T2;
+        }
     }
     return R(0) / R(0);
 }

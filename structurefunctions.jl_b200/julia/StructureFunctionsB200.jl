@@ -345,6 +345,85 @@ function SFC._dispatch_single_pass!(
     return single_pass_into!(b, sums, counts, x, u, distance_bins, distance_metric)
 end
 
+# ---------------------------------------------------------------------- two-dimensional single pass
+#
+# calculate_structure_functions_single_pass_2d[!] (src/Calculations/serial_single_pass.jl:712-728,
+# 1161-1181) route here through _dispatch_single_pass_2d[!]. Row t of the (6, n_dist, n_val)
+# accumulator is the joint histogram of invariant t (S2, L2, T2, S3, L3, L1T2), computed on the device
+# with the pass's own formulas (operator kind SFB200_OP_SP2D, nl = t - 1; flat du_L = (du . dx) *
+# inv(sqrt(r2)), serial_single_pass.jl:889-893) and binned on that row's value edges as the reference's
+# scatter digitizes them (:852-864): a LinearBinEdges by its FMA search, any other vector or range by
+# searchsortedfirst over its elements.
+
+struct SP2DRow <: SFT.AbstractPairwiseStructureFunctionType
+    t::Int
+end
+c_op(r::SP2DRow) = COperator(6, r.t - 1, 0, 0)
+
+# a row's value axis cut to its first n_val + 1 edges (bins above n_val are dropped by the scatter)
+function sp2d_row_bins(vb, n_val::Int)
+    vb isa SF.LinearBinEdges && length(vb) == n_val + 1 && return vb
+    vb isa SF.LinearBinEdges && throw(ArgumentError("B200Backend needs a LinearBinEdges value axis of exactly n_val + 1 edges"))
+    vb isa SF.InfPaddedBinEdges && throw(ArgumentError("InfPaddedBinEdges are not supported by B200Backend"))
+    return Float64.(collect(vb))[1:n_val + 1]
+end
+
+# Adds the six rows of one point set into `sums` / `counts` ((6, n_dist, n_val)).
+function single_pass_2d_into!(b::B200Backend, sums::AbstractArray, counts::AbstractArray, x, u, distance_bins,
+                              value_bins, metric)
+    nd, n_val = size(sums, 2), size(sums, 3)
+    SFC._validate_value_bins!(value_bins, n_val)
+    s = zeros(Float64, nd * n_val)
+    c = zeros(UInt64, nd * n_val)
+    for t in 1:SFC.SINGLE_PASS_N
+        vb = sp2d_row_bins(value_bins isa Tuple ? value_bins[t] : value_bins, n_val)
+        run_pairs(b, (SP2DRow(t),), x, u, distance_bins, vb, metric, s, c, UInt32(0))
+        @views sums[t, :, :] .+= reshape(s, nd, n_val)
+        @views counts[t, :, :] .+= reshape(c, nd, n_val)
+    end
+    return sums, counts
+end
+
+function SFC._dispatch_single_pass_2d(
+    b::B200Backend, ::SFC.PointField, x::AbstractMatrix{FT1}, u::AbstractMatrix{FT2}, distance_bins::AbstractVector,
+    value_bins::SFC.SinglePass2DValueBins; count_eltype::Type{CT} = UInt32,
+    distance_metric::DI.PreMetric = DI.Euclidean(), kwargs...,
+) where {FT1, FT2, CT}
+    OT = promote_type(float(FT1), float(FT2))
+    nd = length(distance_bins) - 1
+    n_val = length(value_bins isa Tuple ? value_bins[1] : value_bins) - 1
+    sums = zeros(OT, SFC.SINGLE_PASS_N, nd, n_val)
+    counts = zeros(CT, SFC.SINGLE_PASS_N, nd, n_val)
+    single_pass_2d_into!(b, sums, counts, x, u, distance_bins, value_bins, distance_metric)
+    return (sums = sums, counts = counts)
+end
+
+function SFC._dispatch_single_pass_2d(
+    b::B200Backend, shape::Union{SFC.SharedPositionField, SFC.VaryingPositionField}, x::AbstractArray{FT1},
+    u::AbstractArray{FT2}, distance_bins::AbstractVector, value_bins::SFC.SinglePass2DValueBins;
+    count_eltype::Type{CT} = UInt32, distance_metric::DI.PreMetric = DI.Euclidean(), kwargs...,
+) where {FT1, FT2, CT}
+    OT = promote_type(float(FT1), float(FT2))
+    nd = length(distance_bins) - 1
+    n_val = length(value_bins isa Tuple ? value_bins[1] : value_bins) - 1
+    aux = size(u)[3:end]
+    sums = zeros(OT, SFC.SINGLE_PASS_N, nd, n_val, aux...)
+    counts = zeros(CT, SFC.SINGLE_PASS_N, nd, n_val, aux...)
+    for (k, (xb, ub)) in zip(CartesianIndices(aux), aux_slices(x, u))
+        single_pass_2d_into!(b, view(sums, :, :, :, k), view(counts, :, :, :, k), xb, ub, distance_bins,
+                             value_bins, distance_metric)
+    end
+    return (sums = sums, counts = counts)
+end
+
+function SFC._dispatch_single_pass_2d!(
+    b::B200Backend, sums_3d::AbstractArray, counts_3d::AbstractArray, x::AbstractMatrix, u::AbstractMatrix,
+    distance_bins::AbstractVector, value_bins::SFC.SinglePass2DValueBins;
+    distance_metric::DI.PreMetric = DI.Euclidean(), kwargs...,
+)
+    return single_pass_2d_into!(b, sums_3d, counts_3d, x, u, distance_bins, value_bins, distance_metric)
+end
+
 # auxiliary-axis shapes (src/Calculations/shapes.jl:19-20): one pair pass per auxiliary slice, results
 # of shape (n_bins, aux...) / (n_dist, n_val, aux...) as the reference's batch drivers return them
 # (src/Calculations/batch.jl:209-217)

@@ -15,7 +15,9 @@ from .operators import *  # noqa: F401,F403  (operator types and singletons)
 from .operators import get_structure_function_type, order
 from .results import (AbstractStructureFunction, StructureFunction, StructureFunction2DSumsAndCounts,
                       StructureFunctionSumsAndCounts, bin_average, marginalize)
-from .single_pass import (SINGLE_PASS_OPERATORS, HelmholtzDecomposition2D, calculate_structure_functions_single_pass,
+from .single_pass import (SINGLE_PASS_OPERATORS, HelmholtzDecomposition2D, SinglePass2DRow,
+                          calculate_structure_functions_single_pass, calculate_structure_functions_single_pass_2d,
+                          calculate_structure_functions_single_pass_2d_inplace,
                           calculate_structure_functions_single_pass_inplace, helmholtz_decompose_2d)
 
 __version__ = "0.1.0"

@@ -29,6 +29,7 @@ OP_S3 = 2
 OP_FULLVEC = 3
 OP_T2C = 4
 OP_L1T2C = 5
+OP_SP2D = 6  # row nl of the two-dimensional single pass (S2, L2, T2, S3, L3, L1T2)
 
 BINS_TABLE = 0
 BINS_SQTABLE = 1

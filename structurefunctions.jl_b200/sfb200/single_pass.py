@@ -4,6 +4,9 @@
                                               distance_metric)
     calculate_structure_functions_single_pass_inplace(sums, counts, x, u, distance_bins; ...)
     helmholtz_decompose_2d(distance_bins, L2_sums, L2_counts, T2_sums, T2_counts)
+    calculate_structure_functions_single_pass_2d(x, u, distance_bins, value_bins; ...)
+    calculate_structure_functions_single_pass_2d_inplace(sums_3d, counts_3d, x, u, distance_bins,
+                                                         value_bins; ...)
 
 One pass over the pairs accumulates four rows per distance bin -- S2 = |du|^2, L2 = du_L^2,
 S3 = du_L |du|^2 and L3 = du_L^3 -- in one fused kernel (operator list {S2SF, L2SF, S3SF, L3SF});
@@ -14,14 +17,20 @@ S2, L2, T2, S3, L3, L1T2 (SINGLE_PASS_N = 6, src/Calculations/batch_api.jl:98).
 """
 import numpy as np
 
-from .api import (B200Backend, _finalize, _output_float_type, _run, _shape_of, assert_counts_representable,
-                  default_backend, validate_array_shape)
+from dataclasses import dataclass
+
+from . import _abi
+from .api import (B200Backend, PointField, _aux_slices, _finalize, _output_float_type, _run, _shape_of,
+                  assert_counts_representable, default_backend, validate_array_shape)
+from .bins import BinEdges, LinearBinEdges, as_bin_edges
 from .errors import ArgumentError, DimensionMismatch
 from .metrics import Euclidean
-from .operators import (DiagonalConsistentThirdOrderStructureFunction, LongitudinalSecondOrderStructureFunction,
-                        OffDiagonalInconsistentThirdOrderStructureFunction, SecondOrderStructureFunction,
-                        ThirdOrderStructureFunction, TransverseSecondOrderStructureFunction)
-from .results import AbstractStructureFunction, StructureFunction, StructureFunctionSumsAndCounts, bin_average
+from .operators import (AbstractPairwiseStructureFunctionType, DiagonalConsistentThirdOrderStructureFunction,
+                        LongitudinalSecondOrderStructureFunction, OffDiagonalInconsistentThirdOrderStructureFunction,
+                        SecondOrderStructureFunction, ThirdOrderStructureFunction,
+                        TransverseSecondOrderStructureFunction)
+from .results import (AbstractStructureFunction, StructureFunction, StructureFunction2DSumsAndCounts,
+                      StructureFunctionSumsAndCounts, bin_average)
 
 SINGLE_PASS_N = 6
 
@@ -157,3 +166,156 @@ def calculate_structure_functions_single_pass_inplace(sums, counts, x, u, distan
     counts[0] += c6[0].astype(counts.dtype)
     derive_rows(sums, counts)
     return sums, counts
+
+
+# ------------------------------------------------------------------- two-dimensional single pass
+#
+# calculate_structure_functions_single_pass_2d (src/Calculations/serial_single_pass.jl:1161-1181) bins
+# each of the six invariants of a pair on its own value axis: row t of the (6, n_dist, n_val)
+# accumulator is the joint (distance x value) histogram of invariant t, with that invariant's counts
+# (_sp2d_scatter!, src/Calculations/serial_single_pass.jl:852-864). Every row runs as one joint histogram on the GPU
+# whose value is the invariant in the pass's own formulas (operator kind SFB200_OP_SP2D): flat
+# du_L = (du . dx) * inv(sqrt(r2)) (:889-893), other metrics du_L = du . r_hat (:839), |du|^2 = du . du,
+# and the rows (|du|^2, du_L^2, |du|^2 - du_L^2, du_L |du|^2, du_L^3, du_L (|du|^2 - du_L^2)) (:843, :905).
+# Value bins are digitized as the reference's scatter does (SFH.digitize, :856): a plain vector by
+# searchsortedfirst(edges, v) - 1 (src/HelperFunctions.jl:77-84), a LinearBinEdges by its FMA search
+# (src/BinEdges.jl:114-131), a LogBinEdges by its exact edge comparisons (a sorted-table search).
+
+
+@dataclass(frozen=True)
+class SinglePass2DRow(AbstractPairwiseStructureFunctionType):
+    """Row `t` (0-based: S2, L2, T2, S3, L3, L1T2) of the two-dimensional single pass as the value of a
+    joint histogram (C-ABI operator kind SFB200_OP_SP2D)."""
+
+    t: int
+
+    def __post_init__(self):
+        if not 0 <= int(self.t) < SINGLE_PASS_N:
+            raise ValueError("single-pass row must be in 0..5")
+
+    def as_abi(self):
+        return _abi.Operator(_abi.OP_SP2D, int(self.t), 0, 0)
+
+    def order(self):
+        return 2 if self.t < 3 else 3
+
+
+def _sp2d_value_bins(value_bins):
+    """Per-row edge vectors and n_val of a SinglePass2DValueBins (a vector shared by the six rows or a
+    6-tuple, src/Calculations/batch_api.jl:101-146): n_val = length(first) - 1 and every row needs at
+    least n_val + 1 edges (_validate_value_bins!)."""
+
+    if isinstance(value_bins, tuple):
+        if len(value_bins) != SINGLE_PASS_N:
+            raise DimensionMismatch(
+                f"single-pass 2D value_bins tuple must have {SINGLE_PASS_N} entries; got {len(value_bins)}")
+        rows = [as_bin_edges(v) for v in value_bins]
+    else:
+        rows = [as_bin_edges(value_bins)] * SINGLE_PASS_N
+    n_val = len(rows[0]) - 1
+    _check_rows(rows, n_val)
+    return n_val, rows
+
+
+def _check_rows(rows, n_val):
+    if n_val < 1:
+        raise DimensionMismatch("value_bins needs at least 2 edges")
+    for t, e in enumerate(rows):
+        if len(e) < n_val + 1:
+            raise DimensionMismatch(f"value_bins[{t + 1}] needs at least {n_val + 1} edges for n_val={n_val} "
+                                    f"(got {len(e)})")
+
+
+def _row_bins(vb, n_val):
+    """A row's value axis cut to its first n_val + 1 edges: value bins above n_val are dropped, as the
+    reference's scatter does (src/Calculations/serial_single_pass.jl:857)."""
+    if len(vb) == n_val + 1:
+        return vb
+    if isinstance(vb, LinearBinEdges):
+        raise ArgumentError("a LinearBinEdges value axis must have exactly n_val + 1 edges on this backend")
+    return BinEdges(np.asarray(vb.edges)[:n_val + 1])
+
+
+def _single_pass_2d_slice(backend, x, u, distance_bins, rows, n_val, distance_metric):
+    """(6, n_dist, n_val) float64 sums and uint64 counts of one point set: one joint run per row, on the
+    row's first n_val + 1 edges (value bins above n_val are dropped, as the reference's scatter does,
+    src/Calculations/serial_single_pass.jl:858)."""
+    nd = len(distance_bins) - 1
+    s = np.zeros((SINGLE_PASS_N, nd, n_val))
+    c = np.zeros((SINGLE_PASS_N, nd, n_val), dtype=np.uint64)
+    ot = None
+    for t in range(SINGLE_PASS_N):
+        vb = _row_bins(rows[t], n_val)
+        sums, counts, _, xcode, ucode = _run(backend, [SinglePass2DRow(t)], x, u, distance_bins, vb, distance_metric)
+        s[t] = sums.reshape((nd, n_val), order="F")
+        c[t] = counts.reshape((nd, n_val), order="F")
+        ot = _output_float_type(xcode, ucode)
+    return s, c, ot
+
+
+def _single_pass_2d_raw(backend, x, u, distance_bins, value_bins, distance_metric):
+    """(6, n_dist, n_val[, aux...]) sums and counts for point-field or auxiliary-axis input."""
+    n_val, rows = _sp2d_value_bins(value_bins)
+    shape = validate_array_shape(x, u, distance_metric)
+    if isinstance(shape, PointField):
+        return _single_pass_2d_slice(backend, x, u, distance_bins, rows, n_val, distance_metric)
+    nd = len(distance_bins) - 1
+    aux = tuple(shape.aux)
+    s = np.zeros((SINGLE_PASS_N, nd, n_val) + aux, order="F")
+    c = np.zeros((SINGLE_PASS_N, nd, n_val) + aux, dtype=np.uint64, order="F")
+    ot = None
+    for k, (xb, ub) in zip(np.ndindex(*aux[::-1]), _aux_slices(shape, x, u)):
+        idx = (slice(None),) * 3 + tuple(reversed(k))
+        sb, cb, ot = _single_pass_2d_slice(backend, xb, ub, distance_bins, rows, n_val, distance_metric)
+        s[idx] = sb
+        c[idx] = cb
+    return s, c, ot
+
+
+def calculate_structure_functions_single_pass_2d(x, u, distance_bins, value_bins, *, backend=None,
+                                                 output_type=StructureFunction2DSumsAndCounts,
+                                                 count_eltype=np.uint32, distance_metric=None):
+    """The reference's `calculate_structure_functions_single_pass_2d`
+    (src/Calculations/serial_single_pass.jl:1161-1181): the six invariants binned on distance x value
+    in one call, as a dict keyed S2, L2, T2, S3, L3, L1T2 of StructureFunction2DSumsAndCounts (the
+    joint histogram has no averaged form; _single_pass_collection_2d, :1139-1148). `value_bins` is a
+    vector shared by the six invariants or a 6-tuple of vectors."""
+    distance_metric = Euclidean() if distance_metric is None else distance_metric
+    backend = default_backend() if backend is None else backend
+    if not isinstance(backend, B200Backend):
+        raise ArgumentError(f"backend {backend!r} is not a B200Backend")
+    if output_type is not StructureFunction2DSumsAndCounts:
+        raise ArgumentError(f"Cannot produce a {getattr(output_type, '__name__', output_type)} from this "
+                            "calculation (got a StructureFunction2DSumsAndCounts). Check the `output_type` keyword.")
+    validate_array_shape(x, u, distance_metric)
+    assert_counts_representable(count_eltype, _shape_of(x)[1])
+    s, c, ot = _single_pass_2d_raw(backend, x, u, distance_bins, value_bins, distance_metric)
+    ct = np.dtype(count_eltype)
+    out = {}
+    for t, (name, op) in enumerate(SINGLE_PASS_OPERATORS.items()):
+        vb = value_bins[t] if isinstance(value_bins, tuple) else value_bins
+        out[name] = StructureFunction2DSumsAndCounts(op, distance_bins, vb, s[t].astype(ot), c[t].astype(ct))
+    return out
+
+
+def calculate_structure_functions_single_pass_2d_inplace(sums_3d, counts_3d, x, u, distance_bins, value_bins, *,
+                                                         backend=None, distance_metric=None):
+    """The reference's mutating `calculate_structure_functions_single_pass_2d!`
+    (src/Calculations/serial_single_pass.jl:712-728 with _accumulate_single_pass_2d!, :731-754 and
+    _sp2d_unpack!, :803-812): adds every row into the caller's (6, n_dist, n_val) `sums_3d` /
+    `counts_3d`."""
+    distance_metric = Euclidean() if distance_metric is None else distance_metric
+    backend = default_backend() if backend is None else backend
+    validate_array_shape(x, u, distance_metric)
+    nd = len(distance_bins) - 1
+    if sums_3d.ndim != 3 or sums_3d.shape[0] != SINGLE_PASS_N or sums_3d.shape[1] != nd:
+        raise DimensionMismatch(f"sums must have shape ({SINGLE_PASS_N}, n_bins, n_val); got {sums_3d.shape}")
+    if counts_3d.shape != sums_3d.shape:
+        raise DimensionMismatch("counts and sums must have the same shape")
+    n_val = sums_3d.shape[2]
+    _, rows = _sp2d_value_bins(value_bins)
+    _check_rows(rows, n_val)
+    s, c, _ = _single_pass_2d_slice(backend, x, u, distance_bins, rows, n_val, distance_metric)
+    sums_3d += s.astype(sums_3d.dtype)
+    counts_3d += c.astype(counts_3d.dtype)
+    return sums_3d, counts_3d
