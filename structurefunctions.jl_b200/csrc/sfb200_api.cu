@@ -873,8 +873,10 @@ extern "C" int sfb200_plan_set_launch(sfb200_plan* p, int tile, int privatizatio
 {
     if (!p) return SFB200_ERR_INVALID_ARG;
     sfb200_ctx* ctx = p->ctx;
-    if (tile != 0 && tile != 32 && tile != 64 && tile != 128 && tile != 256 && tile != 512)
-        return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile must be 0, 32, 64, 128, 256 or 512");
+    if (tile != 0 && tile != 32 && tile != 64 && tile != 128 && tile != 256 && tile != 512 && tile != 768)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile must be 0, 32, 64, 128, 256, 512 or 768");
+    if (tile == 768 && !(p->joint && p->mixed))
+        return set_err(ctx, SFB200_ERR_INVALID_ARG, "tiles of 768 points exist for the mixed joint kernel only");
     if (privatization != -1 && privatization != 0 && privatization != 1 && privatization != 2 &&
         privatization != 3 && privatization != 4 && privatization != 6 && privatization != 8 &&
         privatization != 32)
@@ -1290,7 +1292,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
             smem_hist = false;
             smem = smem_bytes(p, T, lut_bytes, false, 0);
         }
-        kc = p->mixed ? (batch ? pick_joint_mx_batch(p->sphere, p->D, p->opl) : pick_joint_mx(p->sphere, p->D, p->opl))
+        kc = p->mixed ? (batch ? pick_joint_mx_batch(p->sphere, p->D, p->opl) : pick_joint_mx(p->sphere, p->D, p->opl, T))
                    : pick_joint(p->sphere, p->D, p->fp32, smem_hist, p->df, p->opl);
         // block cells hold at most 2^31 pairs between flushes (T^2 pairs per tile pair); the mixed
         // kernel's packed cells fewer than 2^20

@@ -39,7 +39,7 @@ KernelChoice pick_joint(bool sphere, int D, bool fp32, bool smem_hist, bool df, 
 // Mixed-precision kernels (FP64 differences and numerators, FP32 normalisation and accumulation).
 KernelChoice pick_flat1d_mx(int D, int opl, int priv);
 KernelChoice pick_sphere1d_mx(int D, int opl, int priv);
-KernelChoice pick_joint_mx(bool sphere, int D, int opl);
+KernelChoice pick_joint_mx(bool sphere, int D, int opl, int T = 512);
 // FP64 chord-formulation sphere kernels (the mixed sphere kernel's algorithm in FP64).
 KernelChoice pick_sphere1d_chord64(int D, int opl, int priv);
 // Batched (serving) forms of the mixed kernels: BatchArgs parameter, run-length histogram.

@@ -916,8 +916,9 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 
-template <bool SPHERE, int D, class OPS>
-__global__ void __launch_bounds__(512, 1) k_joint_mx(const __grid_constant__ PairArgs a)
+// NT: the block size the launch bound is compiled for (512, or 768 with tighter registers)
+template <bool SPHERE, int D, class OPS, int NT = 512>
+__global__ void __launch_bounds__(NT, 1) k_joint_mx(const __grid_constant__ PairArgs a)
 {
     joint_mx_run<SPHERE, D, OPS>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }

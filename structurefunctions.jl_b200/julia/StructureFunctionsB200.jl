@@ -537,6 +537,7 @@ mutable struct B200Server
     memory_reserve::Int64
     round_pairs::Float64
     min_units::Int
+    max_wait::Float64     # seconds after which a waiting request is admitted before smaller ones
     pending::Vector{B200Ticket}
     active::Vector{ActiveSlice}
     plans::Dict{Any, Ptr{Cvoid}}
@@ -554,9 +555,10 @@ A request loop over one device (mixed precision). `start!` it, `submit!` request
 `calculate_structure_function`), `fetch_result` a ticket, `stop!` it when done.
 """
 B200Server(; device::Integer = 0, max_slots::Integer = 256, memory_reserve::Integer = 1 << 30,
-           round_pairs::Real = 6e9, min_units::Integer = 1) =
+           round_pairs::Real = 6e9, min_units::Integer = 1, max_wait::Real = 1.0) =
     B200Server(Int(device), Int(max_slots), Int64(memory_reserve), Float64(round_pairs), Int(min_units),
-               B200Ticket[], ActiveSlice[], Dict{Any, Ptr{Cvoid}}(), ReentrantLock(), false, nothing, nothing, 0)
+               Float64(max_wait), B200Ticket[], ActiveSlice[], Dict{Any, Ptr{Cvoid}}(), ReentrantLock(), false,
+               nothing, nothing, 0)
 
 """
     submit!(srv, sf, x, u, distance_bins[, value_bins]; distance_metric, count_eltype = UInt32)
@@ -675,15 +677,25 @@ function complete!(ctx, a::ActiveSlice)
     notify(t.done)
 end
 
+# The waiting request to admit next: the oldest once it has waited max_wait seconds, else the one with
+# the fewest pairs (a small request arriving while the slots hold large ones waits for one slot, not
+# for the whole queue).
+function next_pending(srv::B200Server)
+    oldest = srv.pending[1]
+    (length(srv.pending) == 1 || time() - oldest.t_submit > srv.max_wait) && return 1
+    return argmin([size(t.request.x, 2) for t in srv.pending])
+end
+
 function admit!(srv::B200Server, ctx)
     while true
         t = lock(srv.lock) do
             (isempty(srv.pending) || length(srv.active) >= srv.max_slots) && return nothing
-            head = srv.pending[1]
+            k = next_pending(srv)
+            head = srv.pending[k]
             if !isempty(srv.active) && free_bytes(ctx) - estimate_bytes(head.request) < srv.memory_reserve
                 return nothing  # wait for a slice to finish and free its memory
             end
-            popfirst!(srv.pending)
+            popat!(srv.pending, k)
         end
         t === nothing && return nothing
         try

@@ -6,7 +6,10 @@ busy with all of them at once:
 
 - Admission. A request is admitted when a slot is free and the device has room for it (free memory
   minus a reserve, checked against an estimate of the request's footprint before its buffers are
-  created). Admission is first come, first served, so a large request cannot be passed over forever.
+  created). Among the waiting requests the one with the fewest pairs goes first ("shortest"), so that
+  a small request arriving while the slots hold large ones waits for one slot, not for the whole
+  queue; a request that has waited longer than `max_wait` seconds goes first whatever its size, so a
+  large one is not passed over forever. `admission="fifo"` admits in arrival order.
 - Residency. An admitted request becomes a slice: its points are packed on the device and its
   histogram lives there until the request completes. Slices are prepared (host-to-device copy,
   ordering, packing) on `prepare_threads` worker threads, so that preparing arrivals never holds up
@@ -113,7 +116,11 @@ class Server:
     """Continuous-batching loop over an executor (see the module documentation)."""
 
     def __init__(self, executor, max_slots=256, memory_reserve=1 << 30, round_pairs=6e9, min_units=1,
-                 depth=2, prepare_threads=1, clock=time.perf_counter):
+                 depth=2, prepare_threads=1, clock=time.perf_counter, admission="shortest", max_wait=1.0):
+        if admission not in ("shortest", "fifo"):
+            raise ArgumentError(f"admission must be 'shortest' or 'fifo'; got {admission!r}")
+        self.admission = admission
+        self.max_wait = float(max_wait)
         self.ex = executor
         self.depth = max(1, int(depth)) if hasattr(executor, "wait_oldest") else 1
         self._prep = (concurrent.futures.ThreadPoolExecutor(int(prepare_threads), thread_name_prefix="sfb200-prep")
@@ -201,6 +208,14 @@ class Server:
             self._activate(t, h)
             block = False
 
+    def _next_pending(self):
+        """The waiting ticket to admit next (called under the lock, with something pending): the
+        oldest once it has waited `max_wait` seconds, else the one with the fewest pairs."""
+        oldest = self._pending[0]
+        if self.admission == "fifo" or len(self._pending) == 1 or self.clock() - oldest.t_submit > self.max_wait:
+            return oldest
+        return min(self._pending, key=lambda t: t.request.pairs)
+
     def _admit(self):
         self._harvest()
         while True:
@@ -208,11 +223,11 @@ class Server:
                 busy = len(self._active) + len(self._preparing)
                 if not self._pending or busy >= self.max_slots:
                     return
-                t = self._pending[0]
+                t = self._next_pending()
                 need = self.ex.estimate_bytes(t.request)
                 if busy and self.ex.free_bytes() - self._prep_bytes - need < self.memory_reserve:
                     return  # wait for a slice to finish and free its memory
-                self._pending.popleft()
+                self._pending.remove(t)
             if self._prep is not None:
                 self._preparing.append((t, self._prep.submit(self.ex.create, t.request), need))
                 self._prep_bytes += need

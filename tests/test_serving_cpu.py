@@ -5,7 +5,8 @@ work (256-point tiles), a round runs tile-pair ranges of several slices, and a s
 readable once every unit ran. The simulation records every range, so the tests can check the
 invariants the GPU path relies on: each tile pair of each request runs exactly once, in order;
 admission honours the slot count and the memory reserve; every admitted slice progresses in every
-round; short requests are not held behind long ones; a bad request fails alone; with pipelined
+round; short requests are not held behind long ones, in the rounds and at admission (the smallest
+waiting request is admitted first, the oldest once it has waited max_wait); a bad request fails alone; with pipelined
 rounds, no more than `depth` rounds are queued at once, rounds complete oldest first, and a slice is
 read only after every round that touched it has completed. Each invariant holds with slices prepared
 on the loop thread and on a preparation thread (prepare_threads 0 and 1).
@@ -271,3 +272,41 @@ def test_loop_failure_fails_every_ticket(prep):
         late.wait(1)
     srv.stop()
     assert ex.live == 0
+
+
+def test_smallest_waiting_request_is_admitted_first():
+    # one slot: a small request submitted after two large ones is admitted before them
+    ex = FakeExecutor()
+    srv = Server(ex, max_slots=1, round_pairs=1e5, memory_reserve=0, prepare_threads=0)
+    big = [srv.submit(req(8000)) for _ in range(2)]
+    small = srv.submit(req(400))
+    srv.run_until_idle()
+    assert small.t_admit < min(t.t_admit for t in big)
+    assert small.t_done < min(t.t_admit for t in big)  # one slot: the small request ran alone first
+
+
+def test_long_waiting_request_is_admitted_before_smaller_ones():
+    # a simulated clock: every reading advances one second, so the oldest waiting request has waited
+    # longer than max_wait by the time its slot frees and goes before a smaller, newer one
+    now = [0.0]
+
+    def clock():
+        now[0] += 1.0
+        return now[0]
+
+    ex = FakeExecutor()
+    srv = Server(ex, max_slots=1, round_pairs=1e5, memory_reserve=0, prepare_threads=0, clock=clock,
+                 max_wait=2.5)
+    old = srv.submit(req(8000))
+    srv.submit(req(7000))
+    small = srv.submit(req(400))
+    srv.run_until_idle()
+    assert old.t_admit < small.t_admit
+
+
+def test_fifo_admission_keeps_arrival_order():
+    ex = FakeExecutor()
+    srv = Server(ex, max_slots=1, round_pairs=1e5, memory_reserve=0, prepare_threads=0, admission="fifo")
+    ts = [srv.submit(req(n)) for n in (6000, 8000, 400)]
+    srv.run_until_idle()
+    assert ts[0].t_admit < ts[1].t_admit < ts[2].t_admit
