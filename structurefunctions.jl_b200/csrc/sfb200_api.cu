@@ -875,7 +875,7 @@ extern "C" int sfb200_plan_set_launch(sfb200_plan* p, int tile, int privatizatio
     sfb200_ctx* ctx = p->ctx;
     if (tile != 0 && tile != 32 && tile != 64 && tile != 128 && tile != 256 && tile != 512 && tile != 768)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "tile must be 0, 32, 64, 128, 256, 512 or 768");
-    if (tile == 768 && !(p->joint && p->mixed))
+    if (tile > 512 && !(p->joint && p->mixed))
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "tiles of 768 points exist for the mixed joint kernel only");
     if (privatization != -1 && privatization != 0 && privatization != 1 && privatization != 2 &&
         privatization != 3 && privatization != 4 && privatization != 6 && privatization != 8 &&
@@ -1235,10 +1235,18 @@ static int prepare_inputs(sfb200_plan* p, Workspace& w, const void* x, const voi
 }
 
 // Tiles of the batched kernels (one per launch, shared by every slice of the launch): 256 points for
-// the 1D histograms; 512 for the joint histogram, whose large shared table leaves room for one or two
-// blocks per SM, so that each block carries more warps.
+// the 1D histograms; for the joint histogram, whose large shared table leaves room for one block per
+// SM, 768 (flat) or 512 (sphere) points, so that each block carries many warps.
 static const int kBatchTile1D = 256;
-static const int kBatchTileJoint = 512;
+static int batch_tile(const sfb200_plan* p) { return p->joint ? (p->sphere ? 512 : 768) : kBatchTile1D; }
+
+// Default tile of a single joint run over n points: 768 points (the 768-thread kernel) for the flat
+// mixed histogram from 32768 points, 512 otherwise from there.
+static int joint_tile(const sfb200_plan* p, long long n)
+{
+    if (n >= 32768) return (p->mixed && !p->sphere) ? 768 : 512;
+    return n >= 4096 ? 256 : 64;
+}
 
 // Launch configuration of one run over n points: kernel, tile, block size, shared memory, grid and
 // the kernel arguments. `batch`: the batched (serving) form of the mixed kernels, with a fixed tile
@@ -1277,11 +1285,11 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     int flush_every = 0;
     int hist_cols = 32;
     if (p->joint) {
-        T = p->tile_ovr ? p->tile_ovr : (n >= 32768 ? 512 : (n >= 4096 ? 256 : 64));
-        if (batch) T = kBatchTileJoint;
+        T = p->tile_ovr ? p->tile_ovr : joint_tile(p, n);
+        if (batch) T = batch_tile(p);
         smem = smem_bytes(p, T, lut_bytes, true, 0);
-        while (p->mixed && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr) {
-            T /= 2;
+        while (p->mixed && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr && !batch) {
+            T = T > 512 ? 512 : T / 2;
             smem = smem_bytes(p, T, lut_bytes, true, 0);
         }
         if (smem > (size_t)dev_smem_max) {
@@ -1299,7 +1307,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
         flush_every = (int)std::max<long long>(1, (p->mixed ? (1ll << 20) - 1 : (1ll << 31)) / ((long long)T * T));
     } else {
         if (batch) {
-            T = kBatchTile1D;
+            T = batch_tile(p);
         } else if (p->tile_ovr) {
             T = p->tile_ovr;
         } else {
@@ -1350,7 +1358,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
         }
     }
     if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this plan");
-    if (batch && T != (p->joint ? kBatchTileJoint : kBatchTile1D))
+    if (batch && T != batch_tile(p))
         return set_err(ctx, SFB200_ERR_UNSUPPORTED, "histogram too large for the batched kernels' fixed tiles");
     {
         const int rc = raise_smem_limit(ctx, kc.fn, smem);

@@ -20,7 +20,7 @@ from . import _abi
 
 # (tile, privatisation, point order); privatisation -1 = the library's default; order -1 = automatic
 CANDIDATES_1D = tuple((t, p, o) for t in (128, 256) for p in (6, 3, 2, 0) for o in (-1, 0))
-CANDIDATES_JOINT = tuple((t, -1, o) for t in (256, 512) for o in (-1, 0))
+CANDIDATES_JOINT = tuple((t, -1, o) for t in (256, 512, 768) for o in (-1, 0))
 
 _cache = {}
 _lock = threading.Lock()

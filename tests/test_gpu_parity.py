@@ -139,6 +139,20 @@ def test_joint_c3_subset(precision, tol):
     check(w.ops, w.x, w.u, w.distance_bins.edges, value_bins=w.value_bins, precision=precision, tol=tol)
 
 
+@pytest.mark.parametrize("tile", [512, 768])
+def test_joint_mixed_tiles(tile):
+    """The mixed joint kernel's 512- and 768-thread forms (flat 2D and 3D, sphere) give the oracle's
+    histogram; the 768-point tile is the flat default from 32768 points."""
+    w = synthetic.config("c3", n=2600)
+    check(w.ops, w.x, w.u, w.distance_bins.edges, value_bins=w.value_bins, tol=TOL_MIXED, tile=tile)
+    w3 = synthetic.config("c1", n=1700)
+    check((SF.ProjectedStructureFunctionType(1, 0),), w3.x, w3.u, w3.distance_bins.edges,
+          value_bins=SF.LinearBinEdges(-4.0, 4.0, 97), tol=TOL_MIXED, tile=tile)
+    ws = synthetic.config("c2", n=1500)
+    check((SF.ProjectedStructureFunctionType(1, 0),), ws.x, ws.u, ws.distance_bins.edges, metric=ws.metric,
+          value_bins=SF.LinearBinEdges(-3.0, 3.0, 61), tol=TOL_MIXED, tile=tile)
+
+
 def test_joint_fp64_vector_value_bins():
     rng = np.random.default_rng(11)
     x = rng.random((2, 800))
