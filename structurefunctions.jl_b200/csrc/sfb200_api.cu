@@ -1240,11 +1240,19 @@ static int prepare_inputs(sfb200_plan* p, Workspace& w, const void* x, const voi
 static const int kBatchTile1D = 256;
 static int batch_tile(const sfb200_plan* p) { return p->joint ? (p->sphere ? 512 : 768) : kBatchTile1D; }
 
-// Default tile of a single joint run over n points: 768 points (the 768-thread kernel) for the flat
-// mixed histogram from 32768 points, 512 otherwise from there.
-static int joint_tile(const sfb200_plan* p, long long n)
+static long long tile_pairs(long long n, int T);
+
+// Default tile of a single joint run over n points. The mixed flat kernel runs one block per SM (its
+// cell table fills shared memory), so it takes the largest tile (768, 512, 256 points) that still gives
+// every SM a tile pair; the other joint kernels 512 points from 32768, 256 from 4096, else 64.
+static int joint_tile(const sfb200_plan* p, long long n, int nsm)
 {
-    if (n >= 32768) return (p->mixed && !p->sphere) ? 768 : 512;
+    if (p->mixed && !p->sphere) {
+        for (int T : {768, 512, 256})
+            if (tile_pairs(n, T) >= nsm) return T;
+        return n >= 1024 ? 256 : 64;
+    }
+    if (n >= 32768) return 512;
     return n >= 4096 ? 256 : 64;
 }
 
@@ -1285,7 +1293,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     int flush_every = 0;
     int hist_cols = 32;
     if (p->joint) {
-        T = p->tile_ovr ? p->tile_ovr : joint_tile(p, n);
+        T = p->tile_ovr ? p->tile_ovr : joint_tile(p, n, ctx->nsm);
         if (batch) T = batch_tile(p);
         smem = smem_bytes(p, T, lut_bytes, true, 0);
         while (p->mixed && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr && !batch) {

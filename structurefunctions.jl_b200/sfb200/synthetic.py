@@ -112,7 +112,15 @@ class Workload:
 
 
 def config(name, n=None):
-    """Workload `name` in {"c0", "c1", "c2", "c3"}; `n` truncates to the first n points (same seed)."""
+    """Workload `name` in {"c0", "c1", "c2", "c3"} or one of the reference's own published GPU shapes
+    {"r1d", "rjoint"}; `n` truncates to the first n points (same seed).
+
+    r1d: 2D, N = 20000, Float32, L2SF, 32 linear bins LinearBinEdges(range(0, 0.3; length = 33)) -- the
+    shape of the reference's A100 figures in gpu/SPEED_OF_LIGHT.md:37-45 and :680-686 (106.8 / 99.2
+    bapps Float32, 60.2 bapps Float64); velocity field as c0.
+    rjoint: the joint histogram at N = 20000, Float32, du_L on 64 linear value bins over +-5 sigma against
+    the same 32 distance bins -- the size of gpu/SPEED_OF_LIGHT.md:291-298 (2.95 ms Float32, 4.51 ms
+    Float64 on the A100); that document does not state the value axis, so this one is chosen."""
     if name == "c0":
         N = 4096 if n is None else n
         rng = np.random.default_rng(0)
@@ -148,6 +156,20 @@ def config(name, n=None):
                         u[:, :N].astype(np.float32), (OP.ProjectedStructureFunctionType(1, 0),),
                         BinEdges(log_edges(1e-3, math.sqrt(2.0), 64)), value_bins=vb,
                         flops_per_pair=FLOPS["c3"], sigma=sigma)
+    if name in ("r1d", "rjoint"):
+        N = 20000 if n is None else n
+        rng = np.random.default_rng(5)
+        x = rng.random((2, 20000))
+        u = planar_field(x, 32, 64.0, rng, 0.01)
+        dist = LinearBinEdges(0.0, 0.3, 33)
+        if name == "r1d":
+            return Workload("r1d 2D N=%d L2SF 32 linear bins (0, 0.3] F32" % N, x[:, :N].astype(np.float32),
+                            u[:, :N].astype(np.float32), (OP.L2SF,), dist, flops_per_pair=FLOPS["r1d"])
+        sigma = math.sqrt(2.0) * float(np.std(u.astype(np.float32).astype(np.float64).ravel()))
+        return Workload("rjoint 2D N=%d joint du_L 32x64 F32" % N, x[:, :N].astype(np.float32),
+                        u[:, :N].astype(np.float32), (OP.ProjectedStructureFunctionType(1, 0),), dist,
+                        value_bins=LinearBinEdges(-5.0 * sigma, 5.0 * sigma, 65), flops_per_pair=FLOPS["rjoint"],
+                        sigma=sigma)
     raise KeyError(name)
 
 
@@ -220,7 +242,8 @@ def serving_requests(count=2000, rate=200.0, seed=4, n_min=1000, n_max=100000, w
 #   c2 (sphere L2, per-point basis precomputed): geodesic frame, tangents and increments 107,
 #        plus 1 atan2 and 2 square roots counted as 1 each                                  = 110
 #   c3 (2D joint du_L): dx 2, r^2 3, sqrt 1, r_hat 2, du 2, dot 3, L 1, acc 1                = 15
-FLOPS = {"c0": 13, "c1": 52, "c2": 110, "c3": 15}
+#   r1d, rjoint: as c0 and c3 (sqrt 1 added to r1d for the linear bins' key)             = 14, 15
+FLOPS = {"c0": 13, "c1": 52, "c2": 110, "c3": 15, "r1d": 14, "rjoint": 15}
 
 # Operations per pair of the mixed kernel's own formulation (FP64 + FP32, same counting), for
 # reference next to FLOPS:
@@ -229,4 +252,4 @@ FLOPS = {"c0": 13, "c1": 52, "c2": 110, "c3": 15}
 #       T3 2, acc 4                                                                        = 41
 #   c2: d 3, s 3, |d|^2 5, |s|^2 5, dU 3, d.dU 5, scale 3, rsqrt 1, L 1, L^2 1, acc 1        = 31
 #   c3: dx 2, r^2 3, du 2, p 3, rsqrt 1, L 1, t 2, centre 1, acc 1                           = 16
-KERNEL_FLOPS = {"c0": 14, "c1": 41, "c2": 31, "c3": 16}
+KERNEL_FLOPS = {"c0": 14, "c1": 41, "c2": 31, "c3": 16, "r1d": 15, "rjoint": 16}

@@ -101,6 +101,36 @@ def test_flat_linear_bins(precision, tol):
     check((SF.L2SF,), x, u, bins, precision=precision, tol=tol)
 
 
+_LINEAR_CASE = {}
+
+
+def _linear_case():
+    """18500 points with LinearBinEdges(0, 0.3, 33) (the shape of the reference's own GPU benchmark) and
+    a row of points whose distances from one point fall on the edges and one ulp either side."""
+    if not _LINEAR_CASE:
+        rng = np.random.default_rng(21)
+        x = rng.random((2, 18500))
+        bins = SF.LinearBinEdges(0.0, 0.3, 33)
+        row = [0.5]
+        for e in bins.edges:
+            for v in (e, np.nextafter(e, 1.0), np.nextafter(e, 0.0)):
+                row.append(0.5 + v)
+        x[0, :len(row)] = row
+        x[1, :len(row)] = 0.5
+        u = rng.standard_normal((2, 18500))
+        _LINEAR_CASE["case"] = (x, u, bins, run_oracle((SF.L2SF,), x, u, bins))
+    return _LINEAR_CASE["case"]
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_flat_linear_bins_large(precision, tol):
+    """A LinearBinEdges distance axis at a size with many tile pairs per block: the oracle's FMA search
+    on the rounded distance, bit for bit, edges and edge +- 1 ulp included."""
+    x, u, bins, (rs, rc, ra) = _linear_case()
+    gs, gc, st = run_gpu((SF.L2SF,), x, u, bins, precision=precision)
+    compare(gs, gc, rs, rc, ra, tol)
+
+
 @pytest.mark.parametrize("precision,tol", PRECISIONS)
 def test_flat_float32_inputs(precision, tol):
     rng = np.random.default_rng(8)
