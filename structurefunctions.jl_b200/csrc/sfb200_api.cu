@@ -1329,7 +1329,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
         if (p->mixed && batch)
             kc = p->sphere ? pick_sphere1d_mx_batch(p->D, p->opl) : pick_flat1d_mx_batch(p->D, p->opl);
         else if (p->mixed)
-            kc = p->sphere ? pick_sphere1d_mx(p->D, p->opl, want) : pick_flat1d_mx(p->D, p->opl, want);
+            kc = p->sphere ? pick_sphere1d_mx(p->D, p->opl, want) : pick_flat1d_mx(p->D, p->opl, want, dlinear);
         else if (p->chord64())
             kc = pick_sphere1d_chord64(p->D, p->opl, want);
         else

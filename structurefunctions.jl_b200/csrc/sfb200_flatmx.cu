@@ -4,15 +4,21 @@
 
 namespace sfb {
 
-template <int D, class OPS, int PRIV>
+template <int D, class OPS, int PRIV, bool LIN = false>
 static KernelChoice flatmx_kernel()
 {
-    return {reinterpret_cast<const void*>(&k_flat1d_mx<D, OPS, PRIV>), 256, PRIV};
+    return {reinterpret_cast<const void*>(&k_flat1d_mx<D, OPS, PRIV, LIN>), 256, PRIV};
 }
 
+// `lin`: a LinearBinEdges distance axis; the specialised lists have a form compiled for it in the
+// default histogram modes (3, 6)
 template <int D, class OPS, bool ALL>
-static KernelChoice flatmx_entry(int priv)
+static KernelChoice flatmx_entry(int priv, bool lin)
 {
+    if constexpr (ALL) {
+        if (lin && priv == 3) return flatmx_kernel<D, OPS, 3, true>();
+        if (lin && priv == 6) return flatmx_kernel<D, OPS, 6, true>();
+    }
     switch (priv) {
     case 3: return flatmx_kernel<D, OPS, 3>();
     case 6: return flatmx_kernel<D, OPS, 6>();
@@ -26,27 +32,27 @@ static KernelChoice flatmx_entry(int priv)
 }
 
 template <int D>
-static KernelChoice flatmx_by_list(int opl, int priv)
+static KernelChoice flatmx_by_list(int opl, int priv, bool lin)
 {
     switch (opl) {
-    case OPL_L2: return flatmx_entry<D, OpList<OC_L2>, true>(priv);
-    case OPL_L3: return flatmx_entry<D, OpList<OC_L3>, true>(priv);
-    case OPL_L1: return flatmx_entry<D, OpList<OC_L1>, true>(priv);
-    case OPL_QUAD: return flatmx_entry<D, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, true>(priv);
-    case OPL_SP: return flatmx_entry<D, OpList<OC_S2, OC_L2, OC_S3, OC_L3>, false>(priv);
-    case OPL_GEN1: return flatmx_entry<D, OpList<OC_GEN>, false>(priv);
-    case OPL_GEN2: return flatmx_entry<D, OpList<OC_GEN, OC_GEN>, false>(priv);
-    case OPL_GEN4: return flatmx_entry<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv);
+    case OPL_L2: return flatmx_entry<D, OpList<OC_L2>, true>(priv, lin);
+    case OPL_L3: return flatmx_entry<D, OpList<OC_L3>, true>(priv, lin);
+    case OPL_L1: return flatmx_entry<D, OpList<OC_L1>, true>(priv, lin);
+    case OPL_QUAD: return flatmx_entry<D, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, true>(priv, lin);
+    case OPL_SP: return flatmx_entry<D, OpList<OC_S2, OC_L2, OC_S3, OC_L3>, false>(priv, lin);
+    case OPL_GEN1: return flatmx_entry<D, OpList<OC_GEN>, false>(priv, lin);
+    case OPL_GEN2: return flatmx_entry<D, OpList<OC_GEN, OC_GEN>, false>(priv, lin);
+    case OPL_GEN4: return flatmx_entry<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv, lin);
     case OPL_GEN8:
-        return flatmx_entry<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv);
+        return flatmx_entry<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv, lin);
     }
     return {nullptr, 0, 0};
 }
 
-KernelChoice pick_flat1d_mx(int D, int opl, int priv)
+KernelChoice pick_flat1d_mx(int D, int opl, int priv, bool lin)
 {
-    if (D == 2) return flatmx_by_list<2>(opl, priv);
-    if (D == 3) return flatmx_by_list<3>(opl, priv);
+    if (D == 2) return flatmx_by_list<2>(opl, priv, lin);
+    if (D == 3) return flatmx_by_list<3>(opl, priv, lin);
     return {nullptr, 0, 0};
 }
 

@@ -37,7 +37,7 @@ KernelChoice pick_flat1d(int D, bool fp32, bool df, int opl, int priv);
 KernelChoice pick_sphere1d(int D, bool fp32, int opl, int priv);
 KernelChoice pick_joint(bool sphere, int D, bool fp32, bool smem_hist, bool df, int opl);
 // Mixed-precision kernels (FP64 differences and numerators, FP32 normalisation and accumulation).
-KernelChoice pick_flat1d_mx(int D, int opl, int priv);
+KernelChoice pick_flat1d_mx(int D, int opl, int priv, bool lin = false);
 KernelChoice pick_sphere1d_mx(int D, int opl, int priv);
 KernelChoice pick_joint_mx(bool sphere, int D, int opl, int T = 512);
 // FP64 chord-formulation sphere kernels (the mixed sphere kernel's algorithm in FP64).

@@ -195,6 +195,13 @@ __device__ __noinline__ FlatValues<D, OPS> flat_values_fp64_ool(double dx0, doub
     return r;
 }
 
+// The LinearBinEdges search of a flat pair on its correctly rounded distance sqrt(r2), kept out of line
+// (the mixed kernels take it only for pairs near an edge); NaN keys fall out of range.
+static __device__ __noinline__ int linear_bin_sqrt_ool(const LinearParams* p, double r2)
+{
+    return (r2 != r2) ? p->n : linear_bin(*p, SFB_SQRT(r2));
+}
+
 // ================================================================================================
 // Flat (Euclidean) 1D
 //
@@ -204,7 +211,9 @@ __device__ __noinline__ FlatValues<D, OPS> flat_values_fp64_ool(double dx0, doub
 // ================================================================================================
 // SINGLE: the single-run kernel (J-tile sorting and the byte table compiled in); the batched kernel
 // leaves both out, so that its tighter register budget (four blocks per SM) holds without spills.
-template <int D, class OPS, int PRIV, bool SINGLE = true>
+// LIN: compiled for a LinearBinEdges distance axis (the bin from the FP32 distance, the FP64 search
+// near an edge); the other forms take the FP64 search for every pair of such an axis.
+template <int D, class OPS, int PRIV, bool SINGLE = true, bool LIN = false>
 __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, long long p1, long long ps)
 {
     constexpr int NV = OPS::n;
@@ -226,6 +235,9 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
     load_bin_table(a, smem);
     const int ku = pow2_exponent_above(a.g_stats[2]);
     const double us = ldexp(1.0, -ku);
+    // LinearBinEdges distance axis: FP32 images of the search's scale and offset, and the last index
+    const float linv = (float)a.dlin.inv_step, lnegf = (float)a.dlin.neg_f_inv;
+    const float ltop = (float)(a.dlin.n - 1);
 
     int iter = 0;
     for (long long p = p0; p < p1; p += ps, ++iter) {
@@ -265,6 +277,18 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
             bool slow;
             if (SINGLE && a.byte_lut) {
                 key = byte_bin(lut8, sqx, r2, slow);  // slow: several edges in the cell or r^2 outside FP32
+            } else if (LIN) {
+                // the FMA search's bin from the FP32 distance r2f rsqrt(r2f) (relative error below
+                // 2^-22): t = (r - first) / step, bin = floor(t) + 1 in range; within 2^-19 of the
+                // index scale from an integer (an edge), or r^2 outside FP32, the FP64 search decides
+                const float r2f = f32(r2);
+                slow = !f32_range_ok(r2f);
+                const float t = fmaf(r2f * rsqrt_normal(r2f), linv, lnegf);
+                const float fl = floorf(t);
+                const float fr = t - fl;
+                const float wt = (fabsf(t) + fabsf(lnegf)) * 0x1p-19f;
+                if (slow || !(fr > wt && fr < 1.f - wt)) key = linear_bin_sqrt_ool(&a.dlin, r2);
+                else key = t < 0.f ? 0 : (fl >= ltop ? a.dlin.n : (int)fl + 1);
             } else {
                 if (a.dist_linear) key = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
                 else key = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
@@ -309,10 +333,10 @@ __device__ __forceinline__ void flat1d_mx_run(const PairArgs& a, long long p0, l
     hist.merge(a.g_sums, a.g_counts, a.nops, a.nb, unscale);
 }
 
-template <int D, class OPS, int PRIV>
+template <int D, class OPS, int PRIV, bool LIN = false>
 __global__ void __launch_bounds__(256, OPS::n >= 4 ? 3 : 4) k_flat1d_mx(const __grid_constant__ PairArgs a)
 {
-    flat1d_mx_run<D, OPS, PRIV>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
+    flat1d_mx_run<D, OPS, PRIV, true, LIN>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.
@@ -764,6 +788,9 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
     // below this |value| (2^-8 of the largest half width) a pair of a bin near zero takes the FP64 route
     const double tiny64 = ldexp(a.vq_inv, 22);
     const float tiny32 = (float)(tiny64 / unscale[0]);
+    // LinearBinEdges distance axis: FP32 images of the search's scale and offset, and the last index
+    const float linv = (float)a.dlin.inv_step, lnegf = (float)a.dlin.neg_f_inv;
+    const float ltop = (float)(a.dlin.n - 1);
     bool cok = vfast && vqcs != 0.f && f32_zero_or_normal(vqcs) && vqfs != 0.f && f32_zero_or_normal(vqfs);
     for (int k = threadIdx.x; k < nv; k += T) {
         const double c64 = value_center(a, k + 1);
@@ -832,9 +859,19 @@ __device__ __forceinline__ void joint_mx_run(const PairArgs& a, long long p0, lo
                 if constexpr (D == 3) r2 = SFB_ADD(h2, SFB_MUL(dx[2], dx[2]));
                 if (a.byte_lut) {
                     db = byte_bin(lut8, sqx, r2, slow);  // slow: the exact route decides the bin
+                } else if (a.dist_linear) {
+                    // as the flat 1D kernel: the search's bin from the FP32 distance, the FP64 search
+                    // within 2^-19 of the index scale from an edge or for r^2 outside FP32
+                    const float r2f = f32(r2);
+                    slow = !f32_range_ok(r2f);
+                    const float t = fmaf(r2f * rsqrt_normal(r2f), linv, lnegf);
+                    const float fl = floorf(t);
+                    const float fr = t - fl;
+                    const float wt = (fabsf(t) + fabsf(lnegf)) * 0x1p-19f;
+                    if (slow || !(fr > wt && fr < 1.f - wt)) db = linear_bin_sqrt_ool(&a.dlin, r2);
+                    else db = t < 0.f ? 0 : (fl >= ltop ? a.dlin.n : (int)fl + 1);
                 } else {
-                    if (a.dist_linear) db = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
-                    else db = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+                    db = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
                     slow = !f32_range_ok(f32(r2));
                 }
                 // flat bins are exact: a pair outside the distance range needs no value
