@@ -207,12 +207,14 @@ SFB200_API int sfb200_distance_range(sfb200_plan* plan, const void* x, const voi
 /* Statistics of the last sfb200_run on this plan. */
 SFB200_API int sfb200_plan_last_stats(const sfb200_plan* plan, sfb200_stats* out);
 
-/* Autotuner override of the 1D kernels' launch: tile size (points per tile = threads per block; 0 =
- * automatic), histogram privatization depth (-1 = automatic; 0 = one warp-aggregated histogram per
- * warp; 2 = warp-aggregated with shared-memory atomics; 3 = per-lane runs added into a block table
- * of lane columns (the default); 1, 4, 8 = copies per warp updated with shared-memory atomics; 32 =
- * one column per lane of every warp), and a cap on resident blocks per SM (0 = occupancy limit).
- * No counterpart in the reference (its GPU backend has no launch knobs). */
+/* Autotuner override of a plan's launch: tile size (points per tile = threads per block; 0 =
+ * automatic; 32, 64, 128, 256, 512, and 768 for the mixed joint kernel), histogram privatization
+ * depth of the 1D kernels (-1 = automatic; 0 = one warp-aggregated histogram per warp; 2 =
+ * warp-aggregated with shared-memory atomics; 3 = per-lane runs added into a block table of lane
+ * columns; 6 = the same with two open runs per lane (flat FP64 / MIXED kernels; the default for
+ * 256-point tiles from 32768 points); 1, 4, 8 = copies per warp updated with shared-memory atomics;
+ * 32 = one column per lane of every warp), and a cap on resident blocks per SM (0 = occupancy
+ * limit). No counterpart in the reference (its GPU backend has no launch knobs). */
 SFB200_API int sfb200_plan_set_launch(sfb200_plan* plan, int tile, int privatization, int blocks_per_sm);
 
 /* Plan options for sfb200_plan_set_option. */
