@@ -484,6 +484,15 @@ __device__ __forceinline__ double sphere_primitives_mx(const double* ra, const d
     return ch2;
 }
 
+// sphere_pair_exact out of line (the pairs of the chord ambiguity band, near-coincident and
+// near-antipodal pairs are rare): the pair loop only branches to it, and the kernel parameters are read
+// in place (grid constants), so the FP64 frame's registers are not held across the loop.
+template <int D, class OPS, typename R>
+__device__ __noinline__ ExactPair<OPS::n, R> sphere_pair_exact_ool(const PairArgs* a, int i, int j, int ku)
+{
+    return sphere_pair_exact<D, OPS, R>(*a, i, j, ku);
+}
+
 template <int D, class OPS, int PRIV, typename R = float>
 __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0, long long p1, long long ps)
 {
@@ -506,8 +515,6 @@ __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0,
     // FP32 values carry velocities scaled into FP32 range; the FP64 chord kernel needs no scaling
     const int ku = sizeof(R) == 4 ? pow2_exponent_above(a.g_stats[2]) : 0;
     const double us = ldexp(1.0, -ku);
-    double unscale[NV];
-    op_unscale(OPS{}, a.gen, ku, unscale);
     constexpr int NF = 9 + (D == 3);  // stored fields
 
     int iter = 0;
@@ -542,7 +549,7 @@ __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0,
             key = sphere_chord_bin(lut, a, ch2, slow);
             eval_ops(OPS{}, L, Tt, T2, Q, D, a.gen, v);
             if (slow) {
-                const ExactPair<NV, R> ex = sphere_pair_exact<D, OPS, R>(a, i, j0 + jj, ku);
+                const ExactPair<NV, R> ex = sphere_pair_exact_ool<D, OPS, R>(&a, i, j0 + jj, ku);
                 key = ex.bin;
 #pragma unroll
                 for (int o = 0; o < NV; ++o) v[o] = ex.v[o];
@@ -575,12 +582,14 @@ __device__ __forceinline__ void sphere1d_mx_run(const PairArgs& a, long long p0,
         }
     }
     if (my_recheck) atomicAdd(&s_recheck, (unsigned long long)my_recheck);
+    double unscale[NV];  // formed after the pair loop: no registers held across it
+    op_unscale(OPS{}, a.gen, ku, unscale);
     hist.merge(a.g_sums, a.g_counts, a.nops, a.nb, unscale);
     if (threadIdx.x == 0 && s_recheck) atomicAdd(&a.g_stats[0], s_recheck);
 }
 
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
+__global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const __grid_constant__ PairArgs a)
 {
     sphere1d_mx_run<D, OPS, PRIV>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
@@ -591,14 +600,14 @@ __global__ void __launch_bounds__(256, 3) k_sphere1d_mx(const PairArgs a)
 // reference-formulation FP64 kernel (k_sphere1d_fp64: the reference's frame for every pair)
 // remains selectable with SFB200_OPT_FORMULATION.
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256, 2) k_sphere1d_chord64(const PairArgs a)
+__global__ void __launch_bounds__(256, 2) k_sphere1d_chord64(const __grid_constant__ PairArgs a)
 {
     sphere1d_mx_run<D, OPS, PRIV, double>(a, a.tp_lo + blockIdx.x, a.tp_hi, gridDim.x);
 }
 
 // Batched form: work items (slice, tile-pair range) pulled from a device counter.
 template <int D, class OPS, int PRIV>
-__global__ void __launch_bounds__(256, 3) k_sphere1d_mx_batch(const BatchArgs b)
+__global__ void __launch_bounds__(256, 3) k_sphere1d_mx_batch(const __grid_constant__ BatchArgs b)
 {
     batch_items(b, [&](const PairArgs& a, long long q0, long long q1) { sphere1d_mx_run<D, OPS, PRIV>(a, q0, q1, 1); });
 }
