@@ -49,9 +49,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4", "r1d", "rjoint"],
-                    help="c0-c4: the benchmark configs; r1d / rjoint: the reference's own published GPU shapes "
-                         "(N = 20000)")
+    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4", "r1d", "rjoint", "rsp2d"],
+                    help="c0-c4: the benchmark configs; r1d / rjoint / rsp2d: the reference's own published GPU "
+                         "shapes (N = 20000; rsp2d the two-dimensional single pass, six row histograms)")
     ap.add_argument("--requests", type=int, default=2000, help="c4: number of requests")
     ap.add_argument("--rate", type=float, default=200.0, help="c4: Poisson arrival rate per second")
     ap.add_argument("--slots", type=int, default=256, help="c4: slices resident at once (admission slots)")
@@ -460,6 +460,10 @@ def run_reference(args):
     import oracle_py
     from sfb200 import synthetic
 
+    if args.config in ("c4", "rsp2d"):
+        print(json.dumps({"impl": "reference", "unavailable": f"no CPU arm for {args.config}: the oracle restates "
+                          "the pair loop of one histogram, not the serving loop or the six-row single pass"}))
+        return
     w = synthetic.config(args.config)
     threads = max(1, oracle_py.threads_available())
     rate0, _ = cpu_sample_rate(w, min(w.n, 4096), threads)
@@ -675,6 +679,89 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def run_single_pass_2d(args):
+    """rsp2d: the two-dimensional single pass of one point set, as the library runs it -- one joint
+    histogram per row (S2, L2, T2, S3, L3, L1T2) on the device-resident points, the six launches of a
+    step timed together with CUDA events on the library's stream, L2 flushed between steps. The metric
+    counts each pair once (its six row updates included), as the reference's SP2D rate does. Runs on
+    rank 0 only (one point set; the other ranks exit without work)."""
+    import torch
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    from sfb200 import _abi, _lib, synthetic
+    from sfb200.api import plan_description
+
+    w = synthetic.config("rsp2d")
+    ctx = _lib.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    xd = torch.from_numpy(np.ascontiguousarray(np.asfortranarray(w.x).T)).cuda()
+    ud = torch.from_numpy(np.ascontiguousarray(np.asfortranarray(w.u).T)).cuda()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    flags = _abi.RUN_DEVICE_INPUT | _abi.RUN_DEVICE_OUTPUT
+    precisions = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+    clocks = ClockSampler(local)
+    out, counts_of = {}, {}
+    for k, prec in enumerate(precisions):
+        rows = []
+        for op in w.ops:
+            desc, keep = plan_description((op,), 2, w.distance_bins, w.value_bins, w.metric, prec, w.x.dtype, w.u.dtype)
+            plan = _lib.Plan(ctx, desc, keep)
+            rows.append((plan, torch.zeros(plan.n_sums, dtype=torch.float64, device="cuda"),
+                         torch.zeros(plan.n_counts, dtype=torch.int64, device="cuda")))
+
+        def step():
+            for plan, sums, counts in rows:
+                plan.run(xd.data_ptr(), ud.data_ptr(), w.n, flags, sums.data_ptr(), counts.data_ptr(), ctx.stream)
+
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                step()
+        torch.cuda.synchronize()
+        if k == 0:
+            clocks.start()
+        total, kernel_ms, launches = 0.0, [], 0
+        with torch.cuda.stream(stream):
+            for _ in range(args.steps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step()
+                e1.record(stream)
+                e1.synchronize()
+                total += e0.elapsed_time(e1)
+                sts = [plan.stats() for plan, _, _ in rows]
+                kernel_ms.append([st["kernel_ms"] for st in sts])
+                launches += sum(st["kernel_launches"] for st in sts)
+        torch.cuda.synchronize()
+        ms = total / args.steps
+        out[prec] = {"value": w.pairs / (ms * 1e-3), "ms_per_step": ms, "gpu_launches": launches,
+                     "row_kernel_ms": [round(min(r[t] for r in kernel_ms), 4) for t in range(len(rows))],
+                     "rechecked": [st["rechecked"] for st in sts]}
+        counts_of[prec] = [c.cpu().numpy() for _, _, c in rows]
+        for plan, _, _ in rows:
+            plan.close()
+    clk = clocks.stop()
+    head = out[precisions[0]]
+    line = {"metric": "single-pass 2D pair-evals/s (six row updates per pair)", "value": head["value"],
+            "unit": "pair-evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "replicas only",
+            "vs_baseline": None, "dtype": "f64",  # flat single-pass 2D rows run the FP64 joint kernel at either precision
+            "data": "synthetic (seeded; no dataset)",
+            "config": {"workload": w.name, "precision": precisions[0], "l2": "flushed between steps"},
+            "gpu_launches": head["gpu_launches"], "clocks": clk,
+            "reference_published": {"value": 2.8e10, "unit": "pair-evals/s", "hardware": "A100",
+                                    "source": "gpu/OPTIMAL_KERNEL_DESIGN.md:186,210-216 (64 slices of 20000 points)"},
+            "by_precision": out}
+    if len(precisions) == 2:
+        line["counts_equal"] = all(np.array_equal(a, b) for a, b in zip(counts_of["mixed"], counts_of["fp64"]))
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def spawn_ranks(n):
     """`--gpus N` without a launcher: run this script as N ranks under torch.distributed.run (one
     process per GPU, rendezvous on 127.0.0.1) and return its exit status."""
@@ -700,6 +787,8 @@ def main():
         run_reference(args)
     elif args.config == "c4":
         run_serving(args)
+    elif args.config == "rsp2d":
+        run_single_pass_2d(args)
     else:
         run_ours(args)
 

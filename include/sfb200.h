@@ -86,7 +86,9 @@ typedef enum {
                                 du_L = (du . dx) * inv(sqrt(r2)), sphere du_L = du . r_hat, |du|^2 = du . du,
                                 S2 = |du|^2, L2 = du_L^2, T2 = |du|^2 - L2, S3 = du_L |du|^2, L3 = du_L L2,
                                 L1T2 = du_L T2 (src/Calculations/serial_single_pass.jl:886-905 flat,
-                                :838-843 other metrics) */
+                                :838-843 other metrics). A flat joint plan of this kind at precision
+                                MIXED runs the FP64 joint kernel (faster for these rows, and within the
+                                mixed tolerance); it cannot be a batched slice. */
 } sfb200_op_kind;
 
 typedef struct {

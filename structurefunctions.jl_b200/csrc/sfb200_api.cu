@@ -88,6 +88,7 @@ struct sfb200_plan {
     bool sphere = false, joint = false;
     bool fp32 = false;   // precision FP32: FP32-bulk kernels with the FP64 recheck
     bool mixed = false;  // precision MIXED: FP64 differences / numerators, FP32 normalisation + accumulation
+    bool promoted = false;  // precision MIXED requested, the FP64 kernels run (flat single-pass 2D rows)
     bool df = false;  // FP32 records carry (hi, lo) pairs (an input is FP64, or the sphere basis)
     bool l_only = false;  // the joint value depends on du_L only (compensated in FP32)
     int D = 0, W = 0, nb = 0, nv = 0, nops = 0, nops_pad = 0, opl = 0, vorder = 1;
@@ -639,6 +640,14 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         if (o.nl < 0 || o.nt < 0 || o.nf < 0 || o.nl > 16 || o.nt > 16 || o.nf > 16)
             return set_err(ctx, SFB200_ERR_INVALID_ARG, "operator powers must be in 0..16");
     }
+    // Flat rows of the two-dimensional single pass requested at precision MIXED run the FP64 joint
+    // kernel, whose results meet the mixed tolerance too. Their cubic rows put many values within 2^-8
+    // of a half bin width of zero, which the mixed kernel recomputes pair by pair in FP64, and their
+    // small tables let the FP64 kernel run several blocks per SM. Measured on B200 (20000 points,
+    // 50 x 50 bins, six rows): 22.9 ms mixed (one row 1.8 ms, the cubic rows 4.0-5.2 ms) against
+    // 10.0 ms in FP64 (1.6-1.7 ms per row).
+    p->promoted = p->mixed && p->joint && !p->sphere && d.ops[0].kind == SFB200_OP_SP2D;
+    if (p->promoted) p->mixed = false;
     int rc = validate_bins(ctx, d.distance, "distance_bins", !p->sphere);
     if (rc) return rc;
     if (p->joint && (rc = validate_bins(ctx, d.value, "value_bins", false))) return rc;
@@ -1624,6 +1633,9 @@ extern "C" int sfb200_slice_create(sfb200_plan* p, const void* x, const void* u,
     if (!p || !out) return SFB200_ERR_INVALID_ARG;
     sfb200_ctx* ctx = p->ctx;
     *out = nullptr;
+    if (p->promoted)
+        return set_err(ctx, SFB200_ERR_UNSUPPORTED,
+                       "flat single-pass 2D rows run the FP64 joint kernel: run them with sfb200_run, not as batched slices");
     if (!p->mixed) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "batched slices need a plan of precision MIXED");
     if (n < 0) return set_err(ctx, SFB200_ERR_INVALID_ARG, "negative point count");
     if (n > (1ll << 31) - 1024) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "more than 2^31 points");

@@ -113,14 +113,18 @@ class Workload:
 
 def config(name, n=None):
     """Workload `name` in {"c0", "c1", "c2", "c3"} or one of the reference's own published GPU shapes
-    {"r1d", "rjoint"}; `n` truncates to the first n points (same seed).
+    {"r1d", "rjoint", "rsp2d"}; `n` truncates to the first n points (same seed).
 
     r1d: 2D, N = 20000, Float32, L2SF, 32 linear bins LinearBinEdges(range(0, 0.3; length = 33)) -- the
     shape of the reference's A100 figures in gpu/SPEED_OF_LIGHT.md:37-45 and :680-686 (106.8 / 99.2
     bapps Float32, 60.2 bapps Float64); velocity field as c0.
     rjoint: the joint histogram at N = 20000, Float32, du_L on 64 linear value bins over +-5 sigma against
     the same 32 distance bins -- the size of gpu/SPEED_OF_LIGHT.md:291-298 (2.95 ms Float32, 4.51 ms
-    Float64 on the A100); that document does not state the value axis, so this one is chosen."""
+    Float64 on the A100); that document does not state the value axis, so this one is chosen.
+    rsp2d: the two-dimensional single pass at N = 20000, Float32, 50 linear distance bins over (0, 0.3]
+    and one 50-bin value axis of +-5 sigma^2 shared by the six rows -- the shape of the "SP2D 50x50" rate
+    of gpu/OPTIMAL_KERNEL_DESIGN.md:186,210-216 (28 G pairs/s on the A100, 64 slices of 20000 points),
+    whose axes that document does not state either."""
     if name == "c0":
         N = 4096 if n is None else n
         rng = np.random.default_rng(0)
@@ -170,6 +174,19 @@ def config(name, n=None):
                         u[:, :N].astype(np.float32), (OP.ProjectedStructureFunctionType(1, 0),), dist,
                         value_bins=LinearBinEdges(-5.0 * sigma, 5.0 * sigma, 65), flops_per_pair=FLOPS["rjoint"],
                         sigma=sigma)
+    if name == "rsp2d":
+        from .single_pass import SINGLE_PASS_N, SinglePass2DRow  # (imports the API; kept out of module scope)
+
+        N = 20000 if n is None else n
+        rng = np.random.default_rng(6)
+        x = rng.random((2, 20000))
+        u = planar_field(x, 32, 64.0, rng, 0.01)
+        sigma = math.sqrt(2.0) * float(np.std(u.astype(np.float32).astype(np.float64).ravel()))
+        s2 = sigma * sigma
+        return Workload("rsp2d 2D N=%d single pass 2D, six rows 50x50 F32" % N, x[:, :N].astype(np.float32),
+                        u[:, :N].astype(np.float32), tuple(SinglePass2DRow(t) for t in range(SINGLE_PASS_N)),
+                        LinearBinEdges(0.0, 0.3, 51), value_bins=LinearBinEdges(-5.0 * s2, 5.0 * s2, 51),
+                        flops_per_pair=FLOPS["rsp2d"], sigma=sigma)
     raise KeyError(name)
 
 
@@ -243,7 +260,9 @@ def serving_requests(count=2000, rate=200.0, seed=4, n_min=1000, n_max=100000, w
 #        plus 1 atan2 and 2 square roots counted as 1 each                                  = 110
 #   c3 (2D joint du_L): dx 2, r^2 3, sqrt 1, r_hat 2, du 2, dot 3, L 1, acc 1                = 15
 #   r1d, rjoint: as c0 and c3 (sqrt 1 added to r1d for the linear bins' key)             = 14, 15
-FLOPS = {"c0": 13, "c1": 52, "c2": 110, "c3": 15, "r1d": 14, "rjoint": 15}
+#   rsp2d (six rows of one pair, serial_single_pass.jl:886-905): dx 2, r^2 3, du 2, inv(sqrt) 2,
+#         du_L 4, |du|^2 3, L2 / T2 / S3 / L3 / L1T2 5, acc 6                               = 27
+FLOPS = {"c0": 13, "c1": 52, "c2": 110, "c3": 15, "r1d": 14, "rjoint": 15, "rsp2d": 27}
 
 # Operations per pair of the mixed kernel's own formulation (FP64 + FP32, same counting), for
 # reference next to FLOPS:

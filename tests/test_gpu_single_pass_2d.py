@@ -110,3 +110,34 @@ def test_auxiliary_axis_slices():
         for name in NAMES:
             assert np.array_equal(sp[name].counts[:, :, b], one[name].counts)
             assert np.allclose(sp[name].sums[:, :, b], one[name].sums, rtol=1e-13, atol=0)
+
+
+def test_flat_mixed_rows_run_the_fp64_kernel():
+    """Flat rows requested at precision MIXED run the FP64 joint kernel: the oracle's FP64 tolerance holds,
+    nothing is rechecked, and such a plan refuses to become a batched slice."""
+    import ctypes
+
+    from sfb200 import _lib
+    rng = np.random.default_rng(12)
+    x = rng.random((2, 2000))
+    u = rng.standard_normal((2, 2000))
+    dist = synthetic.log_edges(1e-3, math.sqrt(2.0), 20)
+    vb = SF.LinearBinEdges(-40.0, 40.0, 41)
+    be = SF.B200Backend(precision="mixed")
+    raw_s, raw_c, _ = _single_pass_2d_raw(be, x, u, dist, vb, SF.Euclidean())
+    for t, (rs, rc, ra) in enumerate(oracle_rows(x, u, dist, (vb,) * 6)):
+        compare(np.ravel(raw_s[t], order="F"), np.ravel(raw_c[t], order="F"), rs, rc, ra, TOL_FP64)
+    ctx = _lib.Context(0)
+    try:
+        desc, keep = plan_description((SF.SinglePass2DRow(4),), 2, dist, vb, None, "mixed", x.dtype, u.dtype)
+        plan = _lib.Plan(ctx, desc, keep)
+        xs = np.asfortranarray(x)  # (D, N) column-major, the C ABI's layout
+        us = np.asfortranarray(u)
+        sums = np.zeros(plan.n_sums)
+        counts = np.zeros(plan.n_counts, dtype=np.uint64)
+        plan.run(xs.ctypes.data, us.ctypes.data, x.shape[1], 0, sums.ctypes.data, counts.ctypes.data)
+        assert plan.stats()["rechecked"] == 0
+        with pytest.raises(SF.ArgumentError, match="FP64 joint kernel"):
+            _lib.Slice(plan, xs.ctypes.data_as(ctypes.c_void_p), us.ctypes.data_as(ctypes.c_void_p), x.shape[1])
+    finally:
+        ctx.close()
