@@ -680,8 +680,9 @@ def run_serving(args):
 
 
 def run_single_pass_2d(args):
-    """rsp2d: the two-dimensional single pass of one point set, as the library runs it -- one joint
-    histogram per row (S2, L2, T2, S3, L3, L1T2) on the device-resident points, the six launches of a
+    """rsp2d: the two-dimensional single pass of one point set, as the public call runs it -- the rows
+    (S2, L2, T2, S3, L3, L1T2) grouped into as few joint launches as their cells allow (one for the six
+    rows here, sfb200.single_pass._rows_per_launch) on the device-resident points, the launches of a
     step timed together with CUDA events on the library's stream, L2 flushed between steps. The metric
     counts each pair once (its six row updates included), as the reference's SP2D rate does. Runs on
     rank 0 only (one point set; the other ranks exit without work)."""
@@ -693,8 +694,12 @@ def run_single_pass_2d(args):
     torch.cuda.set_device(local)
     from sfb200 import _abi, _lib, synthetic
     from sfb200.api import plan_description
+    from sfb200.single_pass import SINGLE_PASS_N, _rows_per_launch
 
     w = synthetic.config("rsp2d")
+    nd, nv = len(w.distance_bins) - 1, len(w.value_bins) - 1
+    k_rows = _rows_per_launch([w.value_bins] * SINGLE_PASS_N, nd, nv, w.metric, 2)
+    groups = [w.ops[t:t + k_rows] for t in range(0, SINGLE_PASS_N, k_rows)]
     ctx = _lib.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
     xd = torch.from_numpy(np.ascontiguousarray(np.asfortranarray(w.x).T)).cuda()
@@ -704,10 +709,13 @@ def run_single_pass_2d(args):
     precisions = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
     clocks = ClockSampler(local)
     out, counts_of = {}, {}
-    for k, prec in enumerate(precisions):
+    # the precisions on the grouped launches, then FP64 with one launch per row (the form before grouping)
+    variants = [(prec, prec, groups) for prec in precisions] + [("fp64, one launch per row", "fp64",
+                                                                 [(op,) for op in w.ops])]
+    for k, (label, prec, vgroups) in enumerate(variants):
         rows = []
-        for op in w.ops:
-            desc, keep = plan_description((op,), 2, w.distance_bins, w.value_bins, w.metric, prec, w.x.dtype, w.u.dtype)
+        for ops in vgroups:
+            desc, keep = plan_description(ops, 2, w.distance_bins, w.value_bins, w.metric, prec, w.x.dtype, w.u.dtype)
             plan = _lib.Plan(ctx, desc, keep)
             rows.append((plan, torch.zeros(plan.n_sums, dtype=torch.float64, device="cuda"),
                          torch.zeros(plan.n_counts, dtype=torch.int64, device="cuda")))
@@ -738,10 +746,11 @@ def run_single_pass_2d(args):
                 launches += sum(st["kernel_launches"] for st in sts)
         torch.cuda.synchronize()
         ms = total / args.steps
-        out[prec] = {"value": w.pairs / (ms * 1e-3), "ms_per_step": ms, "gpu_launches": launches,
-                     "row_kernel_ms": [round(min(r[t] for r in kernel_ms), 4) for t in range(len(rows))],
-                     "rechecked": [st["rechecked"] for st in sts]}
-        counts_of[prec] = [c.cpu().numpy() for _, _, c in rows]
+        out[label] = {"value": w.pairs / (ms * 1e-3), "ms_per_step": ms, "gpu_launches": launches,
+                      "rows_per_launch": len(vgroups[0]),
+                      "launch_kernel_ms": [round(min(r[t] for r in kernel_ms), 4) for t in range(len(rows))],
+                      "rechecked": [st["rechecked"] for st in sts]}
+        counts_of[label] = np.concatenate([c.cpu().numpy() for _, _, c in rows])
         for plan, _, _ in rows:
             plan.close()
     clk = clocks.stop()
@@ -755,9 +764,9 @@ def run_single_pass_2d(args):
             "gpu_launches": head["gpu_launches"], "clocks": clk,
             "reference_published": {"value": 2.8e10, "unit": "pair-evals/s", "hardware": "A100",
                                     "source": "gpu/OPTIMAL_KERNEL_DESIGN.md:186,210-216 (64 slices of 20000 points)"},
-            "by_precision": out}
-    if len(precisions) == 2:
-        line["counts_equal"] = all(np.array_equal(a, b) for a, b in zip(counts_of["mixed"], counts_of["fp64"]))
+            "variants": out}
+    first = next(iter(counts_of.values()))
+    line["counts_equal"] = all(np.array_equal(first, c) for c in counts_of.values())
     print(json.dumps(line), flush=True)
     ctx.close()
 

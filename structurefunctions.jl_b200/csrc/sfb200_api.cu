@@ -89,6 +89,7 @@ struct sfb200_plan {
     bool fp32 = false;   // precision FP32: FP32-bulk kernels with the FP64 recheck
     bool mixed = false;  // precision MIXED: FP64 differences / numerators, FP32 normalisation + accumulation
     bool promoted = false;  // precision MIXED requested, the FP64 kernels run (flat single-pass 2D rows)
+    int sp2d_rows = 0;      // >= 2: a joint plan of that many consecutive flat single-pass 2D rows
     bool df = false;  // FP32 records carry (hi, lo) pairs (an input is FP64, or the sphere basis)
     bool l_only = false;  // the joint value depends on du_L only (compensated in FP32)
     int D = 0, W = 0, nb = 0, nv = 0, nops = 0, nops_pad = 0, opl = 0, vorder = 1;
@@ -629,8 +630,15 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
     p->df = p->fp32 && (p->sphere || d.x_dtype == SFB200_F64 || d.u_dtype == SFB200_F64);
     if (d.n_ops < 1 || d.n_ops > SFB200_MAX_OPS)
         return set_err(ctx, SFB200_ERR_INVALID_ARG, "n_ops must be in 1..%d", SFB200_MAX_OPS);
-    if (p->joint && d.n_ops != 1)
-        return set_err(ctx, SFB200_ERR_INVALID_ARG, "a joint histogram takes exactly one operator");
+    // consecutive rows of the flat two-dimensional single pass share one joint plan (one launch)
+    bool rows = p->joint && !p->sphere && d.n_ops >= 2 && d.n_ops <= 6 && d.ops[0].nl >= 0 &&
+                d.ops[0].nl + d.n_ops <= 6;
+    for (int k = 0; rows && k < d.n_ops; ++k)
+        rows = d.ops[k].kind == SFB200_OP_SP2D && d.ops[k].nl == d.ops[0].nl + k;
+    if (p->joint && d.n_ops != 1 && !rows)
+        return set_err(ctx, SFB200_ERR_INVALID_ARG,
+                       "a joint histogram takes exactly one operator (or consecutive flat single-pass 2D rows)");
+    p->sp2d_rows = rows ? d.n_ops : 0;
     for (int k = 0; k < d.n_ops; ++k) {
         const sfb200_operator& o = d.ops[k];
         if (o.kind < SFB200_OP_PROJECTED || o.kind > SFB200_OP_SP2D)
@@ -640,14 +648,14 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         if (o.nl < 0 || o.nt < 0 || o.nf < 0 || o.nl > 16 || o.nt > 16 || o.nf > 16)
             return set_err(ctx, SFB200_ERR_INVALID_ARG, "operator powers must be in 0..16");
     }
-    // Flat rows of the two-dimensional single pass requested at precision MIXED run the FP64 joint
-    // kernel, whose results meet the mixed tolerance too. Their cubic rows put many values within 2^-8
+    // Flat rows of the two-dimensional single pass requested at precision MIXED (and plans of several
+    // rows at any precision) run the FP64 joint kernels, whose results meet those tolerances too. Their cubic rows put many values within 2^-8
     // of a half bin width of zero, which the mixed kernel recomputes pair by pair in FP64, and their
     // small tables let the FP64 kernel run several blocks per SM. Measured on B200 (20000 points,
     // 50 x 50 bins, six rows): 22.9 ms mixed (one row 1.8 ms, the cubic rows 4.0-5.2 ms) against
     // 10.0 ms in FP64 (1.6-1.7 ms per row).
-    p->promoted = p->mixed && p->joint && !p->sphere && d.ops[0].kind == SFB200_OP_SP2D;
-    if (p->promoted) p->mixed = false;
+    p->promoted = p->joint && !p->sphere && d.ops[0].kind == SFB200_OP_SP2D && (p->mixed || (p->fp32 && p->sp2d_rows));
+    if (p->promoted) p->mixed = p->fp32 = p->df = false;
     int rc = validate_bins(ctx, d.distance, "distance_bins", !p->sphere);
     if (rc) return rc;
     if (p->joint && (rc = validate_bins(ctx, d.value, "value_bins", false))) return rc;
@@ -826,8 +834,9 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         if ((e = upload(&p->d_rowlo, rowlo.data(), rowlo.size())) != cudaSuccess) return cuda_fail(ctx, e, "upload rows");
         if ((e = cudaMalloc(&p->d_vwin, sizeof(float) * (p->nb + 2))) != cudaSuccess) return cuda_fail(ctx, e, "alloc windows");
     }
-    p->n_sums = p->joint ? (long long)p->nb * p->nv : (long long)p->nb * p->nops;
-    p->n_counts = p->joint ? (long long)p->nb * p->nv : (long long)p->nb;
+    const long long jrows = std::max(1, p->sp2d_rows);  // joint matrices (single-pass rows)
+    p->n_sums = p->joint ? (long long)p->nb * p->nv * jrows : (long long)p->nb * p->nops;
+    p->n_counts = p->joint ? (long long)p->nb * p->nv * jrows : (long long)p->nb;
     if ((e = cudaMalloc(&p->ws.d_sums, sizeof(double) * p->n_sums)) != cudaSuccess) return cuda_fail(ctx, e, "alloc sums");
     if ((e = cudaMalloc(&p->ws.d_counts, sizeof(unsigned long long) * p->n_counts)) != cudaSuccess)
         return cuda_fail(ctx, e, "alloc counts");
@@ -841,7 +850,7 @@ static int plan_build(sfb200_ctx* ctx, sfb200_plan* p)
         kc = p->joint ? pick_joint_mx(p->sphere, p->D, p->opl)
                       : (p->sphere ? pick_sphere1d_mx(p->D, p->opl, 0) : pick_flat1d_mx(p->D, p->opl, 0));
     else
-        kc = p->joint ? pick_joint(p->sphere, p->D, p->fp32, true, p->df, p->opl)
+        kc = p->joint ? (p->sp2d_rows ? pick_sp2d(p->D, true, 2) : pick_joint(p->sphere, p->D, p->fp32, true, p->df, p->opl))
                       : (p->sphere ? pick_sphere1d(p->D, p->fp32, p->opl, 0)
                                    : pick_flat1d(p->D, p->fp32, p->df, p->opl, 0));
     if (!kc.fn) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "no kernel for this operator on the joint mixed path");
@@ -1137,7 +1146,7 @@ static size_t smem_bytes(const sfb200_plan* p, int T, int lut_bytes, bool smem_h
         return (size_t)lut_bytes + (size_t)rec * T * 8 + hist_bytes(true, NV, priv, NW, NBP, lc);
     }
     if (p->joint) {
-        const long long ncell = (long long)p->nb * p->nv;
+        const long long ncell = (long long)p->nb * p->nv * std::max(1, p->sp2d_rows);
         if (!p->fp32) {
             const int nx = p->sphere ? 8 : p->D;
             return (size_t)(nx + p->D) * T * 8 + (smem_hist ? (size_t)ncell * 12 : 0);
@@ -1256,6 +1265,12 @@ static long long tile_pairs(long long n, int T);
 // every SM a tile pair; the other joint kernels 512 points from 32768, 256 from 4096, else 64.
 static int joint_tile(const sfb200_plan* p, long long n, int nsm)
 {
+    if (p->sp2d_rows) {  // one block per SM (the rows' cells fill shared memory): the widest tile that
+                         // still gives every SM a tile pair
+        for (int T : {512, 256})
+            if (tile_pairs(n, T) >= nsm) return T;
+        return n >= 1024 ? 256 : 64;
+    }
     if (p->mixed && !p->sphere) {
         for (int T : {768, 512, 256})
             if (tile_pairs(n, T) >= nsm) return T;
@@ -1301,11 +1316,14 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     CK(cudaDeviceGetAttribute(&dev_smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
     int flush_every = 0;
     int hist_cols = 32;
+    // threads per point of the tile: the single-pass row groups run one block per SM (their cells fill
+    // shared memory), with two threads per point for twice the warps
+    const int split = p->sp2d_rows ? 2 : 1;
     if (p->joint) {
         T = p->tile_ovr ? p->tile_ovr : joint_tile(p, n, ctx->nsm);
         if (batch) T = batch_tile(p);
         smem = smem_bytes(p, T, lut_bytes, true, 0);
-        while (p->mixed && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr && !batch) {
+        while ((p->mixed || p->sp2d_rows) && smem > (size_t)dev_smem_max && T > 64 && !p->tile_ovr && !batch) {
             T = T > 512 ? 512 : T / 2;
             smem = smem_bytes(p, T, lut_bytes, true, 0);
         }
@@ -1318,7 +1336,8 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
             smem = smem_bytes(p, T, lut_bytes, false, 0);
         }
         kc = p->mixed ? (batch ? pick_joint_mx_batch(p->sphere, p->D, p->opl) : pick_joint_mx(p->sphere, p->D, p->opl, T))
-                   : pick_joint(p->sphere, p->D, p->fp32, smem_hist, p->df, p->opl);
+                   : p->sp2d_rows ? pick_sp2d(p->D, smem_hist, split)
+                                  : pick_joint(p->sphere, p->D, p->fp32, smem_hist, p->df, p->opl);
         // block cells hold at most 2^31 pairs between flushes (T^2 pairs per tile pair); the mixed
         // kernel's packed cells fewer than 2^20
         flush_every = (int)std::max<long long>(1, (p->mixed ? (1ll << 20) - 1 : (1ll << 31)) / ((long long)T * T));
@@ -1382,7 +1401,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
         if (rc) return rc;
     }
     int occ = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc.fn, T, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc.fn, T * split, smem));
     if (occ < 1) return set_err(ctx, SFB200_ERR_UNSUPPORTED, "kernel does not fit on an SM (%zu bytes shared)", smem);
     if (p->bps_ovr) occ = std::min(occ, p->bps_ovr);
     const long long ntp = tile_pairs(n, T);
@@ -1444,7 +1463,7 @@ static int configure(sfb200_plan* p, Workspace& w, long long n, bool batch, Laun
     a.g_stats = w.d_aux;
     out->kc = kc;
     out->T = T;
-    out->threads = T;
+    out->threads = T * split;
     out->smem = smem;
     out->ntp = ntp;
     out->grid = (long long)ctx->nsm * occ;  // resident blocks; a single run launches min(grid, ntp)

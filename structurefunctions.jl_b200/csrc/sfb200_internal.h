@@ -36,6 +36,8 @@ struct KernelChoice {
 KernelChoice pick_flat1d(int D, bool fp32, bool df, int opl, int priv);
 KernelChoice pick_sphere1d(int D, bool fp32, int opl, int priv);
 KernelChoice pick_joint(bool sphere, int D, bool fp32, bool smem_hist, bool df, int opl);
+// flat single-pass 2D, rows r0 .. r0 + n_ops - 1 (FP64), `split` (1 or 2) threads per tile point
+KernelChoice pick_sp2d(int D, bool smem_hist, int split);
 // Mixed-precision kernels (FP64 differences and numerators, FP32 normalisation and accumulation).
 KernelChoice pick_flat1d_mx(int D, int opl, int priv, bool lin = false);
 KernelChoice pick_sphere1d_mx(int D, int opl, int priv);

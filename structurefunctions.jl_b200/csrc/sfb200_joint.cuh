@@ -139,6 +139,106 @@ __global__ void __launch_bounds__(512) k_joint_fp64(const PairArgs a)
     }
 }
 
+// ------------------------------------------------------------------------------------ single pass
+// Consecutive rows r0 .. r0 + nr - 1 (nr >= 2) of the flat two-dimensional single pass in one launch,
+// on one value axis shared by the rows (src/Calculations/serial_single_pass.jl:876-909, the scatter
+// :852-864): a pair's distance bin, r^2, inv(sqrt(r2)), du_L = (du . dx) inv_r and |du|^2 are formed
+// once, then each row's invariant, its value bin and its cell update (the reference's pass does the
+// same; one launch per row would repeat the pair arithmetic for every row). Every quantity is the
+// per-row FP64 kernel's (k_joint_fp64 with x_sf_raw), so the result is that of nr single-row runs.
+// Row t's cells follow row t - 1's: sums and counts are nr consecutive (n_dist x n_val) matrices.
+// SPLIT threads share each point i of the tile (T = blockDim.x / SPLIT points), thread h of them taking
+// the j with jj = h mod SPLIT: the cells fill shared memory, so one block runs per SM, and this raises
+// its warps without narrowing the tile.
+template <int D, bool SMEM, int SPLIT>
+__global__ void __launch_bounds__(512 * SPLIT) k_sp2d_fp64(const PairArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x / SPLIT;
+    const int tid = threadIdx.x % T, half = threadIdx.x / T;
+    const int n = a.n;
+    const int nd = a.nb, nv = a.nv;
+    const int ncell = nd * nv;  // cells per row
+    const int r0 = a.gen.op[0].nl, r1 = r0 + a.nops;
+    double* sx = reinterpret_cast<double*>(smem);  // D * T
+    double* su = sx + D * T;                        // D * T
+    double* hs = su + D * T;                        // nops * ncell (SMEM)
+    unsigned* hc = reinterpret_cast<unsigned*>(hs + (SMEM ? (size_t)a.nops * ncell : 0));
+    const LutEntry64* lut = static_cast<const LutEntry64*>(a.lut);
+    const int nall = a.nops * ncell;
+
+    if constexpr (SMEM) {
+        for (int k = threadIdx.x; k < nall; k += blockDim.x) { hs[k] = 0.0; hc[k] = 0u; }
+    }
+    int iter = 0;
+    for (long long p = a.tp_lo + blockIdx.x; p < a.tp_hi; p += gridDim.x, ++iter) {
+        if constexpr (SMEM) {
+            if (iter && iter % a.flush_every == 0) {
+                __syncthreads();
+                joint_flush_fp64(a, hs, hc, nall);
+            }
+        }
+        int ti, tj;
+        decode_tile_pair(p, a.ntiles, ti, tj);
+        const int i = ti * T + tid;
+        const bool iv = i < n;
+        double xa[D], ua[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            xa[d] = iv ? a.X64[(size_t)d * n + i] : 0.0;
+            ua[d] = iv ? a.U64[(size_t)d * n + i] : 0.0;
+        }
+        __syncthreads();
+        const int j0 = tj * T;
+        const int jn = min(T, n - j0);
+        if ((int)threadIdx.x < jn) {
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                sx[d * T + threadIdx.x] = a.X64[(size_t)d * n + j0 + threadIdx.x];
+                su[d * T + threadIdx.x] = a.U64[(size_t)d * n + j0 + threadIdx.x];
+            }
+        }
+        __syncthreads();
+        if (!iv) continue;
+        const int jbeg = ((ti == tj) ? tid + 1 : 0) + half;
+        for (int jj = jbeg; jj < jn; jj += SPLIT) {
+            double dx[D], du[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                dx[d] = SFB_SUB(sx[d * T + jj], xa[d]);
+                du[d] = SFB_SUB(su[d * T + jj], ua[d]);
+            }
+            const double r2 = x_dot<D>(dx, dx);
+            int db;
+            if (a.dist_linear) db = (r2 != r2) ? a.n_edges : linear_bin(a.dlin, SFB_SQRT(r2));
+            else db = (r2 != r2) ? a.n_edges : lut64_bin(lut, a, r2);
+            if (db < 1 || db > nd) continue;
+            const double inv_r = SFB_DIV(1.0, SFB_SQRT(r2));
+            const double duL = SFB_MUL(x_dot<D>(du, dx), inv_r);
+            const double dn2 = x_dot<D>(du, du);
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+                if (t < r0 || t >= r1) continue;
+                const double v = x_sp2d_row(t, duL, dn2);
+                const int vb = value_exact_bin(a, v);
+                if (vb < 1 || vb > nv) continue;
+                const int cell = (t - r0) * ncell + (db - 1) + nd * (vb - 1);
+                if constexpr (SMEM) {
+                    atomicAdd(&hs[cell], v);
+                    atomicAdd(&hc[cell], 1u);
+                } else {
+                    atomicAdd(&a.g_sums[cell], v);
+                    atomicAdd(&a.g_counts[cell], 1ull);
+                }
+            }
+        }
+    }
+    if constexpr (SMEM) {
+        __syncthreads();
+        joint_flush_fp64(a, hs, hc, nall);
+    }
+}
+
 // ------------------------------------------------------------------------------------ mixed
 // Value-bin centre of value bin vb in [1, nv] (FP64: the offsets from it stay within half a bin
 // width even where the bin is narrow next to its centre).

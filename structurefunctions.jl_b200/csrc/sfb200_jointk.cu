@@ -34,4 +34,20 @@ KernelChoice pick_joint(bool sphere, int D, bool fp32, bool smem_hist, bool df, 
     return D == 2 ? joint_mixed<false, 2, false>(opl) : joint_mixed<false, 3, false>(opl);
 }
 
+// Consecutive rows of the flat two-dimensional single pass in one launch (FP64); `split` threads per
+// point of the tile (1 or 2).
+template <int D, bool SMEM>
+static KernelChoice sp2d_kernel(int split)
+{
+    if (split == 2) return {reinterpret_cast<const void*>(&k_sp2d_fp64<D, SMEM, 2>), 1024, 0};
+    return {reinterpret_cast<const void*>(&k_sp2d_fp64<D, SMEM, 1>), 512, 0};
+}
+
+KernelChoice pick_sp2d(int D, bool smem_hist, int split)
+{
+    if (D == 2) return smem_hist ? sp2d_kernel<2, true>(split) : sp2d_kernel<2, false>(split);
+    if (D == 3) return smem_hist ? sp2d_kernel<3, true>(split) : sp2d_kernel<3, false>(split);
+    return {nullptr, 0, 0};
+}
+
 }  // namespace sfb

@@ -24,7 +24,7 @@ from .api import (B200Backend, PointField, _aux_slices, _finalize, _output_float
                   assert_counts_representable, default_backend, validate_array_shape)
 from .bins import BinEdges, LinearBinEdges, as_bin_edges
 from .errors import ArgumentError, DimensionMismatch
-from .metrics import Euclidean
+from .metrics import Euclidean, pair_geometry_for
 from .operators import (AbstractPairwiseStructureFunctionType, DiagonalConsistentThirdOrderStructureFunction,
                         LongitudinalSecondOrderStructureFunction, OffDiagonalInconsistentThirdOrderStructureFunction,
                         SecondOrderStructureFunction, ThirdOrderStructureFunction,
@@ -236,19 +236,40 @@ def _row_bins(vb, n_val):
     return BinEdges(np.asarray(vb.edges)[:n_val + 1])
 
 
+# Shared-memory budget of the cells of one launch of several rows (FP64 sum and 32-bit count per cell;
+# 227 KB per block on B200, less the J tile).
+_ROW_CELL_BYTES = 196 * 1024
+
+
+def _rows_per_launch(rows, nd, n_val, distance_metric, D):
+    """How many consecutive rows one joint run takes: on flat geometry with one value axis shared by the
+    six rows, as many as the shared-memory cell budget holds (the pair arithmetic is then done once for
+    them); otherwise one."""
+    shared = all(r is rows[0] for r in rows) and len(rows[0]) == n_val + 1
+    if not shared or pair_geometry_for(distance_metric, D).kind != _abi.GEOM_FLAT:
+        return 1
+    return int(max(1, min(SINGLE_PASS_N, _ROW_CELL_BYTES // max(1, nd * n_val * 12))))
+
+
 def _single_pass_2d_slice(backend, x, u, distance_bins, rows, n_val, distance_metric):
-    """(6, n_dist, n_val) float64 sums and uint64 counts of one point set: one joint run per row, on the
-    row's first n_val + 1 edges (value bins above n_val are dropped, as the reference's scatter does,
-    src/Calculations/serial_single_pass.jl:858)."""
+    """(6, n_dist, n_val) float64 sums and uint64 counts of one point set, on each row's first n_val + 1
+    edges (value bins above n_val are dropped, as the reference's scatter does,
+    src/Calculations/serial_single_pass.jl:858): one joint run per group of consecutive rows (several
+    rows per run on flat geometry with a shared value axis, see _rows_per_launch; one otherwise)."""
     nd = len(distance_bins) - 1
     s = np.zeros((SINGLE_PASS_N, nd, n_val))
     c = np.zeros((SINGLE_PASS_N, nd, n_val), dtype=np.uint64)
     ot = None
-    for t in range(SINGLE_PASS_N):
-        vb = _row_bins(rows[t], n_val)
-        sums, counts, _, xcode, ucode = _run(backend, [SinglePass2DRow(t)], x, u, distance_bins, vb, distance_metric)
-        s[t] = sums.reshape((nd, n_val), order="F")
-        c[t] = counts.reshape((nd, n_val), order="F")
+    k = _rows_per_launch(rows, nd, n_val, distance_metric, _shape_of(u)[0])
+    for t0 in range(0, SINGLE_PASS_N, k):
+        group = range(t0, min(SINGLE_PASS_N, t0 + k))
+        vb = _row_bins(rows[t0], n_val)
+        sums, counts, _, xcode, ucode = _run(backend, [SinglePass2DRow(t) for t in group], x, u, distance_bins, vb,
+                                             distance_metric)
+        m = nd * n_val
+        for g, t in enumerate(group):
+            s[t] = sums[g * m:(g + 1) * m].reshape((nd, n_val), order="F")
+            c[t] = counts[g * m:(g + 1) * m].reshape((nd, n_val), order="F")
         ot = _output_float_type(xcode, ucode)
     return s, c, ot
 

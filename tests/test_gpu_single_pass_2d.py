@@ -141,3 +141,41 @@ def test_flat_mixed_rows_run_the_fp64_kernel():
             _lib.Slice(plan, xs.ctypes.data_as(ctypes.c_void_p), us.ctypes.data_as(ctypes.c_void_p), x.shape[1])
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("D", [2, 3])
+def test_row_group_plan_equals_single_row_plans(D):
+    """A joint plan of consecutive flat rows (here rows 1-3, one launch) gives each row's single-row plan
+    result: counts bit-exact, sums to FP64 rounding (the cell updates come in another order); rows that
+    are not consecutive are refused."""
+    from sfb200 import _lib
+    rng = np.random.default_rng(13 + D)
+    n = 1800
+    x = np.asfortranarray(rng.random((D, n)))
+    u = np.asfortranarray(rng.standard_normal((D, n)))
+    dist = synthetic.log_edges(1e-3, math.sqrt(float(D)), 24)
+    vb = SF.LinearBinEdges(-6.0, 10.0, 33)
+    ctx = _lib.Context(0)
+    try:
+        def run(rows):
+            desc, keep = plan_description(tuple(SF.SinglePass2DRow(t) for t in rows), D, dist, vb, None, "mixed",
+                                          x.dtype, u.dtype)
+            plan = _lib.Plan(ctx, desc, keep)
+            sums = np.zeros(plan.n_sums)
+            counts = np.zeros(plan.n_counts, dtype=np.uint64)
+            plan.run(x.ctypes.data, u.ctypes.data, n, 0, sums.ctypes.data, counts.ctypes.data)
+            return sums, counts
+
+        gs, gc = run((1, 2, 3))
+        m = 24 * 32
+        assert gs.size == 3 * m and gc.size == 3 * m
+        for g, t in enumerate((1, 2, 3)):
+            s1, c1 = run((t,))
+            assert np.array_equal(gc[g * m:(g + 1) * m], c1)
+            # the value axis has an edge at 0, so a cell's values share one sign (no cancellation)
+            assert np.allclose(gs[g * m:(g + 1) * m], s1, rtol=1e-11, atol=1e-300)
+        assert int(gc.sum()) > 0
+        with pytest.raises(SF.ArgumentError, match="consecutive"):
+            run((1, 3))
+    finally:
+        ctx.close()
