@@ -28,8 +28,9 @@
  *   - Outputs: sums are double, counts are uint64. For a 1D plan with n_ops operators and nb
  *     distance bins, sums is (nb, n_ops) column-major (operator k at sums + k*nb) and counts
  *     has nb entries (shared by all operators: a pair is counted once per bin). For a joint plan
- *     (exactly one operator), sums and counts are (n_dist, n_val) column-major, as the reference's
- *     StructureFunction2DSumsAndCounts matrices.
+ *     (one operator), sums and counts are (n_dist, n_val) column-major, as the reference's
+ *     StructureFunction2DSumsAndCounts matrices; a joint plan of r single-pass 2D rows holds r such
+ *     matrices one after the other.
  *   - Every call returns 0 on success or a negative sfb200_status. Nothing aborts or traps.
  */
 #ifndef SFB200_H
@@ -88,7 +89,11 @@ typedef enum {
                                 L1T2 = du_L T2 (src/Calculations/serial_single_pass.jl:886-905 flat,
                                 :838-843 other metrics). A flat joint plan of this kind at precision
                                 MIXED runs the FP64 joint kernel (faster for these rows, and within the
-                                mixed tolerance); it cannot be a batched slice. */
+                                mixed tolerance); it cannot be a batched slice. A flat joint plan may
+                                hold 2..6 consecutive rows (ops[k].nl = ops[0].nl + k, one value axis):
+                                one FP64 launch forms each pair's arithmetic once for all of them, at
+                                any precision, and its outputs are the rows' (n_dist, n_val) matrices
+                                one after the other. */
 } sfb200_op_kind;
 
 typedef struct {
@@ -135,7 +140,7 @@ typedef struct {
     int32_t dim;         /* velocity components D in {2, 3} */
     int32_t angle_unit;  /* sphere only */
     double radius;       /* sphere only: r = radius * central angle */
-    int32_t n_ops;       /* 1..SFB200_MAX_OPS (joint plans: exactly 1) */
+    int32_t n_ops;       /* 1..SFB200_MAX_OPS (joint plans: 1, or 2..6 consecutive flat SFB200_OP_SP2D rows) */
     sfb200_operator ops[SFB200_MAX_OPS];
     sfb200_bins distance;
     int32_t joint;       /* 0: 1D histogram; 1: joint (distance x value) histogram */

@@ -369,17 +369,31 @@ function sp2d_row_bins(vb, n_val::Int)
 end
 
 # Adds the six rows of one point set into `sums` / `counts` ((6, n_dist, n_val)).
+# Rows per joint run: on flat (Euclidean) geometry with one value axis shared by the six rows, as many
+# consecutive rows as the shared-memory cell budget holds (one FP64 launch forms each pair's arithmetic
+# once for all of them; sfb200.h, SFB200_OP_SP2D); one otherwise.
+const SP2D_ROW_CELL_BYTES = 196 * 1024
+function sp2d_rows_per_run(value_bins, nd::Int, n_val::Int, metric)
+    (value_bins isa Tuple || !(metric isa DI.Euclidean)) && return 1
+    return clamp(SP2D_ROW_CELL_BYTES ÷ max(1, 12 * nd * n_val), 1, SFC.SINGLE_PASS_N)
+end
+
 function single_pass_2d_into!(b::B200Backend, sums::AbstractArray, counts::AbstractArray, x, u, distance_bins,
                               value_bins, metric)
     nd, n_val = size(sums, 2), size(sums, 3)
     SFC._validate_value_bins!(value_bins, n_val)
-    s = zeros(Float64, nd * n_val)
-    c = zeros(UInt64, nd * n_val)
-    for t in 1:SFC.SINGLE_PASS_N
-        vb = sp2d_row_bins(value_bins isa Tuple ? value_bins[t] : value_bins, n_val)
-        run_pairs(b, (SP2DRow(t),), x, u, distance_bins, vb, metric, s, c, UInt32(0))
-        @views sums[t, :, :] .+= reshape(s, nd, n_val)
-        @views counts[t, :, :] .+= reshape(c, nd, n_val)
+    k = sp2d_rows_per_run(value_bins, nd, n_val, metric)
+    m = nd * n_val
+    s = zeros(Float64, k * m)
+    c = zeros(UInt64, k * m)
+    for t0 in 1:k:SFC.SINGLE_PASS_N
+        rows = t0:min(SFC.SINGLE_PASS_N, t0 + k - 1)
+        vb = sp2d_row_bins(value_bins isa Tuple ? value_bins[t0] : value_bins, n_val)
+        run_pairs(b, Tuple(SP2DRow(t) for t in rows), x, u, distance_bins, vb, metric, s, c, UInt32(0))
+        for (g, t) in enumerate(rows)
+            @views sums[t, :, :] .+= reshape(s[(g - 1) * m + 1:g * m], nd, n_val)
+            @views counts[t, :, :] .+= reshape(c[(g - 1) * m + 1:g * m], nd, n_val)
+        end
     end
     return sums, counts
 end
