@@ -49,9 +49,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4", "r1d", "rjoint", "rsp2d"],
-                    help="c0-c4: the benchmark configs; r1d / rjoint / rsp2d: the reference's own published GPU "
-                         "shapes (N = 20000; rsp2d the two-dimensional single pass, six row histograms)")
+    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4", "r1d", "rjoint", "rsp1d",
+                                                       "rsp2d"],
+                    help="c0-c4: the benchmark configs; r1d / rjoint / rsp1d / rsp2d: the reference's own published "
+                         "GPU shapes (N = 20000; rsp1d / rsp2d the one- and two-dimensional single pass)")
     ap.add_argument("--requests", type=int, default=2000, help="c4: number of requests")
     ap.add_argument("--rate", type=float, default=200.0, help="c4: Poisson arrival rate per second")
     ap.add_argument("--slots", type=int, default=256, help="c4: slices resident at once (admission slots)")

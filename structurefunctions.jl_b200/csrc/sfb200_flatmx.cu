@@ -10,12 +10,12 @@ static KernelChoice flatmx_kernel()
     return {reinterpret_cast<const void*>(&k_flat1d_mx<D, OPS, PRIV, LIN>), 256, PRIV};
 }
 
-// `lin`: a LinearBinEdges distance axis; the specialised lists have a form compiled for it in the
+// `lin`: a LinearBinEdges distance axis; the specialised lists (LINF) have a form compiled for it in the
 // default histogram modes (3, 6)
-template <int D, class OPS, bool ALL>
+template <int D, class OPS, bool ALL, bool LINF = ALL>
 static KernelChoice flatmx_entry(int priv, bool lin)
 {
-    if constexpr (ALL) {
+    if constexpr (LINF) {
         if (lin && priv == 3) return flatmx_kernel<D, OPS, 3, true>();
         if (lin && priv == 6) return flatmx_kernel<D, OPS, 6, true>();
     }
@@ -39,7 +39,7 @@ static KernelChoice flatmx_by_list(int opl, int priv, bool lin)
     case OPL_L3: return flatmx_entry<D, OpList<OC_L3>, true>(priv, lin);
     case OPL_L1: return flatmx_entry<D, OpList<OC_L1>, true>(priv, lin);
     case OPL_QUAD: return flatmx_entry<D, OpList<OC_L2, OC_T2, OC_L3, OC_T3>, true>(priv, lin);
-    case OPL_SP: return flatmx_entry<D, OpList<OC_S2, OC_L2, OC_S3, OC_L3>, false>(priv, lin);
+    case OPL_SP: return flatmx_entry<D, OpList<OC_S2, OC_L2, OC_S3, OC_L3>, false, true>(priv, lin);
     case OPL_GEN1: return flatmx_entry<D, OpList<OC_GEN>, false>(priv, lin);
     case OPL_GEN2: return flatmx_entry<D, OpList<OC_GEN, OC_GEN>, false>(priv, lin);
     case OPL_GEN4: return flatmx_entry<D, OpList<OC_GEN, OC_GEN, OC_GEN, OC_GEN>, false>(priv, lin);

@@ -113,7 +113,7 @@ class Workload:
 
 def config(name, n=None):
     """Workload `name` in {"c0", "c1", "c2", "c3"} or one of the reference's own published GPU shapes
-    {"r1d", "rjoint", "rsp2d"}; `n` truncates to the first n points (same seed).
+    {"r1d", "rjoint", "rsp1d", "rsp2d"}; `n` truncates to the first n points (same seed).
 
     r1d: 2D, N = 20000, Float32, L2SF, 32 linear bins LinearBinEdges(range(0, 0.3; length = 33)) -- the
     shape of the reference's A100 figures in gpu/SPEED_OF_LIGHT.md:37-45 and :680-686 (106.8 / 99.2
@@ -121,6 +121,9 @@ def config(name, n=None):
     rjoint: the joint histogram at N = 20000, Float32, du_L on 64 linear value bins over +-5 sigma against
     the same 32 distance bins -- the size of gpu/SPEED_OF_LIGHT.md:291-298 (2.95 ms Float32, 4.51 ms
     Float64 on the A100); that document does not state the value axis, so this one is chosen.
+    rsp1d: the one-dimensional single pass (the fused S2/L2/S3/L3 accumulation behind
+    calculate_structure_functions_single_pass) on r1d's points and bins -- the shape of the "SP1D" rate
+    of gpu/OPTIMAL_KERNEL_DESIGN.md:210-216 (43 G pairs/s on the A100, slices of 20000 points).
     rsp2d: the two-dimensional single pass at N = 20000, Float32, 50 linear distance bins over (0, 0.3]
     and one 50-bin value axis of +-5 sigma^2 shared by the six rows -- the shape of the "SP2D 50x50" rate
     of gpu/OPTIMAL_KERNEL_DESIGN.md:186,210-216 (28 G pairs/s on the A100, 64 slices of 20000 points),
@@ -160,7 +163,7 @@ def config(name, n=None):
                         u[:, :N].astype(np.float32), (OP.ProjectedStructureFunctionType(1, 0),),
                         BinEdges(log_edges(1e-3, math.sqrt(2.0), 64)), value_bins=vb,
                         flops_per_pair=FLOPS["c3"], sigma=sigma)
-    if name in ("r1d", "rjoint"):
+    if name in ("r1d", "rjoint", "rsp1d"):
         N = 20000 if n is None else n
         rng = np.random.default_rng(5)
         x = rng.random((2, 20000))
@@ -169,6 +172,10 @@ def config(name, n=None):
         if name == "r1d":
             return Workload("r1d 2D N=%d L2SF 32 linear bins (0, 0.3] F32" % N, x[:, :N].astype(np.float32),
                             u[:, :N].astype(np.float32), (OP.L2SF,), dist, flops_per_pair=FLOPS["r1d"])
+        if name == "rsp1d":
+            return Workload("rsp1d 2D N=%d single pass S2/L2/S3/L3 32 linear bins (0, 0.3] F32" % N,
+                            x[:, :N].astype(np.float32), u[:, :N].astype(np.float32),
+                            (OP.S2SF, OP.L2SF, OP.S3SF, OP.L3SF), dist, flops_per_pair=FLOPS["rsp1d"])
         sigma = math.sqrt(2.0) * float(np.std(u.astype(np.float32).astype(np.float64).ravel()))
         return Workload("rjoint 2D N=%d joint du_L 32x64 F32" % N, x[:, :N].astype(np.float32),
                         u[:, :N].astype(np.float32), (OP.ProjectedStructureFunctionType(1, 0),), dist,
@@ -260,9 +267,11 @@ def serving_requests(count=2000, rate=200.0, seed=4, n_min=1000, n_max=100000, w
 #        plus 1 atan2 and 2 square roots counted as 1 each                                  = 110
 #   c3 (2D joint du_L): dx 2, r^2 3, sqrt 1, r_hat 2, du 2, dot 3, L 1, acc 1                = 15
 #   r1d, rjoint: as c0 and c3 (sqrt 1 added to r1d for the linear bins' key)             = 14, 15
+#   rsp1d (S2, L2, S3, L3 of one pair, serial_single_pass.jl:151-400): dx 2, r^2 3, du 2,
+#         inv(sqrt) 2, du_L 4, |du|^2 3, L2 / S3 / L3 3, acc 4                              = 23
 #   rsp2d (six rows of one pair, serial_single_pass.jl:886-905): dx 2, r^2 3, du 2, inv(sqrt) 2,
 #         du_L 4, |du|^2 3, L2 / T2 / S3 / L3 / L1T2 5, acc 6                               = 27
-FLOPS = {"c0": 13, "c1": 52, "c2": 110, "c3": 15, "r1d": 14, "rjoint": 15, "rsp2d": 27}
+FLOPS = {"c0": 13, "c1": 52, "c2": 110, "c3": 15, "r1d": 14, "rjoint": 15, "rsp1d": 23, "rsp2d": 27}
 
 # Operations per pair of the mixed kernel's own formulation (FP64 + FP32, same counting), for
 # reference next to FLOPS:
@@ -271,4 +280,6 @@ FLOPS = {"c0": 13, "c1": 52, "c2": 110, "c3": 15, "r1d": 14, "rjoint": 15, "rsp2
 #       T3 2, acc 4                                                                        = 41
 #   c2: d 3, s 3, |d|^2 5, |s|^2 5, dU 3, d.dU 5, scale 3, rsqrt 1, L 1, L^2 1, acc 1        = 31
 #   c3: dx 2, r^2 3, du 2, p 3, rsqrt 1, L 1, t 2, centre 1, acc 1                           = 16
-KERNEL_FLOPS = {"c0": 14, "c1": 41, "c2": 31, "c3": 16, "r1d": 15, "rjoint": 16}
+#   rsp1d: dx 2, r^2 3, du 2, p 3, |du|^2 3, rsqrt 1, L 1, L^2 1, S3 1, L3 1, acc 4        = 22
+#          (S2 is |du|^2 itself)
+KERNEL_FLOPS = {"c0": 14, "c1": 41, "c2": 31, "c3": 16, "r1d": 15, "rjoint": 16, "rsp1d": 22}

@@ -60,6 +60,15 @@ def test_single_pass_c1_fields_morton_order(precision, tol):
 
 
 @pytest.mark.parametrize("precision,tol", PRECISIONS)
+def test_single_pass_linear_distance_axis(precision, tol):
+    """The reference's published single-pass shape (20000 points, 32 LinearBinEdges bins over (0, 0.3]):
+    the mixed kernel's form compiled for a linear distance axis (bin from the FP32 distance, the FP64
+    search near an edge)."""
+    w = synthetic.config("rsp1d")
+    check(w.x.astype(np.float64), w.u.astype(np.float64), w.distance_bins, precision=precision, tol=tol)
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS)
 def test_single_pass_sphere(precision, tol):
     w = synthetic.config("c2", n=2000)
     # Float64 copies of the Float32 inputs (exact): the results then come back as Float64, so the
