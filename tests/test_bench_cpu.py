@@ -37,6 +37,18 @@ def test_reference_arm_prints_one_contract_line():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
 
 
+@pytest.mark.parametrize("config", ["c4", "rsp2d"])
+def test_reference_arm_without_cpu_restatement_says_so(config):
+    """The serving loop and the six-row single pass have no CPU restatement: one `unavailable` line,
+    exit 0 (no crash on a workload the oracle does not run)."""
+    p = run_bench(["--impl", "reference", "--config", config, "--steps", "1", "--warmup", "3"])
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [l for l in p.stdout.splitlines() if l.strip().startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and config in d["unavailable"]
+
+
 def test_reference_arm_is_silent_on_other_ranks():
     p = run_bench(["--impl", "reference", "--config", "c0", "--steps", "2", "--warmup", "3"],
                   {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})

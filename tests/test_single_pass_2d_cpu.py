@@ -11,7 +11,7 @@ import pytest
 import oracle_py
 import sfb200 as SF
 from sfb200.api import plan_description
-from sfb200.single_pass import SINGLE_PASS_OPERATORS, _row_bins, _sp2d_value_bins
+from sfb200.single_pass import SINGLE_PASS_OPERATORS, _row_bins, _rows_per_launch, _sp2d_value_bins
 
 
 def _oracle_rows(x, u, dist_edges, rows, metric=None):
@@ -149,3 +149,20 @@ def test_value_axis_validation():
     x = np.zeros((2, 3))
     with pytest.raises(SF.ArgumentError):
         SF.calculate_structure_functions_single_pass_2d(x, x, [0.0, 1.0], [0.0, 1.0], output_type=SF.StructureFunction)
+
+
+def test_rows_per_launch():
+    """Rows share one joint run on flat geometry with one shared value axis, as many as 196 KB of cells
+    (12 bytes each) hold; per-row axes and the sphere keep one run per row."""
+    shared = SF.LinearBinEdges(-1.0, 1.0, 51)
+    n, rows = _sp2d_value_bins(shared)
+    assert _rows_per_launch(rows, 50, n, SF.Euclidean(), 2) == 6          # 50 x 50: all six rows
+    n, rows = _sp2d_value_bins(np.linspace(-1.0, 1.0, 101))
+    assert _rows_per_launch(rows, 64, n, SF.Euclidean(), 3) == 2          # 64 x 100: 76.8 KB per row
+    assert _rows_per_launch(rows, 512, n, SF.Euclidean(), 2) == 1         # one row's cells exceed the budget
+    n, rows = _sp2d_value_bins((shared,) * 6)                             # a tuple of one axis object
+    assert _rows_per_launch(rows, 50, n, SF.Euclidean(), 2) == 6
+    n, rows = _sp2d_value_bins(tuple(SF.LinearBinEdges(-1.0, 1.0 + k, 51) for k in range(6)))
+    assert _rows_per_launch(rows, 50, n, SF.Euclidean(), 2) == 1          # per-row axes
+    n, rows = _sp2d_value_bins(shared)
+    assert _rows_per_launch(rows, 50, n, SF.Haversine(6371.0), 2) == 1    # sphere
