@@ -61,9 +61,9 @@ def _colmajor64(a):
 
 def out_sizes(desc):
     nd = desc.distance.n_edges - 1
-    if desc.joint:
+    if desc.joint:  # several operators: consecutive single-pass 2D rows, one (nd, nv) matrix each
         nv = desc.value.n_edges - 1
-        return nd * nv, nd * nv
+        return nd * nv * desc.n_ops, nd * nv * desc.n_ops
     return nd * desc.n_ops, nd
 
 

@@ -27,6 +27,9 @@
  *   bin average                    src/Calculations/serial.jl:132-141
  *   six-invariant single pass      src/Calculations/serial_single_pass.jl:238-270 (Euclidean SIMD loop),
  *                                  321-350 (other metrics), 209-219 (derived rows T2, L1T2)
+ *   two-dimensional single pass    src/Calculations/serial_single_pass.jl:876-909 (Euclidean SIMD loop:
+ *                                  du_L and |du|^2 once per pair), _sp2d_scatter! :852-864 (one cell
+ *                                  per row); a joint description of consecutive SFB200_OP_SP2D rows
  *
  * Third-party arithmetic that is not in the reference tree: StaticArrays `dot`/`cross` (compat 1.9,
  * plain left-to-right products and sums, restated literally), StaticArrays `normalize` (restated as
@@ -287,6 +290,24 @@ static void flat_row(const plan_view* pv, const double* x, const double* u, int6
                 if (abss) abss[(size_t)o * pv->nd + (b - 1)] += fabs(val);
             }
             counts[b - 1] += 1;
+        } else if (d->n_ops > 1) {
+            /* consecutive rows of the two-dimensional single pass on one value axis: the pass's own
+             * du_L = (du . dx) * inv(sqrt(r2)) and |du|^2 once, then each row's scatter; row o's cells
+             * follow row o - 1's (the same arithmetic as sf_raw's SFB200_OP_SP2D case) */
+            const double inv_r = 1.0 / sqrt(r2);
+            const double duL = dotn(du, dx, D) * inv_r;
+            const double dn2 = dotn(du, du, D);
+            for (int o = 0; o < d->n_ops; ++o) {
+                const double val = sp2d_row(d->ops[o].nl, duL, dn2);
+                const int64_t vb = oracle_digitize(&d->value, val);
+                if (vb >= 1 && vb <= pv->nv) {
+                    const size_t cell = (size_t)o * (size_t)(pv->nd * pv->nv) + (size_t)(b - 1) +
+                                        (size_t)pv->nd * (size_t)(vb - 1);
+                    sums[cell] += val;
+                    counts[cell] += 1;
+                    if (abss) abss[cell] += fabs(val);
+                }
+            }
         } else {
             const double val = sf_raw(&d->ops[0], D, du, dx, r2);
             const int64_t vb = oracle_digitize(&d->value, val);
@@ -409,14 +430,25 @@ static void sphere_row(const plan_view* pv, const sph_point* P, const double* u,
 
 /* ---------------------------------------------------------------- drivers */
 
+/* a joint description of several operators: consecutive flat single-pass 2D rows (one matrix each) */
 static int64_t out_len(const plan_view* pv)
 {
-    return pv->d->joint ? pv->nd * pv->nv : pv->nd * pv->d->n_ops;
+    return pv->d->joint ? pv->nd * pv->nv * pv->d->n_ops : pv->nd * pv->d->n_ops;
 }
 
 static int64_t count_len(const plan_view* pv)
 {
-    return pv->d->joint ? pv->nd * pv->nv : pv->nd;
+    return pv->d->joint ? pv->nd * pv->nv * pv->d->n_ops : pv->nd;
+}
+
+/* A joint description of several operators must be consecutive flat single-pass 2D rows. */
+static int joint_ops_ok(const sfb200_plan_desc* d)
+{
+    if (!d->joint || d->n_ops == 1) return 1;
+    if (d->geometry != SFB200_GEOM_FLAT || d->n_ops < 2 || d->n_ops > 6) return 0;
+    for (int o = 0; o < d->n_ops; ++o)
+        if (d->ops[o].kind != SFB200_OP_SP2D || d->ops[o].nl != d->ops[0].nl + o || d->ops[o].nl > 5) return 0;
+    return 1;
 }
 
 /* Rows i = i0, i0 + istep, ... (the round-robin share of src/Calculations/serial.jl:372-377 and
@@ -447,7 +479,7 @@ OR_EXPORT int oracle_run(const sfb200_plan_desc* d, const double* x, const doubl
                          int64_t i0, int64_t istep, double* sums, uint64_t* counts, double* abss)
 {
     double sqbuf[4096];
-    if (d->distance.n_edges > 4096) return -1;
+    if (d->distance.n_edges > 4096 || !joint_ops_ok(d)) return -1;
     plan_view pv;
     plan_view_init(&pv, d, sqbuf);
     sph_point* P = NULL;
@@ -467,7 +499,7 @@ OR_EXPORT int oracle_run_threaded(const sfb200_plan_desc* d, const double* x, co
                                   int64_t N, int nthreads, double* sums, uint64_t* counts)
 {
     double sqbuf[4096];
-    if (d->distance.n_edges > 4096) return -1;
+    if (d->distance.n_edges > 4096 || !joint_ops_ok(d)) return -1;
     plan_view pv;
     plan_view_init(&pv, d, sqbuf);
     sph_point* P = NULL;

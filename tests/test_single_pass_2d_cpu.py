@@ -166,3 +166,32 @@ def test_rows_per_launch():
     assert _rows_per_launch(rows, 50, n, SF.Euclidean(), 2) == 1          # per-row axes
     n, rows = _sp2d_value_bins(shared)
     assert _rows_per_launch(rows, 50, n, SF.Haversine(6371.0), 2) == 1    # sphere
+
+
+@pytest.mark.parametrize("D", [2, 3])
+def test_oracle_row_group_equals_single_rows(D):
+    """The oracle's fused pass over consecutive rows (the reference's own loop: du_L and |du|^2 once per
+    pair) gives each row's single-row result bit for bit, serial and threaded."""
+    rng = np.random.default_rng(60 + D)
+    x = rng.random((D, 700))
+    u = rng.standard_normal((D, 700))
+    dist = np.exp(np.linspace(math.log(1e-3), math.log(math.sqrt(D)), 17))
+    vb = SF.LinearBinEdges(-6.0, 10.0, 33)
+    m = 16 * 32
+    for rows in ((0, 1, 2, 3, 4, 5), (2, 3)):
+        desc, keep = plan_description(tuple(SF.SinglePass2DRow(t) for t in rows), D, dist, vb, None, "fp64",
+                                      x.dtype, u.dtype)
+        gs, gc, ga = oracle_py.run(desc, x, u, with_abs=True)
+        ts, tc = oracle_py.run(desc, x, u, threads=4)
+        assert gs.size == len(rows) * m and np.array_equal(tc, gc)
+        assert np.allclose(ts, gs, rtol=1e-12, atol=0)  # the threaded merge adds partial sums in another order
+        for g, t in enumerate(rows):
+            d1, k1 = plan_description((SF.SinglePass2DRow(t),), D, dist, vb, None, "fp64", x.dtype, u.dtype)
+            s1, c1, a1 = oracle_py.run(d1, x, u, with_abs=True)
+            assert np.array_equal(gc[g * m:(g + 1) * m], c1)
+            assert np.array_equal(gs[g * m:(g + 1) * m], s1) and np.array_equal(ga[g * m:(g + 1) * m], a1)
+        assert int(gc.sum()) > 0
+    bad, keep = plan_description((SF.SinglePass2DRow(1), SF.SinglePass2DRow(3)), D, dist, vb, None, "fp64",
+                                 x.dtype, u.dtype)
+    with pytest.raises(RuntimeError):
+        oracle_py.run(bad, x, u)
